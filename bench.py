@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SGM stereo path.
+
+Workload (default): the batched mixed-size workload - 64 seeded synthetic
+rectified pairs, resolution drawn from {320x240, 640x480, 1242x375, 1280x720},
+D from {64, 128, 192}, 8 paths, 5x5 census, P1=10, P2=120, subpixel, LR check
+(tolerance 1). One step = one batched pass (census, all 8 paths of all pairs,
+WTA + LR) over the 64 pairs with the images already in device memory.
+
+Metric: Gpixel-disparities/s (sum of W*H*D over pairs / seconds), whole job.
+Also reported: the plain per-pair path on the same pairs (one synchronous
+compute_disparity call per pair, like the reference) with p50/p99 latency per
+pair, the end-to-end rate through the C ABI with host buffers (H2D of the
+images and D2H of the disparity maps inside the timed region), the roofline
+of the aggregation kernel, and the CPU oracle on a bounded sample.
+
+Multi-GPU (torchrun): replicas only - every rank runs its own 64 pairs
+(different seeds), no data-path collective; value = all ranks' pixel-
+disparities / the slowest rank's time.
+
+--impl reference: the reference algorithm on the host cores (the CPU
+restatement in oracle/, since the reference's Metal GPU path cannot run here),
+same metric and workload, each step a bounded sample of the pairs.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "vx-rs_b200"))
+
+METRIC = "SGM Gpixel-disparities/s (batched, mixed sizes, 8 paths)"
+UNIT = "Gpd/s"
+SIZES = [(320, 240), (640, 480), (1242, 375), (1280, 720)]
+DISPARITIES = [64, 128, 192]
+NUM_PAIRS = 64
+
+
+def workload(rank: int):
+    """64 (w, h, D, seed) tuples; seeds differ per rank (replicas)."""
+    rng = np.random.default_rng(20261203 + 7919 * rank)
+    items = []
+    for i in range(NUM_PAIRS):
+        w, h = SIZES[int(rng.integers(len(SIZES)))]
+        d = int(DISPARITIES[int(rng.integers(len(DISPARITIES)))])
+        items.append((w, h, d, 1_000_003 * (rank + 1) + i))
+    return items
+
+
+def sgm_config(vx_sgm, d):
+    return vx_sgm.SGMStereoConfig(num_disparities=d, p1=10.0, p2=120.0, census_radius_x=2,
+                                  census_radius_y=2, num_paths=8, subpixel=True, lr_check=True,
+                                  lr_tolerance=1, invalid_value=-1.0)
+
+
+def make_pairs(vx_sgm, items):
+    pairs = []
+    for (w, h, d, seed) in items:
+        L, R, _ = vx_sgm.synth_pair(vx_sgm.SCENE_PLANES, w, h, 4, int(0.9 * d), seed)
+        pairs.append((L, R))
+    return pairs
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"vx_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v == "Active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])),
+                "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+def cpu_reference_rate(items, pairs, max_pd, threads):
+    """The oracle (CPU restatement of the reference algorithm) on a bounded sample:
+    leading pairs of the workload until max_pd pixel-disparities."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    done_pd, secs, n = 0, 0.0, 0
+    for (w, h, d, _), (L, R) in zip(items, pairs):
+        cfg = oracle.config(num_disparities=d, p1=10, p2=120, census_radius_x=2,
+                            census_radius_y=2, num_paths=8, subpixel=True, lr_check=True)
+        t0 = time.perf_counter()
+        oracle.sgm(L, R, cfg, nthreads=threads)
+        secs += time.perf_counter() - t0
+        done_pd += w * h * d
+        n += 1
+        if done_pd >= max_pd:
+            break
+    return done_pd / secs / 1e9, n, done_pd, secs
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import vx_sgm
+    items = workload(0)
+    threads = os.cpu_count() or 1
+    pairs = make_pairs(vx_sgm, items[:8])
+    rates = []
+    for step in range(args.warmup + args.steps):
+        rate, n, pd, secs = cpu_reference_rate(items, pairs, 3e8, threads)
+        if step >= args.warmup:
+            rates.append(rate)
+    value = float(np.mean(rates))
+    sample = f"leading {n} pairs of the workload per step ({pd / 1e6:.0f} M pd, {secs:.1f} s)"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * pd / 1e9 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": "64 mixed pairs (c2), CPU sample", "paths": 8},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=1)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    import vx_sgm
+    items = workload(rank)
+    pairs = make_pairs(vx_sgm, items)
+    cfgs = [sgm_config(vx_sgm, d) for (_, _, d, _) in items]
+    total_pd = sum(w * h * d for (w, h, d, _) in items)
+    total_px = sum(w * h for (w, h, _, _) in items)
+
+    ctx = vx_sgm.Context(local_rank)
+    sgm = vx_sgm.SGMStereo(ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    tl = [ctx.texture_gray8(L, L.shape[1], L.shape[0]) for (L, _) in pairs]
+    tr = [ctx.texture_gray8(R, R.shape[1], R.shape[0]) for (_, R) in pairs]
+    of = [ctx.texture_output_r32float(w, h) for (w, h, _, _) in items]
+    oi = [ctx.texture_output_i16(w, h) for (w, h, _, _) in items]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def batch():
+        sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
+
+    # ---- device-resident batched steps (headline value) ----
+    for _ in range(args.warmup):
+        batch()
+    ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.enable_stage_timing(True)
+    launches0 = vx_sgm.kernel_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch()
+        e1.record(stream)
+        e1.synchronize()
+    launches = vx_sgm.kernel_launch_count() - launches0
+    census_ms, agg_ms, wta_ms = ctx.stage_times()
+    ctx.enable_stage_timing(False)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    value = world * total_pd / (ms * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers ----
+    pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
+    hl = [pin(L.size, torch.uint8).reshape(L.shape) for (L, _) in pairs]
+    hr = [pin(R.size, torch.uint8).reshape(R.shape) for (_, R) in pairs]
+    ho = [pin(w * h, torch.float32).reshape(h, w) for (w, h, _, _) in items]
+    for (L, R), a, b in zip(pairs, hl, hr):
+        a[...] = L
+        b[...] = R
+    h2d = sum(a.nbytes + b.nbytes for a, b in zip(hl, hr))
+    d2h = sum(o.nbytes for o in ho)
+
+    def e2e_step():
+        for t, a in zip(tl, hl):
+            t.upload(a, stream=ctx.stream)
+        for t, b in zip(tr, hr):
+            t.upload(b, stream=ctx.stream)
+        batch()
+        for t, o in zip(of, ho):
+            t.download(o, stream=ctx.stream)
+
+    for _ in range(2):
+        e2e_step()
+    ctx.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    e2e_value = world * total_pd / (e2e_ms * 1e-3) / 1e9
+
+    # ---- plain per-pair path (synchronous call per pair, like the reference) ----
+    lat = []
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sgm.compute_disparity(ctx, tl[0], tr[0], of[0], cfgs[0], output_i16=oi[0])
+    barrier()
+    plain_ms = 0.0
+    for _ in range(args.plain_steps):
+        for i in range(NUM_PAIRS):
+            pe0.record(stream)
+            sgm.compute_disparity(ctx, tl[i], tr[i], of[i], cfgs[i], output_i16=oi[i])
+            pe1.record(stream)
+            pe1.synchronize()
+            t = pe0.elapsed_time(pe1)
+            lat.append(t)
+            plain_ms += t
+    plain_ms = max_over_ranks(plain_ms / args.plain_steps)
+    plain_value = world * total_pd / (plain_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel (path aggregation) ----
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    census_bytes = 4  # 5x5 census: one u32 word per pixel
+    agg_bytes = sum(8 * (w * h * d * 2 + 2 * w * h * census_bytes) for (w, h, d, _) in items)
+    agg_gbs = agg_bytes / (agg_ms * 1e-3) / 1e9
+    pipeline_bytes = sum(4 * 8 * w * h * d + 6 * w * h for (w, h, d, _) in items)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": "c2: 64 mixed pairs {320x240,640x480,1242x375,1280x720} x D{64,128,192}, "
+                               "8 paths, 5x5 census, P1=10 P2=120, subpixel, LR tol 1",
+                   "pairs_per_rank": NUM_PAIRS, "pd_per_rank": total_pd, "pixels_per_rank": total_px,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "working set larger than L2 (path slabs %.1f GB per step)" % (
+                       sum(8 * w * h * d * 2 for (w, h, d, _) in items) / 1e9)},
+        "plain": {"value": plain_value, "unit": UNIT, "ms_per_pass": plain_ms,
+                  "latency_ms_p50": float(np.percentile(lat, 50)),
+                  "latency_ms_p99": float(np.percentile(lat, 99)),
+                  "batched_over_plain": value / plain_value},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
+        "roofline": {"bound": "hbm", "kernel": "path aggregation (all pairs, all paths)",
+                     "achieved": agg_gbs, "peak": peak, "unit": "GB/s", "frac": agg_gbs / peak,
+                     "peak_source": peak_src, "traffic": None,
+                     "algorithmic_bytes_per_launch": agg_bytes},
+        "pipeline_roofline": {"bytes_per_step": pipeline_bytes,
+                              "achieved_gbs": pipeline_bytes / (ms * 1e-3) / 1e9,
+                              "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / peak},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, pd, secs = cpu_reference_rate(items, pairs, 1.0e9, threads)
+        result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                  "sample": f"leading {n} of the 64 pairs ({pd / 1e6:.0f} M pd, "
+                                            f"{secs:.1f} s), oracle with {threads} threads"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/*
+ * vx_sgm.h - C ABI of the B200 (sm_100a) semi-global matching stereo library.
+ *
+ * Drop-in boundary for vx-vision's SGM path (MisterEkole/vx-rs). Each entry
+ * point names the reference interface it replaces (paths are within the
+ * vx-rs project). Plain C types only: pointers, sizes, enums, PODs.
+ *
+ * Semantics follow vx-vision/shaders/SGMStereo.metal exactly (census, Hamming
+ * cost with 64 for x-d < 0, the shader's in-place u16 path recurrence, u16
+ * accumulation, first-minimum WTA, parabola subpixel). Extensions over the
+ * reference are opt-in config fields: 4/8 paths and a left-right check.
+ *
+ * Threading: every handle may be shared between host threads; calls that
+ * take a stream are ordered on that stream, calls given a NULL stream are
+ * synchronous like the reference's commit() + waitUntilCompleted()
+ * (vx-vision/src/kernels/sgm.rs:260-261).
+ */
+#ifndef VX_SGM_H
+#define VX_SGM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Mirrors vx-vision/src/error.rs:8-23 (Error), plus codes for the additions. */
+typedef enum vx_status {
+    VX_OK = 0,
+    VX_ERR_DEVICE_NOT_FOUND = 1,   /* Error::DeviceNotFound */
+    VX_ERR_SHADER_MISSING = 2,     /* Error::ShaderMissing: kernel image absent for this GPU */
+    VX_ERR_PIPELINE_COMPILE = 3,   /* Error::PipelineCompile */
+    VX_ERR_BUFFER_ALLOC = 4,       /* Error::BufferAlloc { bytes } */
+    VX_ERR_SIZE_MISMATCH = 5,      /* Error::TextureSizeMismatch */
+    VX_ERR_INVALID_CONFIG = 6,     /* Error::InvalidConfig(String) */
+    VX_ERR_GPU = 7,                /* Error::Gpu(String) */
+    VX_ERR_BUDGET = 8,             /* request larger than the server's memory budget */
+    VX_ERR_TIMEOUT = 9,            /* a bounded wait gave up */
+    VX_ERR_INVALID_ARGUMENT = 10,  /* null handle / pointer, bad format */
+    VX_ERR_NOT_READY = 11,         /* asynchronous result not finished yet */
+    VX_ERR_CANCELLED = 12          /* request cancelled before it ran */
+} vx_status;
+
+/* Human-readable detail of the last error on the calling host thread
+ * (the String payloads of vx-vision's Error). Never NULL. */
+const char* vx_last_error(void);
+
+typedef struct vx_ctx vx_ctx;
+typedef struct vx_image vx_image;
+typedef struct vx_sgm vx_sgm;
+typedef void* vx_stream; /* a cudaStream_t; NULL = synchronous call */
+
+/* Replaces Context::new() (vx-vision/src/context.rs:26): selects a CUDA
+ * device, creates its stream and a stream-ordered device memory pool. */
+vx_status vx_ctx_create(int device_ordinal, vx_ctx** out);
+void vx_ctx_destroy(vx_ctx* ctx);
+/* The context's default stream (Context::queue(), context.rs:83). */
+vx_stream vx_ctx_stream(vx_ctx* ctx);
+/* Blocks until all work on the context's stream has finished. */
+vx_status vx_ctx_synchronize(vx_ctx* ctx);
+
+/* Image formats: R8Unorm input (texture.rs:38 from_gray8), R32Float output
+ * (texture.rs:324 output_r32float), and an int16 integer-disparity map. */
+typedef enum vx_format { VX_FORMAT_U8 = 0, VX_FORMAT_F32 = 1, VX_FORMAT_I16 = 2 } vx_format;
+
+/* Replaces Context::texture_gray8 / texture_output_r32float
+ * (context.rs:39, context.rs:64): allocates a pitched device image. */
+vx_status vx_image_create(vx_ctx* ctx, uint32_t width, uint32_t height, vx_format format,
+                          vx_image** out);
+/* Replaces Texture::from_metal_texture (texture.rs:449): wraps caller-owned
+ * device memory (pitch in bytes). The image never frees it. */
+vx_status vx_image_wrap_device(vx_ctx* ctx, void* device_ptr, size_t pitch_bytes, uint32_t width,
+                               uint32_t height, vx_format format, vx_image** out);
+void vx_image_destroy(vx_image* img);
+uint32_t vx_image_width(const vx_image* img);   /* Texture::width, texture.rs */
+uint32_t vx_image_height(const vx_image* img);  /* Texture::height */
+void* vx_image_device_ptr(const vx_image* img);
+size_t vx_image_pitch(const vx_image* img);
+/* Host <-> device copies. Replace Texture::from_gray8's replaceRegion
+ * (texture.rs:38-75) and Texture::read_r32float (texture.rs:404).
+ * host_pitch in bytes (0 = tightly packed). NULL stream = synchronous. */
+vx_status vx_image_upload(vx_image* img, const void* host, size_t host_pitch, vx_stream stream);
+vx_status vx_image_download(const vx_image* img, void* host, size_t host_pitch, vx_stream stream);
+
+/* Replaces SGMStereoConfig (vx-vision/src/kernels/sgm.rs:23-37). The first
+ * five fields are the reference's; the rest are extensions whose defaults
+ * reproduce the reference (2 paths, subpixel on, no LR check). */
+typedef struct vx_sgm_config {
+    uint32_t num_disparities; /* 1..256 (SGMStereo.metal:108 caps at 256) */
+    float p1;                 /* penalty for |dd| = 1, used as ushort(p1) */
+    float p2;                 /* penalty for |dd| > 1, used as ushort(p2) */
+    uint32_t census_radius_x;
+    uint32_t census_radius_y; /* (2rx+1)(2ry+1)-1 <= 64 census bits */
+    uint32_t num_paths;       /* 2 = reference ((1,0),(0,1)); 4; 8 */
+    uint32_t subpixel;        /* 1 = parabola refinement (reference) */
+    uint32_t lr_check;        /* 1 = left-right consistency check */
+    uint32_t lr_tolerance;    /* pixels */
+    float invalid_value;      /* written where the LR check fails */
+} vx_sgm_config;
+
+/* SGMStereoConfig::default() (sgm.rs:39-49): D=128, P1=10, P2=120, 4x3. */
+void vx_sgm_config_default(vx_sgm_config* cfg);
+/* SGMStereoConfig::new(num_disparities) (sgm.rs:51-59). */
+void vx_sgm_config_new(vx_sgm_config* cfg, uint32_t num_disparities);
+
+/* Replaces SGMStereo::new(&ctx) (sgm.rs:73-105): checks that the sm_100a
+ * kernel images load on the context's device (ShaderMissing otherwise). */
+vx_status vx_sgm_create(vx_ctx* ctx, vx_sgm** out);
+void vx_sgm_destroy(vx_sgm* sgm);
+
+/* Replaces SGMStereo::compute_disparity(&ctx, &left, &right, &output, &cfg)
+ * (sgm.rs:108-265). left/right: U8 images of equal size; out_f32: F32 image
+ * of that size (subpixel disparity, or invalid_value); out_i16: optional I16
+ * image (integer disparity, -1 where invalid). Unlike the reference, sizes and
+ * config are validated (VX_ERR_SIZE_MISMATCH / VX_ERR_INVALID_CONFIG).
+ * Intermediates come from the context's stream-ordered pool. */
+vx_status vx_sgm_compute_disparity(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left,
+                                   const vx_image* right, vx_image* out_f32, vx_image* out_i16,
+                                   const vx_sgm_config* cfg, vx_stream stream);
+
+/* Batched form of compute_disparity (no reference counterpart; the
+ * reference only has the per-pair call, sgm.rs:108): n independent pairs of
+ * any sizes and configs in one pass: one census launch, path aggregation as
+ * persistent launches over a (pair, path, scanline-group) work queue, one
+ * WTA launch. out_i16 may be NULL or contain NULLs. */
+vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
+                               const vx_image* const* right, vx_image* const* out_f32,
+                               vx_image* const* out_i16, const vx_sgm_config* cfgs,
+                               vx_stream stream);
+
+/* Device bytes of intermediate state one pair needs (census + path slabs). */
+size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg);
+
+/* Debug dump for parity tests (no reference counterpart): runs one pair and
+ * copies to host the census words (u64 per pixel, may be NULL), the per-path
+ * aggregated costs L_r (num_paths * H * W * D u16, HWD per path, may be
+ * NULL) and the summed cost volume S (H * W * D u16, may be NULL). */
+vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,
+                            const vx_sgm_config* cfg, uint64_t* census_left,
+                            uint64_t* census_right, uint16_t* path_costs, uint16_t* cost_volume);
+
+/* Per-stage device timing (no reference counterpart; the reference only times
+ * whole calls with Instant, examples/depth_to_cloud_demo.rs:48-53). Enabling
+ * (re)starts a record: every later batch records CUDA events on its stream
+ * around its census, path aggregation and WTA launches (the first 256 batches
+ * are kept). vx_ctx_stage_times waits for those events and returns the mean
+ * duration per batch of each stage in milliseconds (VX_ERR_NOT_READY when no
+ * batch ran since timing was enabled). */
+vx_status vx_ctx_enable_stage_timing(vx_ctx* ctx, int enable);
+vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms, float* wta_ms);
+
+/* Number of this library's kernel launches issued since load (all threads). */
+uint64_t vx_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VX_SGM_H */

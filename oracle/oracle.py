@@ -1,0 +1,144 @@
+"""ctypes front end of the CPU oracle (liboracle.so) and of the literal reference
+shader compiled as C++ (_ref/libsgm_ref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, always as the checker or the timed CPU baseline,
+never as the thing measured or shipped.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libsgm_ref.so")
+_P = ctypes.c_void_p
+
+
+class OracleConfig(ctypes.Structure):
+    _fields_ = [("num_disparities", ctypes.c_int32), ("p1", ctypes.c_float),
+                ("p2", ctypes.c_float), ("census_radius_x", ctypes.c_int32),
+                ("census_radius_y", ctypes.c_int32), ("num_paths", ctypes.c_int32),
+                ("subpixel", ctypes.c_int32), ("lr_check", ctypes.c_int32),
+                ("lr_tolerance", ctypes.c_int32), ("invalid_value", ctypes.c_float)]
+
+
+class OracleStats(ctypes.Structure):
+    _fields_ = [("pixel_steps", ctypes.c_uint64), ("wrap_steps", ctypes.c_uint64),
+                ("wide_values", ctypes.c_uint64)]
+
+
+_lib = None
+_ref = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        _lib = ctypes.CDLL(ORACLE_SO)
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+    return _ref
+
+
+def config(num_disparities=128, p1=10.0, p2=120.0, census_radius_x=4, census_radius_y=3,
+           num_paths=2, subpixel=True, lr_check=False, lr_tolerance=1, invalid_value=-1.0,
+           **_ignored) -> OracleConfig:
+    return OracleConfig(int(num_disparities), float(p1), float(p2), int(census_radius_x),
+                        int(census_radius_y), int(num_paths), int(bool(subpixel)),
+                        int(bool(lr_check)), int(lr_tolerance), float(invalid_value))
+
+
+def path_dir(k: int):
+    dx, dy = ctypes.c_int(), ctypes.c_int()
+    lib().oracle_path_dir(k, ctypes.byref(dx), ctypes.byref(dy))
+    return dx.value, dy.value
+
+
+def census(img: np.ndarray, rx: int, ry: int, nthreads: int = 0) -> np.ndarray:
+    img = np.ascontiguousarray(img, np.uint8)
+    h, w = img.shape
+    out = np.zeros((h, w), np.uint64)
+    r = lib().oracle_census(_P(img.ctypes.data), ctypes.c_size_t(w), w, h, rx, ry,
+                            _P(out.ctypes.data), nthreads)
+    if r != 0:
+        raise ValueError("oracle_census rejected its arguments")
+    return out
+
+
+def path_costs(cl, cr, nd, p1, p2, dx, dy, nthreads=0):
+    """L_r of one path direction, (H, W, D) u16."""
+    h, w = cl.shape
+    L = np.zeros((h, w, nd), np.uint16)
+    r = lib().oracle_path(_P(cl.ctypes.data), _P(cr.ctypes.data), w, h, nd, int(p1), int(p2),
+                          dx, dy, _P(L.ctypes.data), None, None, nthreads)
+    if r != 0:
+        raise ValueError("oracle_path rejected its arguments")
+    return L
+
+
+def sgm(left, right, cfg: OracleConfig, want_S=False, nthreads=0, stats=None):
+    """Full pipeline. Returns (disparity f32, disparity i16, S or None)."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    h, w = left.shape
+    disp = np.zeros((h, w), np.float32)
+    di = np.zeros((h, w), np.int16)
+    S = np.zeros((h, w, cfg.num_disparities), np.uint16) if want_S else None
+    r = lib().oracle_sgm(_P(left.ctypes.data), ctypes.c_size_t(w), _P(right.ctypes.data),
+                         ctypes.c_size_t(w), w, h, ctypes.byref(cfg), _P(disp.ctypes.data),
+                         _P(di.ctypes.data), _P(S.ctypes.data) if want_S else None,
+                         ctypes.byref(stats) if stats is not None else None, nthreads)
+    if r != 0:
+        raise ValueError("oracle_sgm rejected its arguments")
+    return disp, di, S
+
+
+def wta(S, cfg: OracleConfig, nthreads=0):
+    S = np.ascontiguousarray(S, np.uint16)
+    h, w, _ = S.shape
+    disp = np.zeros((h, w), np.float32)
+    di = np.zeros((h, w), np.int16)
+    r = lib().oracle_wta(_P(S.ctypes.data), w, h, ctypes.byref(cfg), _P(disp.ctypes.data),
+                         _P(di.ctypes.data), nthreads)
+    if r != 0:
+        raise ValueError("oracle_wta rejected its arguments")
+    return disp, di
+
+
+def reference_sgm(left, right, nd, p1=10.0, p2=120.0, rx=4, ry=3, nthreads=0):
+    """The reference shader itself (2 paths, subpixel). Returns (census_l, census_r, S, disp)."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    h, w = left.shape
+    cl = np.zeros((h, w, 2), np.uint32)
+    cr = np.zeros((h, w, 2), np.uint32)
+    S = np.zeros((h, w, nd), np.uint16)
+    disp = np.zeros((h, w), np.float32)
+    r = ref_lib().ref_sgm_compute(_P(left.ctypes.data), _P(right.ctypes.data), w, h, nd,
+                                  ctypes.c_float(p1), ctypes.c_float(p2), rx, ry,
+                                  _P(cl.ctypes.data), _P(cr.ctypes.data), _P(S.ctypes.data),
+                                  _P(disp.ctypes.data), nthreads)
+    if r != 0:
+        raise ValueError("ref_sgm_compute rejected its arguments")
+    as64 = lambda c: c[..., 0].astype(np.uint64) | (c[..., 1].astype(np.uint64) << np.uint64(32))
+    return as64(cl), as64(cr), S, disp

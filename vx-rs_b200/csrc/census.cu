@@ -1,0 +1,96 @@
+// Census transform for a batch of stereo pairs (both views in one launch).
+//
+// Semantics: vx-vision/shaders/SGMStereo.metal:25-66 - bit b of the descriptor
+// is set iff neighbour < centre (strict), neighbours in raster order with the
+// centre skipped, coordinates clamped to the image. The shader reads R8Unorm
+// texels as value/255 floats; comparing those is the same as comparing the
+// u8 values, which is what this kernel does.
+//
+// Layout: each 32x8 tile of one view is staged once in shared memory with its
+// (rx, ry) apron (clamped coordinates), then every thread builds one
+// descriptor from shared memory. Descriptors are written twice: row-major
+// (read by vertical and diagonal paths) and column-major (read by horizontal
+// paths, so that the 32 scanlines of a warp - 32 consecutive rows - load
+// consecutive words). Output word: u32 when the window has <= 32 bits, else u64.
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+#include "launch.hpp"
+
+namespace vxsgm {
+
+namespace {
+
+__device__ __forceinline__ int find_pair_by_tile(const PairDev* pairs, int n, int tile) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].census_tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename CT>
+__global__ void __launch_bounds__(kCensusTileW * kCensusTileH)
+census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
+    extern __shared__ uint8_t tile_px[];
+    const int pi = find_pair_by_tile(pairs, num_pairs, blockIdx.x);
+    const PairDev& pr = pairs[pi];
+    const int W = pr.width, H = pr.height, rx = pr.rx, ry = pr.ry;
+    const int tiles_x = (W + kCensusTileW - 1) / kCensusTileW;
+    const int tiles_y = (H + kCensusTileH - 1) / kCensusTileH;
+    int t = blockIdx.x - pr.census_tile_begin;
+    const int view = t / (tiles_x * tiles_y);  // 0 = left, 1 = right
+    t -= view * tiles_x * tiles_y;
+    const int bx = (t % tiles_x) * kCensusTileW;
+    const int by = (t / tiles_x) * kCensusTileH;
+    const uint8_t* img = view ? pr.right : pr.left;
+    const size_t pitch = view ? pr.right_pitch : pr.left_pitch;
+
+    const int sw = kCensusTileW + 2 * rx, sh = kCensusTileH + 2 * ry;
+    const int tid = threadIdx.y * kCensusTileW + threadIdx.x;
+    for (int i = tid; i < sw * sh; i += kCensusTileW * kCensusTileH) {
+        const int sx = min(max(bx - rx + i % sw, 0), W - 1);
+        const int sy = min(max(by - ry + i / sw, 0), H - 1);
+        tile_px[i] = img[(size_t)sy * pitch + sx];
+    }
+    __syncthreads();
+
+    const int x = bx + threadIdx.x, y = by + threadIdx.y;
+    if (x >= W || y >= H) return;
+    // Clamped reads at the image border equal reads of the staged apron, which
+    // was filled with clamped coordinates; interior threads read their window.
+    const int cx = threadIdx.x + rx, cy = threadIdx.y + ry;
+    const int c = tile_px[cy * sw + cx];
+    uint64_t bits = 0;
+    int b = 0;
+    for (int dy = -ry; dy <= ry; ++dy) {
+        const uint8_t* row = tile_px + (cy + dy) * sw + cx;
+        for (int dx = -rx; dx <= rx; ++dx) {
+            if (dx == 0 && dy == 0) continue;
+            bits |= (uint64_t)(row[dx] < c) << b;
+            ++b;
+        }
+    }
+    CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
+    CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
+    rm[(size_t)y * W + x] = (CT)bits;
+    cm[(size_t)x * H + y] = (CT)bits;
+}
+
+}  // namespace
+
+cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
+                          int max_ry, bool census64, cudaStream_t stream) {
+    if (total_tiles == 0) return cudaSuccess;
+    const dim3 block(kCensusTileW, kCensusTileH);
+    const size_t smem = (size_t)(kCensusTileW + 2 * max_rx) * (kCensusTileH + 2 * max_ry);
+    count_launch();
+    if (census64)
+        census_kernel<uint64_t><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+    else
+        census_kernel<uint32_t><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+    return cudaGetLastError();
+}
+
+}  // namespace vxsgm

@@ -1,0 +1,58 @@
+// Device-side descriptors shared by the SGM kernels and their host launchers.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace vxsgm {
+
+// One stereo pair of a launch, as the kernels see it. Built on the host by the
+// planner (plan.cpp) and copied into the launch's workspace.
+struct PairDev {
+    const uint8_t* left;   // U8 images, row pitch in bytes
+    const uint8_t* right;
+    size_t left_pitch, right_pitch;
+    void* census_l;        // W*H census words, row-major (y*W + x)
+    void* census_r;
+    void* census_lt;       // W*H census words, column-major (x*H + y)
+    void* census_rt;
+    uint16_t* slabs;       // num_paths slabs of H*W*Dp u16 (pixel-major, d-minor)
+    size_t slab_stride;    // elements per slab = H*W*Dp
+    float* out_f32;        // subpixel (or integer) disparity, pitch in bytes
+    size_t out_f32_pitch;
+    int16_t* out_i16;      // optional integer disparity, pitch in bytes
+    size_t out_i16_pitch;
+    int width, height;
+    int nd;                // number of disparities D (1..256)
+    int nd_pad;            // Dp = D rounded up to 8
+    int num_paths;
+    int p1, p2;            // ushort(p1), ushort(p2)
+    int rx, ry;            // census radii
+    int subpixel, lr_check, lr_tolerance;
+    float invalid_value;
+    int census_tile_begin; // first census tile of this pair (census launch)
+    int row_begin;         // first WTA row of this pair (WTA launch)
+};
+
+// One aggregation job: one path direction of one pair.
+struct JobDev {
+    int pair;
+    int path;              // slab index within the pair
+    int dx, dy;            // unit step of the path
+    int num_scanlines;     // H (horizontal), W (vertical), W+H-1 (diagonal)
+    int k_min;             // scanline index offset (diagonals with dx = +1 start at -(H-1))
+};
+
+// A warp's unit of aggregation work: 32 consecutive scanlines of one job.
+struct UnitDev {
+    int job;
+    int first_scanline;
+};
+
+constexpr int kCensusTileW = 32;
+constexpr int kCensusTileH = 8;
+constexpr int kAggWarpsPerBlock = 4;
+constexpr int kWtaThreads = 256;
+// Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).
+constexpr int kMaxWidth = 16384;
+
+}  // namespace vxsgm

@@ -1,0 +1,253 @@
+// Batch planner: validates pairs, lays out the workspace, builds the work
+// queue of (pair, path, scanline-group) units and issues the launches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "vx_internal.hpp"
+
+namespace vxsgm {
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+// Path directions in slab order; the first two are the reference's
+// (vx-vision/src/kernels/sgm.rs:197-200), the rest are the 4/8-path extension.
+const int kDirs[8][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+
+int pick_dmax(int nd, bool* exact) {
+    for (int v : {64, 128, 192, 256})
+        if (nd == v) {
+            *exact = true;
+            return v;
+        }
+    *exact = false;
+    for (int v : {64, 128, 256})
+        if (nd <= v) return v;
+    return 0;
+}
+
+}  // namespace
+
+int census_bits(const vx_sgm_config& cfg) {
+    return (int)((2 * cfg.census_radius_x + 1) * (2 * cfg.census_radius_y + 1)) - 1;
+}
+
+vx_status validate_pair(const PairSpec& p) {
+    if (!p.left || !p.right || !p.out_f32)
+        return fail(VX_ERR_INVALID_ARGUMENT, "left, right and output images are required");
+    if (p.left->format != VX_FORMAT_U8 || p.right->format != VX_FORMAT_U8)
+        return fail(VX_ERR_INVALID_ARGUMENT, "input images must be U8");
+    if (p.out_f32->format != VX_FORMAT_F32)
+        return fail(VX_ERR_INVALID_ARGUMENT, "output image must be F32");
+    if (p.out_i16 && p.out_i16->format != VX_FORMAT_I16)
+        return fail(VX_ERR_INVALID_ARGUMENT, "integer output image must be I16");
+    const uint32_t w = p.left->width, h = p.left->height;
+    if (p.right->width != w || p.right->height != h || p.out_f32->width != w ||
+        p.out_f32->height != h || (p.out_i16 && (p.out_i16->width != w || p.out_i16->height != h)))
+        return fail(VX_ERR_SIZE_MISMATCH, "texture size mismatch");
+    if (w > (uint32_t)kMaxWidth)
+        return fail(VX_ERR_INVALID_CONFIG, "image width %u exceeds %d", w, kMaxWidth);
+    const vx_sgm_config& c = p.cfg;
+    if (c.num_disparities < 1 || c.num_disparities > 256)
+        return fail(VX_ERR_INVALID_CONFIG, "num_disparities %u not in 1..256", c.num_disparities);
+    if (!(c.p1 >= 0.0f && c.p1 < 65536.0f) || !(c.p2 >= 0.0f && c.p2 < 65536.0f))
+        return fail(VX_ERR_INVALID_CONFIG, "p1/p2 must be in [0, 65536)");
+    if (c.census_radius_x > 31 || c.census_radius_y > 31 || census_bits(c) > 64)
+        return fail(VX_ERR_INVALID_CONFIG, "census window %ux%u exceeds 64 bits",
+                    2 * c.census_radius_x + 1, 2 * c.census_radius_y + 1);
+    if (c.num_paths != 2 && c.num_paths != 4 && c.num_paths != 8)
+        return fail(VX_ERR_INVALID_CONFIG, "num_paths must be 2, 4 or 8");
+    return VX_OK;
+}
+
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
+    Plan& pl = *plan;
+    pl = Plan{};
+    const int n = (int)specs.size();
+    for (const auto& s : specs) {
+        vx_status st = validate_pair(s);
+        if (st != VX_OK) return st;
+        if (census_bits(s.cfg) > 32) pl.census64 = true;
+    }
+    const size_t ct = pl.census64 ? 8 : 4;
+
+    pl.pairs.resize(n);
+    pl.pair_data_off.resize(n);
+    size_t data = 0;
+    int tiles = 0, rows = 0;
+    std::vector<std::vector<UnitDev>> group_units;
+    for (int i = 0; i < n; ++i) {
+        const PairSpec& s = specs[i];
+        const vx_sgm_config& c = s.cfg;
+        const int W = (int)s.left->width, H = (int)s.left->height;
+        const int D = (int)c.num_disparities, Dp = (D + 7) / 8 * 8, P = (int)c.num_paths;
+        PairDev& pd = pl.pairs[i];
+        std::memset(&pd, 0, sizeof pd);
+        pd.left = static_cast<const uint8_t*>(s.left->ptr);
+        pd.right = static_cast<const uint8_t*>(s.right->ptr);
+        pd.left_pitch = s.left->pitch;
+        pd.right_pitch = s.right->pitch;
+        pd.out_f32 = static_cast<float*>(s.out_f32->ptr);
+        pd.out_f32_pitch = s.out_f32->pitch;
+        pd.out_i16 = s.out_i16 ? static_cast<int16_t*>(s.out_i16->ptr) : nullptr;
+        pd.out_i16_pitch = s.out_i16 ? s.out_i16->pitch : 0;
+        pd.width = W;
+        pd.height = H;
+        pd.nd = D;
+        pd.nd_pad = Dp;
+        pd.num_paths = P;
+        pd.p1 = (int)(uint16_t)c.p1;  // ushort(params.p1), SGMStereo.metal:155
+        pd.p2 = (int)(uint16_t)c.p2;
+        pd.rx = (int)c.census_radius_x;
+        pd.ry = (int)c.census_radius_y;
+        pd.subpixel = c.subpixel ? 1 : 0;
+        pd.lr_check = c.lr_check ? 1 : 0;
+        pd.lr_tolerance = (int)c.lr_tolerance;
+        pd.invalid_value = c.invalid_value;
+        pd.census_tile_begin = tiles;
+        pd.row_begin = rows;
+        tiles += 2 * ((W + kCensusTileW - 1) / kCensusTileW) * ((H + kCensusTileH - 1) / kCensusTileH);
+        rows += H;
+        pl.max_width = std::max(pl.max_width, W);
+        pl.max_rx = std::max(pl.max_rx, pd.rx);
+        pl.max_ry = std::max(pl.max_ry, pd.ry);
+
+        // Workspace-relative data: 4 census planes then P slabs.
+        const size_t npx = (size_t)W * H;
+        pl.pair_data_off[i] = data;
+        const size_t cplane = align_up(npx * ct);
+        pd.census_l = reinterpret_cast<void*>(data);
+        pd.census_r = reinterpret_cast<void*>(data + cplane);
+        pd.census_lt = reinterpret_cast<void*>(data + 2 * cplane);
+        pd.census_rt = reinterpret_cast<void*>(data + 3 * cplane);
+        data += 4 * cplane;
+        pd.slab_stride = npx * (size_t)Dp;
+        pd.slabs = reinterpret_cast<uint16_t*>(data);
+        data += align_up(pd.slab_stride * P * sizeof(uint16_t));
+
+        bool exact = false;
+        const int dmax = pick_dmax(D, &exact);
+        for (int p = 0; p < P; ++p) {
+            JobDev j{};
+            j.pair = i;
+            j.path = p;
+            j.dx = kDirs[p][0];
+            j.dy = kDirs[p][1];
+            const bool horiz = j.dy == 0;
+            j.num_scanlines = horiz ? H : (j.dx == 0 ? W : W + H - 1);
+            j.k_min = (j.dx > 0 && j.dy != 0) ? -(H - 1) : 0;
+            const int job = (int)pl.jobs.size();
+            pl.jobs.push_back(j);
+            AggVariant v{dmax, exact, pl.census64, horiz};
+            int g = 0;
+            while (g < (int)pl.groups.size() && !(pl.groups[g].variant == v)) ++g;
+            if (g == (int)pl.groups.size()) {
+                pl.groups.push_back({v, 0, 0});
+                group_units.emplace_back();
+            }
+            for (int k = 0; k < j.num_scanlines; k += 32) group_units[g].push_back({job, k});
+        }
+    }
+    pl.total_tiles = tiles;
+    pl.total_rows = rows;
+
+    // Longest work first inside each persistent launch (LPT order): a unit's
+    // cost is its longest scanline times D.
+    auto unit_cost = [&](const UnitDev& u) -> long long {
+        const JobDev& j = pl.jobs[u.job];
+        const PairDev& p = pl.pairs[j.pair];
+        long long len;
+        if (j.dy == 0) len = p.width;
+        else if (j.dx == 0) len = p.height;
+        else {  // longest of the unit's 32 diagonals
+            len = 0;
+            const int k0 = j.k_min + u.first_scanline;
+            const int k1 = j.k_min + std::min(u.first_scanline + 32, j.num_scanlines);
+            for (int k = k0; k < k1; ++k) {
+                int tb, te;
+                if (j.dx > 0) { tb = std::max(0, -k); te = std::min(p.height, p.width - k); }
+                else { tb = std::max(0, k - p.width + 1); te = std::min(p.height, k + 1); }
+                len = std::max<long long>(len, te - tb);
+            }
+        }
+        return len * p.nd;
+    };
+    for (size_t g = 0; g < pl.groups.size(); ++g) {
+        auto& us = group_units[g];
+        std::vector<std::pair<long long, int>> order(us.size());
+        for (size_t i = 0; i < us.size(); ++i) order[i] = {-unit_cost(us[i]), (int)i};
+        std::sort(order.begin(), order.end());
+        std::vector<UnitDev> sorted(us.size());
+        for (size_t i = 0; i < us.size(); ++i) sorted[i] = us[order[i].second];
+        us.swap(sorted);
+        pl.groups[g].unit_begin = (int)pl.units.size();
+        pl.groups[g].unit_count = (int)us.size();
+        pl.units.insert(pl.units.end(), us.begin(), us.end());
+    }
+
+    size_t off = 0;
+    pl.off_pairs = off;
+    off = align_up(off + pl.pairs.size() * sizeof(PairDev));
+    pl.off_jobs = off;
+    off = align_up(off + pl.jobs.size() * sizeof(JobDev));
+    pl.off_units = off;
+    off = align_up(off + pl.units.size() * sizeof(UnitDev));
+    pl.off_counters = off;
+    off = align_up(off + pl.groups.size() * sizeof(unsigned));
+    pl.off_data = off;
+    pl.ws_bytes = off + data;
+    return VX_OK;
+}
+
+void bind_plan(Plan& pl, char* base) {
+    char* data = base + pl.off_data;
+    for (auto& pd : pl.pairs) {
+        pd.census_l = data + reinterpret_cast<size_t>(pd.census_l);
+        pd.census_r = data + reinterpret_cast<size_t>(pd.census_r);
+        pd.census_lt = data + reinterpret_cast<size_t>(pd.census_lt);
+        pd.census_rt = data + reinterpret_cast<size_t>(pd.census_rt);
+        pd.slabs = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.slabs));
+    }
+}
+
+vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev) {
+    const int n = (int)pl.pairs.size();
+    if (n == 0) return VX_OK;
+    cudaError_t e = cudaMemcpyAsync(base + pl.off_pairs, pl.pairs.data(), n * sizeof(PairDev),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + pl.off_jobs, pl.jobs.data(), pl.jobs.size() * sizeof(JobDev),
+                            cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && !pl.units.empty())
+        e = cudaMemcpyAsync(base + pl.off_units, pl.units.data(), pl.units.size() * sizeof(UnitDev),
+                            cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(base + pl.off_counters, 0, pl.groups.size() * sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "uploading the batch plan");
+
+    const PairDev* d_pairs = reinterpret_cast<const PairDev*>(base + pl.off_pairs);
+    const JobDev* d_jobs = reinterpret_cast<const JobDev*>(base + pl.off_jobs);
+    const UnitDev* d_units = reinterpret_cast<const UnitDev*>(base + pl.off_units);
+    unsigned* counters = reinterpret_cast<unsigned*>(base + pl.off_counters);
+
+    if (ev) cudaEventRecord(ev[0], stream);
+    e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "census launch");
+    if (ev) cudaEventRecord(ev[1], stream);
+    for (size_t g = 0; g < pl.groups.size(); ++g) {
+        const auto& gr = pl.groups[g];
+        e = launch_aggregate(gr.variant, d_pairs, d_jobs, d_units + gr.unit_begin, gr.unit_count,
+                             counters + g, 0, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
+    }
+    if (ev) cudaEventRecord(ev[2], stream);
+    e = launch_wta(d_pairs, n, pl.total_rows, pl.max_width, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "WTA launch");
+    if (ev) cudaEventRecord(ev[3], stream);
+    return VX_OK;
+}
+
+}  // namespace vxsgm

@@ -1,0 +1,173 @@
+// SGMStereo entry points of the vx_sgm C ABI (vx-vision/src/kernels/sgm.rs).
+#include <cstring>
+#include <vector>
+
+#include "vx_internal.hpp"
+
+using namespace vxsgm;
+
+namespace {
+
+// Runs a batch; if keep_ws is non-null the workspace is handed back to the
+// caller (who must free it with cudaFreeAsync) instead of being released.
+vx_status run_batch(vx_ctx* ctx, const std::vector<PairSpec>& specs, cudaStream_t stream,
+                    bool synchronous, char** keep_ws, Plan* plan_out) {
+    Plan plan;
+    vx_status st = build_plan(specs, &plan);
+    if (st != VX_OK) return st;
+    if (specs.empty()) return VX_OK;
+    DeviceGuard g(ctx->device);
+    char* ws = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool, stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
+    }
+    bind_plan(plan, ws);
+    st = run_plan(plan, ws, stream, ctx->next_timing_slot());
+    if (keep_ws && st == VX_OK) {
+        *keep_ws = ws;
+    } else {
+        cudaFreeAsync(ws, stream);
+    }
+    if (st == VX_OK && synchronous) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "SGM execution");
+    }
+    if (plan_out) *plan_out = std::move(plan);
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+void vx_sgm_config_default(vx_sgm_config* cfg) {
+    if (!cfg) return;
+    // SGMStereoConfig::default(), vx-vision/src/kernels/sgm.rs:39-49.
+    cfg->num_disparities = 128;
+    cfg->p1 = 10.0f;
+    cfg->p2 = 120.0f;
+    cfg->census_radius_x = 4;
+    cfg->census_radius_y = 3;
+    // Extensions, defaulting to the reference's behaviour.
+    cfg->num_paths = 2;
+    cfg->subpixel = 1;
+    cfg->lr_check = 0;
+    cfg->lr_tolerance = 1;
+    cfg->invalid_value = -1.0f;
+}
+
+void vx_sgm_config_new(vx_sgm_config* cfg, uint32_t num_disparities) {
+    vx_sgm_config_default(cfg);
+    if (cfg) cfg->num_disparities = num_disparities;
+}
+
+vx_status vx_sgm_create(vx_ctx* ctx, vx_sgm** out) {
+    if (!ctx || !out) return fail(VX_ERR_INVALID_ARGUMENT, "vx_sgm_create: NULL argument");
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    // The reference resolves and compiles its three pipelines here
+    // (sgm.rs:73-105); the equivalent check is that this library's sm_100a
+    // kernel images load on the device.
+    cudaError_t e = prepare_wta_kernel();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(VX_ERR_SHADER_MISSING, "SGM kernels unavailable on device %d: %s", ctx->device,
+                    cudaGetErrorString(e));
+    }
+    AggVariant probe{128, true, false, false};
+    if (aggregate_grid_ctas(probe) <= 0) {
+        cudaGetLastError();
+        return fail(VX_ERR_PIPELINE_COMPILE, "aggregation kernel has no occupancy on device %d",
+                    ctx->device);
+    }
+    auto* s = new vx_sgm;
+    s->ctx = ctx;
+    *out = s;
+    return VX_OK;
+}
+
+void vx_sgm_destroy(vx_sgm* sgm) { delete sgm; }
+
+vx_status vx_sgm_compute_disparity(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left,
+                                   const vx_image* right, vx_image* out_f32, vx_image* out_i16,
+                                   const vx_sgm_config* cfg, vx_stream stream) {
+    if (!sgm || !ctx || !cfg) return fail(VX_ERR_INVALID_ARGUMENT, "compute_disparity: NULL argument");
+    std::vector<PairSpec> specs{{left, right, out_f32, out_i16, *cfg}};
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return run_batch(ctx, specs, s, stream == nullptr, nullptr, nullptr);
+}
+
+vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
+                               const vx_image* const* right, vx_image* const* out_f32,
+                               vx_image* const* out_i16, const vx_sgm_config* cfgs,
+                               vx_stream stream) {
+    if (!sgm || !ctx || (n && (!left || !right || !out_f32 || !cfgs)))
+        return fail(VX_ERR_INVALID_ARGUMENT, "compute_batch: NULL argument");
+    std::vector<PairSpec> specs(n);
+    for (uint32_t i = 0; i < n; ++i)
+        specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return run_batch(ctx, specs, s, stream == nullptr, nullptr, nullptr);
+}
+
+size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg) {
+    if (!cfg) return 0;
+    const size_t npx = (size_t)width * height;
+    const size_t ct = census_bits(*cfg) > 32 ? 8 : 4;
+    const size_t dp = (cfg->num_disparities + 7) / 8 * 8;
+    auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+    return 4 * al(npx * ct) + al(npx * dp * cfg->num_paths * sizeof(uint16_t));
+}
+
+vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,
+                            const vx_sgm_config* cfg, uint64_t* census_left,
+                            uint64_t* census_right, uint16_t* path_costs, uint16_t* cost_volume) {
+    if (!sgm || !ctx || !left || !cfg) return fail(VX_ERR_INVALID_ARGUMENT, "debug_dump: NULL argument");
+    DeviceGuard g(ctx->device);
+    vx_image* out = nullptr;
+    vx_status st = vx_image_create(ctx, left->width, left->height, VX_FORMAT_F32, &out);
+    if (st != VX_OK) return st;
+    std::vector<PairSpec> specs{{left, right, out, nullptr, *cfg}};
+    char* ws = nullptr;
+    Plan plan;
+    st = run_batch(ctx, specs, ctx->stream, true, &ws, &plan);
+    if (st == VX_OK) {
+        const PairDev& pd = plan.pairs[0];
+        const size_t W = pd.width, H = pd.height, D = pd.nd, Dp = pd.nd_pad, P = pd.num_paths;
+        const size_t npx = W * H;
+        const size_t ct = plan.census64 ? 8 : 4;
+        std::vector<uint8_t> cbuf(npx * ct);
+        auto fetch_census = [&](const void* src, uint64_t* dst) {
+            cudaMemcpy(cbuf.data(), src, npx * ct, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < npx; ++i) {
+                uint64_t v = 0;
+                std::memcpy(&v, cbuf.data() + i * ct, ct);
+                dst[i] = v;
+            }
+        };
+        if (census_left) fetch_census(pd.census_l, census_left);
+        if (census_right) fetch_census(pd.census_r, census_right);
+        if (path_costs || cost_volume) {
+            std::vector<uint16_t> slabs(pd.slab_stride * P);
+            cudaMemcpy(slabs.data(), pd.slabs, slabs.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+            if (cost_volume) std::memset(cost_volume, 0, npx * D * sizeof(uint16_t));
+            for (size_t p = 0; p < P; ++p)
+                for (size_t i = 0; i < npx; ++i)
+                    for (size_t d = 0; d < D; ++d) {
+                        const uint16_t v = slabs[p * pd.slab_stride + i * Dp + d];
+                        if (path_costs) path_costs[(p * npx + i) * D + d] = v;
+                        if (cost_volume) cost_volume[i * D + d] = (uint16_t)(cost_volume[i * D + d] + v);
+                    }
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "debug dump copy");
+        cudaFreeAsync(ws, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    vx_image_destroy(out);
+    return st;
+}
+
+}  // extern "C"

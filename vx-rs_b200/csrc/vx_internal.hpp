@@ -1,0 +1,114 @@
+// Internal host-side definitions of the vx_sgm C ABI implementation.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vx_sgm.h"
+#include "kernels.cuh"
+#include "launch.hpp"
+
+// The reference's Context (vx-vision/src/context.rs:17): device + queue.
+// Here: a CUDA device, one stream and a stream-ordered memory pool whose
+// release threshold keeps freed blocks cached, so steady-state calls do not
+// reach the driver allocator.
+struct vx_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    // Stage timing: per batch, 4 events bracket census | aggregation | WTA.
+    // Batches since the last enable take consecutive slots of the ring.
+    static constexpr int kTimingSlots = 256;
+    bool timing = false;
+    int timing_batches = 0;
+    std::vector<cudaEvent_t> stage_ev;  // kTimingSlots * 4 when enabled
+    std::mutex timing_mu;
+    cudaEvent_t* next_timing_slot();
+};
+
+// The reference's Texture (vx-vision/src/texture.rs:29): a pitched 2D plane.
+struct vx_image {
+    vx_ctx* ctx = nullptr;
+    void* ptr = nullptr;
+    size_t pitch = 0;  // bytes
+    uint32_t width = 0, height = 0;
+    vx_format format = VX_FORMAT_U8;
+    bool owned = false;
+};
+
+// The reference's SGMStereo (vx-vision/src/kernels/sgm.rs:62).
+struct vx_sgm {
+    vx_ctx* ctx = nullptr;
+};
+
+namespace vxsgm {
+
+// Records a message for vx_last_error() on this host thread and returns status.
+vx_status fail(vx_status status, const char* fmt, ...);
+vx_status cuda_fail(cudaError_t err, const char* what);
+
+// Makes ctx->device current for the scope of a call.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int device) {
+        cudaGetDevice(&prev_);
+        if (prev_ != device) cudaSetDevice(device);
+        restore_ = prev_ != device;
+    }
+    ~DeviceGuard() {
+        if (restore_) cudaSetDevice(prev_);
+    }
+
+  private:
+    int prev_ = 0;
+    bool restore_ = false;
+};
+
+size_t format_bytes(vx_format f);
+
+// Validated description of one pair of a batch.
+struct PairSpec {
+    const vx_image* left;
+    const vx_image* right;
+    vx_image* out_f32;
+    vx_image* out_i16;
+    vx_sgm_config cfg;
+};
+
+vx_status validate_pair(const PairSpec& p);
+int census_bits(const vx_sgm_config& cfg);
+
+// Host-side plan of one batched launch sequence (planner.cpp).
+struct Plan {
+    std::vector<PairDev> pairs;     // pointers relative to the workspace base until bound
+    std::vector<JobDev> jobs;
+    std::vector<UnitDev> units;     // all groups, concatenated
+    struct Group {
+        AggVariant variant;
+        int unit_begin, unit_count;
+    };
+    std::vector<Group> groups;
+    bool census64 = false;
+    int total_tiles = 0, total_rows = 0, max_width = 0, max_rx = 0, max_ry = 0;
+    // Workspace layout (byte offsets from the workspace base).
+    size_t off_pairs = 0, off_jobs = 0, off_units = 0, off_counters = 0, off_data = 0;
+    size_t ws_bytes = 0;
+    std::vector<size_t> pair_data_off;  // per pair: census + slabs
+};
+
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan);
+// Resolves the workspace-relative pointers of plan.pairs against `base`.
+void bind_plan(Plan& plan, char* base);
+// Issues the whole batch (census, aggregation, WTA) on `stream` with the
+// workspace at `base` (plan must be bound to it).
+// stage_events: null, or 4 events recorded before census, before aggregation,
+// before WTA and after WTA.
+vx_status run_plan(const Plan& plan, char* base, cudaStream_t stream,
+                   cudaEvent_t* stage_events = nullptr);
+
+}  // namespace vxsgm

@@ -1,0 +1,153 @@
+// Winner-take-all, parabola subpixel refinement and left-right check, fused
+// with the sum of the per-path slabs. One CTA per (pair, image row).
+//
+// Semantics (vx-vision/shaders/SGMStereo.metal:179-214):
+//   S(d)   = sum over paths of L_r(d), modulo 2^16 (the shader's ushort +=)
+//   best_d = first minimum of S over d (strict '<' from 0xFFFF)
+//   disp   = best_d + (c0 - c2) / (2 (c0 + c2 - 2 c1)) when 0 < best_d < D-1 and
+//            the denominator is non-zero, with c0,c1,c2 = S(best_d-1..best_d+1)
+//            (IEEE single precision, correctly rounded division).
+// Extension: right-view WTA dR(x') = first minimum over d of S(x'+d, d) with
+// x'+d < W; a pixel is invalid when x - dL < 0 or |dL - dR(x - dL)| > tol.
+//
+// Mapping: lanes span disparities (8 per lane = one 16-byte chunk of a u16 slab
+// row) so slab reads are coalesced; a warp covers 32/seg pixels at once. The
+// argmin is a min over the key (S << 8 | d), which orders by cost then by d,
+// i.e. the first minimum. The right-view argmin of the row is accumulated in
+// shared memory with atomicMin on the same keys.
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+#include "launch.hpp"
+
+namespace vxsgm {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int find_pair_by_row(const PairDev* pairs, int n, int row) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].row_begin <= row) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kWtaThreads)
+wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
+    extern __shared__ uint32_t smem[];
+    const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
+    const PairDev& pr = pairs[pi];
+    const int y = blockIdx.x - pr.row_begin;
+    const int W = pr.width, D = pr.nd, Dp = pr.nd_pad, P = pr.num_paths;
+    const bool lr = pr.lr_check != 0;
+
+    uint32_t* right_key = smem;                               // W keys (LR only)
+    int* best_d = reinterpret_cast<int*>(smem + W);           // W
+    float* disp = reinterpret_cast<float*>(smem + 2 * W);     // W
+
+    if (lr)
+        for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
+    __syncthreads();
+
+    const int chunks = Dp / 8;                      // 16-byte chunks per pixel
+    int seg = 1;
+    while (seg < chunks) seg <<= 1;                 // lanes per pixel (power of two)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int sub = lane / seg, c = lane % seg;
+    const int ppw = 32 / seg;
+
+    for (int xb = warp * ppw; xb < W; xb += nwarps * ppw) {
+        const int x = xb + sub;
+        const bool act = x < W && c < chunks;
+        uint32_t s[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] = 0;
+        if (act) {
+            const size_t off = ((size_t)y * W + x) * Dp + 8 * c;
+            for (int p = 0; p < P; ++p) {
+                const uint4 v = *reinterpret_cast<const uint4*>(pr.slabs + pr.slab_stride * p + off);
+                s[0] += v.x & 0xFFFFu; s[1] += v.x >> 16;
+                s[2] += v.y & 0xFFFFu; s[3] += v.y >> 16;
+                s[4] += v.z & 0xFFFFu; s[5] += v.z >> 16;
+                s[6] += v.w & 0xFFFFu; s[7] += v.w >> 16;
+            }
+        }
+        uint32_t best = 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            s[j] &= 0xFFFFu;
+            const int d = 8 * c + j;
+            if (act && d < D) best = min(best, (s[j] << 8) | (uint32_t)d);
+        }
+        for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
+        const int bd = (int)(best & 0xFFu);
+        uint32_t c0 = 0, c2 = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int d = 8 * c + j;
+            if (act && d == bd - 1) c0 = s[j];
+            if (act && d == bd + 1 && d < D) c2 = s[j];
+        }
+        for (int o = seg >> 1; o > 0; o >>= 1) {
+            c0 |= __shfl_xor_sync(kFull, c0, o);
+            c2 |= __shfl_xor_sync(kFull, c2, o);
+        }
+        if (lr && act) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int d = 8 * c + j;
+                if (d < D && x - d >= 0) atomicMin(&right_key[x - d], (s[j] << 8) | (uint32_t)d);
+            }
+        }
+        if (c == 0 && x < W) {
+            float v = (float)bd;
+            if (pr.subpixel && bd > 0 && bd < D - 1) {
+                const float f0 = (float)c0, f1 = (float)(best >> 8), f2 = (float)c2;
+                const float denom = 2.0f * (f0 + f2 - 2.0f * f1);
+                if (fabsf(denom) > 1e-6f) v = __fadd_rn(v, __fdiv_rn(f0 - f2, denom));
+            }
+            best_d[x] = bd;
+            disp[x] = v;
+        }
+    }
+    __syncthreads();
+
+    float* out = reinterpret_cast<float*>(reinterpret_cast<char*>(pr.out_f32) + (size_t)y * pr.out_f32_pitch);
+    int16_t* out_i = pr.out_i16
+        ? reinterpret_cast<int16_t*>(reinterpret_cast<char*>(pr.out_i16) + (size_t)y * pr.out_i16_pitch)
+        : nullptr;
+    for (int x = threadIdx.x; x < W; x += blockDim.x) {
+        const int dl = best_d[x];
+        bool valid = true;
+        if (lr) {
+            const int xr = x - dl;
+            valid = xr >= 0 && abs(dl - (int)(right_key[xr] & 0xFFu)) <= pr.lr_tolerance;
+        }
+        out[x] = valid ? disp[x] : pr.invalid_value;
+        if (out_i) out_i[x] = (int16_t)(valid ? dl : -1);
+    }
+}
+
+}  // namespace
+
+size_t wta_smem_bytes(int max_width) { return (size_t)max_width * 3 * sizeof(uint32_t); }
+
+cudaError_t prepare_wta_kernel() {
+    return cudaFuncSetAttribute(wta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)wta_smem_bytes(kMaxWidth));
+}
+
+cudaError_t launch_wta(const PairDev* d_pairs, int num_pairs, int total_rows, int max_width,
+                       cudaStream_t stream) {
+    if (total_rows == 0) return cudaSuccess;
+    const size_t smem = wta_smem_bytes(max_width);
+    count_launch();
+    wta_kernel<<<total_rows, kWtaThreads, smem, stream>>>(d_pairs, num_pairs);
+    return cudaGetLastError();
+}
+
+}  // namespace vxsgm

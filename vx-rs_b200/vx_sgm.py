@@ -1,0 +1,340 @@
+"""Python binding of the B200 SGM stereo library (ctypes over include/vx_sgm.h).
+
+Mirrors vx-vision's SGM API (MisterEkole/vx-rs):
+
+    ctx = Context()                                  # Context::new()         context.rs:26
+    sgm = SGMStereo(ctx)                             # SGMStereo::new(&ctx)   kernels/sgm.rs:73
+    left = ctx.texture_gray8(l, w, h)                # Context::texture_gray8 context.rs:39
+    out = ctx.texture_output_r32float(w, h)          # context.rs:64
+    sgm.compute_disparity(ctx, left, right, out, SGMStereoConfig.new(64))   # sgm.rs:108
+    disp = out.read_r32float()                       # Texture::read_r32float texture.rs:404
+
+Errors raise VxError carrying the C status (the reference's Error variants,
+vx-vision/src/error.rs:8-23). The CUDA library is required: importing this
+module fails loudly if libvx_sgm.so is missing or does not load.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvx_sgm.so")
+SYNTH_PATH = os.path.join(_HERE, "libvx_synth.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}` "
+                      "(or __graft_entry__.build())")
+_lib = ctypes.CDLL(LIB_PATH)
+
+_P = ctypes.c_void_p
+
+VX_OK = 0
+STATUS_NAMES = {
+    0: "VX_OK", 1: "VX_ERR_DEVICE_NOT_FOUND", 2: "VX_ERR_SHADER_MISSING",
+    3: "VX_ERR_PIPELINE_COMPILE", 4: "VX_ERR_BUFFER_ALLOC", 5: "VX_ERR_SIZE_MISMATCH",
+    6: "VX_ERR_INVALID_CONFIG", 7: "VX_ERR_GPU", 8: "VX_ERR_BUDGET", 9: "VX_ERR_TIMEOUT",
+    10: "VX_ERR_INVALID_ARGUMENT", 11: "VX_ERR_NOT_READY", 12: "VX_ERR_CANCELLED",
+}
+FORMAT_U8, FORMAT_F32, FORMAT_I16 = 0, 1, 2
+_FORMAT_DTYPE = {FORMAT_U8: np.uint8, FORMAT_F32: np.float32, FORMAT_I16: np.int16}
+
+
+class VxError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class _CConfig(ctypes.Structure):
+    _fields_ = [("num_disparities", ctypes.c_uint32), ("p1", ctypes.c_float),
+                ("p2", ctypes.c_float), ("census_radius_x", ctypes.c_uint32),
+                ("census_radius_y", ctypes.c_uint32), ("num_paths", ctypes.c_uint32),
+                ("subpixel", ctypes.c_uint32), ("lr_check", ctypes.c_uint32),
+                ("lr_tolerance", ctypes.c_uint32), ("invalid_value", ctypes.c_float)]
+
+
+def _sig(name, restype, *argtypes):
+    fn = getattr(_lib, name)
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+    return fn
+
+
+_last_error = _sig("vx_last_error", ctypes.c_char_p)
+_launch_count = _sig("vx_kernel_launch_count", ctypes.c_uint64)
+_ctx_create = _sig("vx_ctx_create", ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P))
+_ctx_destroy = _sig("vx_ctx_destroy", None, _P)
+_ctx_stream = _sig("vx_ctx_stream", _P, _P)
+_ctx_sync = _sig("vx_ctx_synchronize", ctypes.c_int, _P)
+_ctx_timing = _sig("vx_ctx_enable_stage_timing", ctypes.c_int, _P, ctypes.c_int)
+_ctx_times = _sig("vx_ctx_stage_times", ctypes.c_int, _P, ctypes.POINTER(ctypes.c_float),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float))
+_img_create = _sig("vx_image_create", ctypes.c_int, _P, ctypes.c_uint32, ctypes.c_uint32,
+                   ctypes.c_int, ctypes.POINTER(_P))
+_img_wrap = _sig("vx_image_wrap_device", ctypes.c_int, _P, _P, ctypes.c_size_t, ctypes.c_uint32,
+                 ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(_P))
+_img_destroy = _sig("vx_image_destroy", None, _P)
+_img_upload = _sig("vx_image_upload", ctypes.c_int, _P, _P, ctypes.c_size_t, _P)
+_img_download = _sig("vx_image_download", ctypes.c_int, _P, _P, ctypes.c_size_t, _P)
+_img_ptr = _sig("vx_image_device_ptr", _P, _P)
+_img_pitch = _sig("vx_image_pitch", ctypes.c_size_t, _P)
+_cfg_default = _sig("vx_sgm_config_default", None, ctypes.POINTER(_CConfig))
+_sgm_create = _sig("vx_sgm_create", ctypes.c_int, _P, ctypes.POINTER(_P))
+_sgm_destroy = _sig("vx_sgm_destroy", None, _P)
+_sgm_compute = _sig("vx_sgm_compute_disparity", ctypes.c_int, _P, _P, _P, _P, _P, _P,
+                    ctypes.POINTER(_CConfig), _P)
+_sgm_batch = _sig("vx_sgm_compute_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
+                  ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                  ctypes.POINTER(_CConfig), _P)
+_sgm_ws = _sig("vx_sgm_workspace_bytes", ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
+               ctypes.POINTER(_CConfig))
+_sgm_dump = _sig("vx_sgm_debug_dump", ctypes.c_int, _P, _P, _P, _P, ctypes.POINTER(_CConfig),
+                 _P, _P, _P, _P)
+
+
+def _check(status: int):
+    if status != VX_OK:
+        raise VxError(status, _last_error().decode(errors="replace"))
+
+
+def last_error() -> str:
+    return _last_error().decode(errors="replace")
+
+
+def kernel_launch_count() -> int:
+    """Kernel launches this library has issued since it was loaded."""
+    return int(_launch_count())
+
+
+@dataclass
+class SGMStereoConfig:
+    """vx-vision/src/kernels/sgm.rs:23-59 plus the opt-in extensions."""
+    num_disparities: int = 128
+    p1: float = 10.0
+    p2: float = 120.0
+    census_radius_x: int = 4
+    census_radius_y: int = 3
+    num_paths: int = 2
+    subpixel: bool = True
+    lr_check: bool = False
+    lr_tolerance: int = 1
+    invalid_value: float = -1.0
+
+    @classmethod
+    def new(cls, num_disparities: int) -> "SGMStereoConfig":
+        return cls(num_disparities=num_disparities)
+
+    @classmethod
+    def from_c_default(cls) -> "SGMStereoConfig":
+        c = _CConfig()
+        _cfg_default(ctypes.byref(c))
+        return cls(**{f.name: getattr(c, f.name) for f in fields(cls)})
+
+    def to_c(self) -> _CConfig:
+        return _CConfig(int(self.num_disparities), float(self.p1), float(self.p2),
+                        int(self.census_radius_x), int(self.census_radius_y), int(self.num_paths),
+                        int(bool(self.subpixel)), int(bool(self.lr_check)),
+                        int(self.lr_tolerance), float(self.invalid_value))
+
+
+class Context:
+    """A CUDA device with its stream and stream-ordered memory pool."""
+
+    def __init__(self, device: int = 0):
+        h = _P()
+        _check(_ctx_create(int(device), ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return _ctx_stream(self._h) or 0
+
+    def synchronize(self):
+        _check(_ctx_sync(self._h))
+
+    def enable_stage_timing(self, on: bool = True):
+        _check(_ctx_timing(self._h, int(bool(on))))
+
+    def stage_times(self):
+        """(census_ms, aggregate_ms, wta_ms) of the last batch, from CUDA events."""
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _check(_ctx_times(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self._h:
+            _ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def texture_gray8(self, pixels, width: int, height: int) -> "Texture":
+        t = Texture.create(self, width, height, FORMAT_U8)
+        t.upload(np.asarray(pixels, dtype=np.uint8).reshape(height, width))
+        return t
+
+    def texture_output_r32float(self, width: int, height: int) -> "Texture":
+        return Texture.create(self, width, height, FORMAT_F32)
+
+    def texture_output_i16(self, width: int, height: int) -> "Texture":
+        return Texture.create(self, width, height, FORMAT_I16)
+
+
+class Texture:
+    """A pitched device image (U8 in, F32 / I16 out)."""
+
+    def __init__(self, ctx: Context, handle, width: int, height: int, fmt: int):
+        self.ctx, self._h, self.width, self.height, self.format = ctx, handle, width, height, fmt
+
+    @classmethod
+    def create(cls, ctx: Context, width: int, height: int, fmt: int) -> "Texture":
+        h = _P()
+        _check(_img_create(ctx.handle, width, height, fmt, ctypes.byref(h)))
+        return cls(ctx, h, width, height, fmt)
+
+    @classmethod
+    def wrap_device(cls, ctx: Context, ptr: int, pitch: int, width: int, height: int,
+                    fmt: int) -> "Texture":
+        h = _P()
+        _check(_img_wrap(ctx.handle, _P(ptr), pitch, width, height, fmt, ctypes.byref(h)))
+        return cls(ctx, h, width, height, fmt)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def device_ptr(self) -> int:
+        return _img_ptr(self._h) or 0
+
+    @property
+    def pitch(self) -> int:
+        return int(_img_pitch(self._h))
+
+    def upload(self, host: np.ndarray, stream: int | None = None):
+        a = np.ascontiguousarray(host, dtype=_FORMAT_DTYPE[self.format])
+        assert a.shape == (self.height, self.width), (a.shape, self.height, self.width)
+        _check(_img_upload(self._h, _P(a.ctypes.data), a.strides[0], _P(stream) if stream else None))
+
+    def download(self, host: np.ndarray | None = None, stream: int | None = None) -> np.ndarray:
+        if host is None:
+            host = np.empty((self.height, self.width), dtype=_FORMAT_DTYPE[self.format])
+        _check(_img_download(self._h, _P(host.ctypes.data), host.strides[0],
+                             _P(stream) if stream else None))
+        return host
+
+    def read_r32float(self) -> np.ndarray:
+        assert self.format == FORMAT_F32
+        return self.download()
+
+    def close(self):
+        if self._h:
+            _img_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SGMStereo:
+    """vx-vision's SGMStereo (kernels/sgm.rs:62) on the B200 kernels."""
+
+    def __init__(self, ctx: Context):
+        h = _P()
+        _check(_sgm_create(ctx.handle, ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def new(cls, ctx: Context) -> "SGMStereo":
+        return cls(ctx)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def compute_disparity(self, ctx: Context, left: Texture, right: Texture, output: Texture,
+                          config: SGMStereoConfig, output_i16: Texture | None = None,
+                          stream: int | None = None):
+        c = config.to_c()
+        _check(_sgm_compute(self._h, ctx.handle, left.handle, right.handle, output.handle,
+                            output_i16.handle if output_i16 is not None else None,
+                            ctypes.byref(c), _P(stream) if stream else None))
+
+    def compute_batch(self, ctx: Context, lefts, rights, outputs, configs, outputs_i16=None,
+                      stream: int | None = None):
+        n = len(lefts)
+        arr = lambda ts: (_P * n)(*[t.handle if t is not None else None for t in ts])
+        cfgs = (_CConfig * n)(*[c.to_c() for c in configs])
+        oi = arr(outputs_i16) if outputs_i16 is not None else None
+        _check(_sgm_batch(self._h, ctx.handle, n, arr(lefts), arr(rights), arr(outputs), oi, cfgs,
+                          _P(stream) if stream else None))
+
+    def debug_dump(self, ctx: Context, left: Texture, right: Texture, config: SGMStereoConfig):
+        """Census words, per-path costs L_r and summed cost volume S of one pair."""
+        h, w, d, p = left.height, left.width, config.num_disparities, config.num_paths
+        cl = np.zeros((h, w), np.uint64)
+        cr = np.zeros((h, w), np.uint64)
+        L = np.zeros((p, h, w, d), np.uint16)
+        S = np.zeros((h, w, d), np.uint16)
+        c = config.to_c()
+        _check(_sgm_dump(self._h, ctx.handle, left.handle, right.handle, ctypes.byref(c),
+                         _P(cl.ctypes.data), _P(cr.ctypes.data), _P(L.ctypes.data),
+                         _P(S.ctypes.data)))
+        return cl, cr, L, S
+
+    def close(self):
+        if self._h:
+            _sgm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def workspace_bytes(width: int, height: int, config: SGMStereoConfig) -> int:
+    c = config.to_c()
+    return int(_sgm_ws(width, height, ctypes.byref(c)))
+
+
+# ---------------------------------------------------------------------------
+# Synthetic pairs (libvx_synth.so): R(x - d, y) = L(x, y), the shader's convention.
+SCENE_PLANES, SCENE_SLANTED, SCENE_SURFACE = 0, 1, 2
+_synth = None
+
+
+def synth_pair(scene: int, width: int, height: int, d_lo: float, d_hi: float, seed: int):
+    """Returns (left u8, right u8, ground-truth disparity f32), each (H, W)."""
+    global _synth
+    if _synth is None:
+        _synth = ctypes.CDLL(SYNTH_PATH)
+        _synth.vx_synth_pair.restype = ctypes.c_int
+        _synth.vx_synth_pair.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                         ctypes.c_float, ctypes.c_uint64, _P, _P, _P]
+    L = np.empty((height, width), np.uint8)
+    R = np.empty((height, width), np.uint8)
+    G = np.empty((height, width), np.float32)
+    r = _synth.vx_synth_pair(scene, width, height, d_lo, d_hi, seed, L.ctypes.data,
+                             R.ctypes.data, G.ctypes.data)
+    if r != 0:
+        raise ValueError("vx_synth_pair rejected its arguments")
+    return L, R, G
