@@ -41,8 +41,12 @@ DISPARITIES = [64, 128, 192]
 NUM_PAIRS = 64
 
 
-def workload(rank: int):
-    """64 (w, h, D, seed) tuples; seeds differ per rank (replicas)."""
+def workload(rank: int, name: str = "mixed"):
+    """(w, h, D, seed) tuples; seeds differ per rank (replicas). "mixed" is the 64-pair
+    mixed-size workload; "profile" is a small case for profiler captures (2 pairs of
+    1242x375, D=128: 1.9 GB of path slabs, larger than L2)."""
+    if name == "profile":
+        return [(1242, 375, 128, 1_000_003 * (rank + 1) + i) for i in range(2)]
     rng = np.random.default_rng(20261203 + 7919 * rank)
     items = []
     for i in range(NUM_PAIRS):
@@ -173,6 +177,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile"])
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -195,7 +202,7 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     import vx_sgm
-    items = workload(rank)
+    items = workload(rank, args.workload)
     pairs = make_pairs(vx_sgm, items)
     cfgs = [sgm_config(vx_sgm, d) for (_, _, d, _) in items]
     total_pd = sum(w * h * d for (w, h, d, _) in items)
@@ -245,6 +252,15 @@ def main():
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
     value = world * total_pd / (ms * 1e-3) / 1e9
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms,
+                              "workload": args.workload, "stages_ms": {
+                                  "census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
+                              "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # ---- end to end through the C ABI with host buffers ----
     pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
@@ -285,7 +301,7 @@ def main():
     barrier()
     plain_ms = 0.0
     for _ in range(args.plain_steps):
-        for i in range(NUM_PAIRS):
+        for i in range(len(items)):
             pe0.record(stream)
             sgm.compute_disparity(ctx, tl[i], tr[i], of[i], cfgs[i], output_i16=oi[i])
             pe1.record(stream)
