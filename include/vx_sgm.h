@@ -129,6 +129,29 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
                                vx_image* const* out_i16, const vx_sgm_config* cfgs,
                                vx_stream stream);
 
+/* No counterpart in the reference (its compute_disparity allocates per call,
+ * vx-vision/src/kernels/sgm.rs:122-129). For callers that cannot allocate
+ * device memory when they call - a host that owns all GPU memory through its
+ * own allocator, a real-time loop that must not take the implicit device
+ * synchronisation of cudaMalloc/cudaFree, a plugin whose host forbids
+ * allocation during a call: same result as vx_sgm_compute_disparity, but all
+ * intermediate state lives in a static device array of
+ * vx_sgm_static_scratch_bytes() (64 MiB, held on every GPU where the library's
+ * module is loaded until the process exits) and the call allocates nothing.
+ * Planes are device pointers with pitches in bytes on the calling thread's
+ * current device; out_i16 may be NULL. Pairs whose workspace does not fit are
+ * rejected with VX_ERR_BUDGET. All calls share the array: calls whose GPU work
+ * overlaps race on it. The first call on a device sets that device up; make it
+ * before any stream capture. NULL stream = legacy default stream, synchronous. */
+vx_status vx_sgm_compute_disparity_noalloc(const uint8_t* left, size_t left_pitch,
+                                           const uint8_t* right, size_t right_pitch,
+                                           uint32_t width, uint32_t height, float* out_f32,
+                                           size_t out_f32_pitch, int16_t* out_i16,
+                                           size_t out_i16_pitch, const vx_sgm_config* cfg,
+                                           vx_stream stream);
+/* Size in bytes of the static scratch used by vx_sgm_compute_disparity_noalloc. */
+size_t vx_sgm_static_scratch_bytes(void);
+
 /* Device bytes of intermediate state one pair needs (census + path slabs). */
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg);
 

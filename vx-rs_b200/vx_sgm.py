@@ -93,6 +93,10 @@ _sgm_batch = _sig("vx_sgm_compute_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
                   ctypes.POINTER(_CConfig), _P)
 _sgm_ws = _sig("vx_sgm_workspace_bytes", ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
                ctypes.POINTER(_CConfig))
+_sgm_noalloc = _sig("vx_sgm_compute_disparity_noalloc", ctypes.c_int, _P, ctypes.c_size_t, _P,
+                    ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_size_t, _P,
+                    ctypes.c_size_t, ctypes.POINTER(_CConfig), _P)
+_static_scratch_bytes = _sig("vx_sgm_static_scratch_bytes", ctypes.c_size_t)
 _sgm_dump = _sig("vx_sgm_debug_dump", ctypes.c_int, _P, _P, _P, _P, ctypes.POINTER(_CConfig),
                  _P, _P, _P, _P)
 
@@ -309,6 +313,23 @@ class SGMStereo:
             self.close()
         except Exception:
             pass
+
+
+def compute_disparity_noalloc(left: Texture, right: Texture, output: Texture,
+                              config: SGMStereoConfig, output_i16: Texture | None = None,
+                              stream: int | None = None):
+    """vx_sgm_compute_disparity_noalloc on the planes of existing textures: for callers that
+    cannot allocate device memory during the call (scratch is a static 64 MiB device array)."""
+    c = config.to_c()
+    _check(_sgm_noalloc(_P(left.device_ptr), left.pitch, _P(right.device_ptr), right.pitch,
+                        left.width, left.height, _P(output.device_ptr), output.pitch,
+                        _P(output_i16.device_ptr) if output_i16 is not None else None,
+                        output_i16.pitch if output_i16 is not None else 0, ctypes.byref(c),
+                        _P(stream) if stream else None))
+
+
+def static_scratch_bytes() -> int:
+    return int(_static_scratch_bytes())
 
 
 def workspace_bytes(width: int, height: int, config: SGMStereoConfig) -> int:
