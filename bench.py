@@ -44,9 +44,12 @@ NUM_PAIRS = 64
 def workload(rank: int, name: str = "mixed"):
     """(w, h, D, seed) tuples; seeds differ per rank (replicas). "mixed" is the 64-pair
     mixed-size workload; "profile" is a small case for profiler captures (2 pairs of
-    1242x375, D=128: 1.9 GB of path slabs, larger than L2)."""
+    1242x375, D=128: 1.9 GB of path slabs, larger than L2) and "profile-mix" a
+    medium one that fills the GPU with all three D (32 pairs of 320x240)."""
     if name == "profile":
         return [(1242, 375, 128, 1_000_003 * (rank + 1) + i) for i in range(2)]
+    if name == "profile-mix":  # 32 pairs of 320x240, D cycling 64/128/192: 5 GB of slabs
+        return [(320, 240, DISPARITIES[i % 3], 1_000_003 * (rank + 1) + i) for i in range(32)]
     rng = np.random.default_rng(20261203 + 7919 * rank)
     items = []
     for i in range(NUM_PAIRS):
@@ -177,7 +180,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile", "profile-mix"])
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()

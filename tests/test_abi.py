@@ -46,9 +46,12 @@ def test_config_defaults_match_reference():
 def test_workspace_bytes_formula():
     cfg = vx_sgm.SGMStereoConfig(num_disparities=64, census_radius_x=2, census_radius_y=2, num_paths=4)
     b = vx_sgm.workspace_bytes(640, 480, cfg)
-    assert b == 4 * 640 * 480 * 4 + 640 * 480 * 64 * 4 * 2
+    # guarded row-major census planes + 32-row banded copies (480 = 15 bands) + u16 slabs
+    al = lambda v: (v + 255) // 256 * 256
+    assert b == 2 * al(640 * 480 * 4 + 2 * 320 * 4) + 2 * 640 * 480 * 4 + 640 * 480 * 64 * 4 * 2
     cfg64 = vx_sgm.SGMStereoConfig(num_disparities=60, num_paths=8)  # 9x7 census -> u64 words, Dp=64
-    assert vx_sgm.workspace_bytes(100, 10, cfg64) == 4 * ((1000 * 8 + 255) // 256 * 256) + 1000 * 64 * 8 * 2
+    assert vx_sgm.workspace_bytes(100, 10, cfg64) == (2 * al(1000 * 8 + 2 * 320 * 8) + 2 * al(32 * 100 * 8)
+                                                      + 1000 * 64 * 8 * 2)
 
 
 def test_context_without_gpu_reports_device_not_found():

@@ -1,5 +1,5 @@
-// Path aggregation of semi-global matching, all paths of all pairs of a batch
-// in one persistent launch per kernel variant.
+// Path aggregation of semi-global matching: every path of every pair of a batch
+// in ONE persistent launch over a work queue of (pair, path, 32-scanline) units.
 //
 // Semantics (vx-vision/shaders/SGMStereo.metal:72-173), per scanline, per pixel,
 // for d = 0..D-1 in increasing order with ONE array Lp[] updated in place:
@@ -14,13 +14,34 @@
 // The shader only runs directions (1,0) and (0,1) (sgm.rs:197-200); the other
 // six directions are the same recurrence on the other scanline families.
 //
-// Mapping: one thread owns one scanline and keeps its D costs in registers as
-// packed u16 pairs, so the in-place recurrence is a register sweep with no
-// cross-lane traffic. A warp takes 32 neighbouring scanlines of one job, laid
-// out so that at every step its lanes sit on consecutive pixels of one row
-// (vertical, diagonal) or one column (horizontal, which reads the
-// column-major census): census loads of a warp are consecutive words.
-// Each pixel's D results go to this path's slab with 16-byte stores.
+// Evaluation. With A_d = min(o0, o2, o3) (independent of the current pixel) and
+// f_d = u16(Lp[d] + P1) = o1_{d+1}, one pixel is the chain
+//     t_d = min(A_d, f_{d-1});  f_d = u16(t_d + C_d + P1 - m);  Lp[d] = u16(t_d + C_d - m)
+// whose critical path is one min and one add per disparity. u16 values live in
+// the low half of 32-bit registers: min.u16x2 compares halves on their own and a
+// 32-bit add's low half is the u16 sum, so whatever accumulates in the high half
+// never reaches the low half and no masking is needed. A_d is formed two
+// disparities at a time on packed state words (min.u16x2, and a per-half
+// wrapping add for Lp[d+1] + P1).
+//
+// Mapping. One thread owns one scanline. Its D state values (packed u16 pairs)
+// live in warp-private shared memory as [group of 8 d][lane] 16-byte words, so a
+// warp's access to one group is 512 contiguous bytes (conflict-free) and the
+// per-pixel loop runs over groups with a small loop body and a runtime D: one
+// kernel serves every D of a batch. A warp takes 32 neighbouring scanlines of
+// one (pair, path):
+//  * vertical / diagonal paths: the 32 lanes sit on 32 consecutive pixels of one
+//    row at every step, so the right-census words they need form one segment of
+//    Dp+31 words of that row; it is staged in warp-private shared memory with
+//    16-byte cp.async copies one step ahead (double-buffered).
+//  * horizontal paths: the 32 lanes are 32 consecutive rows (one 32-row band)
+//    at the same x and read the banded census copy: each disparity is one
+//    coalesced 128-byte load at a constant offset, and the window of the last D
+//    columns stays in L1.
+// Census words of the next group are loaded while the current group is
+// processed. Pixels whose window may reach x-d < 0 take a second body with the
+// border test, picked by a warp-uniform branch. Results leave as 16-byte stores
+// into this path's slab.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -32,164 +53,382 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+__device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+
 __device__ __forceinline__ uint32_t popc_xor(uint32_t a, uint32_t b) { return __popc(a ^ b); }
 __device__ __forceinline__ uint32_t popc_xor(uint64_t a, uint64_t b) { return __popcll(a ^ b); }
 
-template <int DMAX, bool EXACT, typename CT, bool HORIZ>
+// 16-byte global -> shared copy that bypasses L1 (staged words are used once).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+__device__ __forceinline__ void cp_async_wait_1() {
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+// Per-scanline constants of one unit.
+struct ScanConst {
+    uint32_t p1x2;        // P1 in both halves
+    uint32_t P1, P2;
+    int Dp, G;            // disparities padded to 8, groups of 8
+    int last_j;           // position of d = D-1 inside the last group (0..7)
+};
+
+// Per-pixel values shared by the groups of one pixel.
+struct PixelState {
+    uint32_t o3x2;   // u16(m + P2) in both halves
+    uint32_t kc;     // f = t + C + (P1 - m)
+    uint32_t km;     // Lp = t + C - m
+    uint32_t f;      // o1 of the next disparity (low half)
+    uint32_t mn;     // running min of the new values (per half)
+};
+
+// Matching costs of one group from its 8 right-census words; x-d < 0 gives 64.
+template <bool CHECK, typename CT>
+__device__ __forceinline__ void group_costs(uint32_t (&c)[8], const CT lc, const CT (&r)[8],
+                                            const int x, const int g) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        c[i] = popc_xor(lc, r[i]);
+        if (CHECK && x - (8 * g + i) < 0) c[i] = 64u;
+    }
+}
+
+// One group of 8 disparities d = 8g..8g+7 of one pixel. cur = old state words of
+// the group, nxt_lo = old Lp[8g+8] in the low half (unused for the last group),
+// c = the group's matching costs. LAST: the group holding d = D-1, whose o2 is
+// forced to 0xFFFF and whose pads (d >= D) are kept out of the minimum.
+template <bool LAST>
+__device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_lo,
+                                           const uint32_t (&c)[8], const ScanConst& k,
+                                           PixelState& ps) {
+    const uint32_t w[5] = {cur.x, cur.y, cur.z, cur.w, nxt_lo};
+    uint32_t out[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        uint32_t o2 = __vadd2(__byte_perm(w[j], w[j + 1], 0x5432), k.p1x2);
+        if (LAST) {
+            if (k.last_j == 2 * j) o2 |= 0x0000FFFFu;
+            if (k.last_j == 2 * j + 1) o2 |= 0xFFFF0000u;
+        }
+        const uint32_t A = vmin2(vmin2(w[j], o2), ps.o3x2);
+        const uint32_t t0 = vmin2(A, ps.f);
+        ps.f = t0 + c[2 * j] + ps.kc;
+        const uint32_t e0 = t0 + c[2 * j] + ps.km;
+        const uint32_t t1 = vmin2(A >> 16, ps.f);
+        ps.f = t1 + c[2 * j + 1] + ps.kc;
+        const uint32_t e1 = t1 + c[2 * j + 1] + ps.km;
+        out[j] = __byte_perm(e0, e1, 0x5410);
+    }
+    if (!LAST) {
+        ps.mn = vmin2(ps.mn, vmin2(vmin2(out[0], out[1]), vmin2(out[2], out[3])));
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            uint32_t pm = out[j];
+            if (2 * j > k.last_j) pm |= 0x0000FFFFu;   // pads never count
+            if (2 * j + 1 > k.last_j) pm |= 0xFFFF0000u;
+            ps.mn = vmin2(ps.mn, pm);
+        }
+    }
+    return make_uint4(out[0], out[1], out[2], out[3]);
+}
+
+// One pixel: Lsm = this lane's state words (group g at Lsm[g * 32]).
+// getR(d) = right census at x-d; it is only called with x-d >= 0 when CHECK.
+// prefetch(d) hints the census word at x-d into L1 (horizontal paths).
+// Software pipeline over groups (loop unrolled by two, register sets in
+// ping-pong): while group g runs its min/add chain, the census words and state
+// of group g+1 are in flight, and g+1's costs are formed right after g's chain,
+// so neither load nor popcount latency sits on the chain.
+template <bool CHECK, typename CT, typename GetR, typename Prefetch>
+__device__ __forceinline__ void sgm_pixel(uint4* __restrict__ Lsm, uint32_t& m, const CT lc,
+                                          const GetR& getR, const Prefetch& prefetch,
+                                          const int x, const ScanConst& k,
+                                          uint16_t* __restrict__ dst) {
+    PixelState ps;
+    const uint32_t o3 = (m + k.P2) & 0xFFFFu;
+    ps.o3x2 = o3 | (o3 << 16);
+    ps.kc = k.P1 - m;
+    ps.km = 0u - m;
+    ps.f = 0xFFFFu;            // o1 at d = 0
+    ps.mn = 0xFFFFFFFFu;
+    auto load = [&](CT (&r)[8], int g) {
+        prefetch(8 * (g + 2));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int d = 8 * g + i;
+            r[i] = (!CHECK || x - d >= 0) ? getR(d) : CT(0);
+        }
+    };
+    // Slab stores are streaming (evict-first): slabs are written once here and
+    // read once by the WTA kernel, and must not push the census planes, which
+    // every path re-reads, out of L2.
+    auto store = [&](const uint4 o, int g) {
+        Lsm[g * 32] = o;
+        __stcs(reinterpret_cast<uint4*>(dst + 8 * g), o);
+    };
+    CT ra[8], rb[8];
+    uint32_t ca[8], cb[8];
+    load(ra, 0);
+    uint4 sa = Lsm[0], sb;
+    group_costs<CHECK>(ca, lc, ra, x, 0);
+    int g = 0;
+#pragma unroll 1
+    for (; g + 2 < k.G; g += 2) {
+        sb = Lsm[(g + 1) * 32];
+        load(rb, g + 1);
+        store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
+        group_costs<CHECK>(cb, lc, rb, x, g + 1);
+        sa = Lsm[(g + 2) * 32];
+        load(ra, g + 2);
+        store(sgm_group<false>(sb, sa.x, cb, k, ps), g + 1);
+        group_costs<CHECK>(ca, lc, ra, x, g + 2);
+    }
+    if (g + 1 < k.G) {
+        sb = Lsm[(g + 1) * 32];
+        load(rb, g + 1);
+        store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
+        group_costs<CHECK>(cb, lc, rb, x, g + 1);
+        store(sgm_group<true>(sb, 0u, cb, k, ps), g + 1);
+    } else {
+        store(sgm_group<true>(sa, 0u, ca, k, ps), g);
+    }
+    m = min(ps.mn & 0xFFFFu, ps.mn >> 16);
+}
+
+__device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
+    ScanConst k;
+    k.P1 = (uint32_t)pr.p1;
+    k.P2 = (uint32_t)pr.p2;
+    k.p1x2 = k.P1 | (k.P1 << 16);
+    k.Dp = pr.nd_pad;
+    k.G = pr.nd_pad / 8;
+    k.last_j = (pr.nd - 1) - 8 * (k.G - 1);
+    return k;
+}
+
+__device__ __forceinline__ void clear_state(uint4* Lsm, int G) {
+    for (int g = 0; g < G; ++g) Lsm[g * 32] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// Unit = 32 scanlines of a vertical or diagonal path.
+template <typename CT>
+__device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
+                                                  uint4* __restrict__ Lsm, CT* __restrict__ stage,
+                                                  int seg_words) {
+    const int lane = threadIdx.x & 31;
+    const int W = pr.width, H = pr.height;
+    const ScanConst k = scan_const(pr);
+    const int Dp = k.Dp;
+    const int dx = job.dx, dy = job.dy;
+
+    const int i = first + lane;
+    const int k0 = job.k_min + first;         // scanline index of lane 0
+    const int kk = k0 + lane;
+    // Lane pixel at step t: x = kk + dx*t, y = y0 + dy*t (vertical: dx = 0).
+    const int y0 = dy > 0 ? 0 : H - 1;
+    int tb, te;
+    if (dx == 0) { tb = 0; te = H; }
+    else if (dx > 0) { tb = max(0, -kk); te = min(H, W - kk); }
+    else { tb = max(0, kk - W + 1); te = min(H, kk + 1); }
+    if (i >= job.num_scanlines) { tb = 0x7fffffff; te = -1; }
+    const int t_lo = __reduce_min_sync(kFull, tb);
+    const int t_hi = __reduce_max_sync(kFull, te);
+    if (t_lo >= t_hi) return;
+
+    const CT* __restrict__ CL = static_cast<const CT*>(pr.census_l);
+    const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
+    uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+
+    // Stage the right-census segment [xb-(Dp-1), xb+31] of the step's row in
+    // 16-byte chunks from the aligned word at or below its start. The planes are
+    // surrounded by guard words (kCensusGuardWords), so the chunks may run past
+    // the row ends: words outside the image are never used for a cost (lanes
+    // with x >= W are idle and x-d < 0 takes the border body).
+    // The alignment is taken on the plane's linear word index (row starts y*W
+    // are not 16-byte aligned in general); the plane base is.
+    constexpr int kPerChunk = 16 / sizeof(CT);
+    auto seg_start = [&](int t) {
+        return (ptrdiff_t)(y0 + dy * t) * W + (k0 + dx * t - (Dp - 1));
+    };
+    auto stage_step = [&](int t, int buf) {
+        const ptrdiff_t ls = seg_start(t);
+        const ptrdiff_t la = ls & ~(ptrdiff_t)(kPerChunk - 1);
+        const CT* src = CR + la;
+        CT* dstb = stage + buf * seg_words;
+        const int chunks = (Dp + 31 + (int)(ls - la) + kPerChunk - 1) / kPerChunk;
+        for (int j = lane; j < chunks; j += 32) cp_async16(dstb + j * kPerChunk, src + j * kPerChunk);
+        cp_async_commit();
+    };
+    auto seg_offset = [&](int t) {
+        const ptrdiff_t ls = seg_start(t);
+        return (int)(ls - (ls & ~(ptrdiff_t)(kPerChunk - 1)));
+    };
+
+    clear_state(Lsm, k.G);
+    uint32_t m = 0u;
+    stage_step(t_lo, t_lo & 1);
+    CT lc_next = CT(0);
+    if (t_lo >= tb && t_lo < te) lc_next = CL[(size_t)(y0 + dy * t_lo) * W + kk + dx * t_lo];
+    for (int t = t_lo; t < t_hi; ++t) {
+        if (t + 1 < t_hi) stage_step(t + 1, (t + 1) & 1);
+        else cp_async_commit();                 // keep one group per step
+        const CT lc = lc_next;
+        const bool active = t >= tb && t < te;
+        const int x = kk + dx * t;
+        const int y = y0 + dy * t;
+        if (t + 1 < t_hi && t + 1 >= tb && t + 1 < te)
+            lc_next = CL[(size_t)(y + dy) * W + (x + dx)];
+        cp_async_wait_1();
+        __syncwarp();
+        const CT* seg = stage + (t & 1) * seg_words + seg_offset(t) + lane + (Dp - 1);  // seg[-d] = R(x-d)
+        auto getR = [seg](int d) { return seg[-d]; };
+        auto no_prefetch = [](int) {};
+        const int xb = k0 + dx * t;             // smallest x of the warp
+        if (active) {
+            uint16_t* dst = out + ((size_t)y * W + x) * Dp;
+            if (xb >= Dp - 1)
+                sgm_pixel<false, CT>(Lsm, m, lc, getR, no_prefetch, x, k, dst);
+            else
+                sgm_pixel<true, CT>(Lsm, m, lc, getR, no_prefetch, x, k, dst);
+        }
+        __syncwarp();
+    }
+}
+
+// Unit = 32 rows of a horizontal path (column-major census).
+template <typename CT>
+__device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job,
+                                                    int first, uint4* __restrict__ Lsm) {
+    const int lane = threadIdx.x & 31;
+    const int W = pr.width, H = pr.height;
+    const ScanConst k = scan_const(pr);
+    const int Dp = k.Dp;
+    const int dx = job.dx;
+    const int y = first + lane;                 // row of this lane
+    const bool active = y < job.num_scanlines;
+    const int yc = active ? y : first;          // keeps idle lanes' addresses in bounds
+    // Banded census: word (x, y) at ((y / 32) * W + x) * 32 + y % 32, so the 32
+    // rows of this unit (first is a multiple of 32) read 128 contiguous bytes per
+    // column and column x-d sits at a constant offset of -32*d words.
+    const size_t band = (size_t)(first >> 5) * W;
+    const CT* __restrict__ CL = static_cast<const CT*>(pr.census_lt) + band * 32 + lane;
+    const CT* __restrict__ CR = static_cast<const CT*>(pr.census_rt) + band * 32 + lane;
+    uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+    (void)H;
+
+    clear_state(Lsm, k.G);
+    uint32_t m = 0u;
+    const int x0 = dx > 0 ? 0 : W - 1;
+    CT lc_next = CL[(size_t)x0 * 32];
+    for (int t = 0; t < W; ++t) {
+        const int x = x0 + dx * t;
+        const CT lc = lc_next;
+        if (t + 1 < W) lc_next = CL[(size_t)(x + dx) * 32];
+        const CT* col = CR + (size_t)x * 32;        // col[-32*d] = R(x-d, y)
+        auto getR = [col](int d) { return col[-32 * d]; };
+        // Two groups further ahead: bring the 8 columns of that group into L1
+        // (one line per column of the band; columns left of x = 0 are skipped).
+        auto prefetch = [col, x, Dp](int d0) {
+            if (d0 < Dp) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (x - d0 - i >= 0)
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(col - 32 * (d0 + i)));
+            }
+        };
+        if (active) {
+            uint16_t* dst = out + ((size_t)yc * W + x) * Dp;
+            if (x >= Dp - 1)
+                sgm_pixel<false, CT>(Lsm, m, lc, getR, prefetch, x, k, dst);
+            else
+                sgm_pixel<true, CT>(Lsm, m, lc, getR, prefetch, x, k, dst);
+        }
+    }
+}
+
+template <typename CT>
 __global__ void __launch_bounds__(kAggWarpsPerBlock * 32)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
-                 const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter) {
-    constexpr int NW = DMAX / 2;  // packed u16 pairs per thread
-    static_assert(NW % 4 == 0, "DMAX must be a multiple of 8");
-    const int lane = threadIdx.x & 31;
-
+                 const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
+                 int dp_max) {
+    extern __shared__ __align__(16) unsigned char agg_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg_words = dp_max + 40;                          // Dp+31 words + alignment
+    const size_t state_bytes = (size_t)dp_max * 64;             // [dp_max/8][32] uint4
+    const size_t warp_bytes = state_bytes + 2 * seg_words * sizeof(CT);
+    unsigned char* base = agg_smem + warp * warp_bytes;
+    uint4* Lsm = reinterpret_cast<uint4*>(base) + lane;
+    CT* stage = reinterpret_cast<CT*>(base + state_bytes);
     for (;;) {
         int u = 0;
         if (lane == 0) u = (int)atomicAdd(counter, 1u);
         u = __shfl_sync(kFull, u, 0);
         if (u >= num_units) break;
-
         const UnitDev unit = units[u];
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
-        const int W = pr.width, H = pr.height;
-        const int D = EXACT ? DMAX : pr.nd;
-        const int Dp = pr.nd_pad;
-        const uint32_t P1 = (uint32_t)pr.p1, P2 = (uint32_t)pr.p2;
-        const int dx = job.dx, dy = job.dy;
-
-        const int i = unit.first_scanline + lane;
-        const bool lane_valid = i < job.num_scanlines;
-        const int k = job.k_min + i;
-
-        // Pixel of scanline k at step t: (x0 + kx*k + tx*t, y0 + ky*k + ty*t).
-        int x0, y0, kx, ky;
-        if (dy == 0) { x0 = dx > 0 ? 0 : W - 1; y0 = 0; kx = 0; ky = 1; }
-        else { x0 = 0; y0 = dy > 0 ? 0 : H - 1; kx = 1; ky = 0; }
-        const int tx = dx, ty = dy;
-        int tb, te;
-        if (dy == 0) { tb = 0; te = W; }
-        else if (dx == 0) { tb = 0; te = H; }
-        else if (dx > 0) { tb = max(0, -k); te = min(H, W - k); }
-        else { tb = max(0, k - W + 1); te = min(H, k + 1); }
-        if (!lane_valid) { tb = 0x7fffffff; te = -1; }
-        const int t_lo = __reduce_min_sync(kFull, tb);
-        const int t_hi = __reduce_max_sync(kFull, te);
-
-        const CT* __restrict__ CL = static_cast<const CT*>(HORIZ ? pr.census_lt : pr.census_l);
-        const CT* __restrict__ CR = static_cast<const CT*>(HORIZ ? pr.census_rt : pr.census_r);
-        uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
-
-        uint32_t Lp[NW];
-#pragma unroll
-        for (int w = 0; w < NW; ++w) Lp[w] = 0u;
-        uint32_t m = 0u;
-
-        for (int t = t_lo; t < t_hi; ++t) {
-            if (t < tb || t >= te) continue;
-            const int x = x0 + kx * k + tx * t;
-            const int y = y0 + ky * k + ty * t;
-            CT lc;
-            const CT* rp;  // right census of (x, y); (x - d, y) is rp - d*stride
-            if (HORIZ) {
-                lc = CL[(size_t)x * H + y];
-                rp = CR + (size_t)x * H + y;
-            } else {
-                lc = CL[(size_t)y * W + x];
-                rp = CR + (size_t)y * W + x;
-            }
-            const uint32_t o3 = (m + P2) & 0xFFFFu;
-            uint32_t e = 0u, nm = 0xFFFFu;
-            uint16_t* dst = out + ((size_t)y * W + x) * Dp;
-#pragma unroll
-            for (int w = 0; w < NW; w += 4) {
-                uint32_t packed[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int wi = w + j;
-                    const uint32_t cur = Lp[wi];
-                    const uint32_t nxt = (wi + 1 < NW) ? Lp[wi + 1] : 0u;
-                    uint32_t ev[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int d = 2 * wi + h;
-                        uint32_t c = 64u;
-                        if (x - d >= 0) c = popc_xor(lc, HORIZ ? rp[-(ptrdiff_t)d * H] : rp[-d]);
-                        const uint32_t o0 = h ? (cur >> 16) : (cur & 0xFFFFu);
-                        const uint32_t nb = h ? (nxt & 0xFFFFu) : (cur >> 16);
-                        uint32_t o2 = (nb + P1) & 0xFFFFu;
-                        if (EXACT ? (d == DMAX - 1) : (d >= D - 1)) o2 = 0xFFFFu;
-                        const uint32_t o1 = (d == 0) ? 0xFFFFu : ((e + P1) & 0xFFFFu);
-                        const uint32_t best = min(min(o0, o1), min(o2, o3));
-                        e = (c + best - m) & 0xFFFFu;
-                        if (EXACT || d < D) nm = min(nm, e);
-                        ev[h] = e;
-                    }
-                    packed[j] = ev[0] | (ev[1] << 16);
-                    Lp[wi] = packed[j];
-                }
-                if (EXACT || 2 * w < D)
-                    *reinterpret_cast<uint4*>(dst + 2 * w) =
-                        make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            }
-            m = nm;
-        }
+        if (job.dy == 0)
+            run_horizontal_unit<CT>(pr, job, unit.first_scanline, Lsm);
+        else
+            run_vertical_unit<CT>(pr, job, unit.first_scanline, Lsm, stage, seg_words);
+        __syncwarp();
     }
-}
-
-using AggKernelFn = void (*)(const PairDev*, const JobDev*, const UnitDev*, int, unsigned*);
-
-template <int DMAX, bool EXACT>
-AggKernelFn pick_ct_dir(bool census64, bool horizontal) {
-    if (census64)
-        return horizontal ? aggregate_kernel<DMAX, EXACT, uint64_t, true>
-                          : aggregate_kernel<DMAX, EXACT, uint64_t, false>;
-    return horizontal ? aggregate_kernel<DMAX, EXACT, uint32_t, true>
-                      : aggregate_kernel<DMAX, EXACT, uint32_t, false>;
-}
-
-AggKernelFn pick_kernel(const AggVariant& v) {
-    if (v.exact) {
-        switch (v.dmax) {
-            case 64: return pick_ct_dir<64, true>(v.census64, v.horizontal);
-            case 128: return pick_ct_dir<128, true>(v.census64, v.horizontal);
-            case 192: return pick_ct_dir<192, true>(v.census64, v.horizontal);
-            case 256: return pick_ct_dir<256, true>(v.census64, v.horizontal);
-        }
-    } else {
-        switch (v.dmax) {
-            case 64: return pick_ct_dir<64, false>(v.census64, v.horizontal);
-            case 128: return pick_ct_dir<128, false>(v.census64, v.horizontal);
-            case 256: return pick_ct_dir<256, false>(v.census64, v.horizontal);
-        }
-    }
-    return nullptr;
 }
 
 }  // namespace
 
-int aggregate_grid_ctas(const AggVariant& v) {
-    AggKernelFn fn = pick_kernel(v);
-    if (!fn) return 0;
+size_t aggregate_smem_bytes(int dp_max, bool census64) {
+    const size_t ct = census64 ? 8 : 4;
+    return (size_t)kAggWarpsPerBlock * ((size_t)dp_max * 64 + 2 * (dp_max + 40) * ct);
+}
+
+cudaError_t prepare_aggregate_kernels() {
+    const int max_bytes = (int)aggregate_smem_bytes(256, true);
+    cudaError_t e = cudaFuncSetAttribute(aggregate_kernel<uint32_t>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(aggregate_kernel<uint64_t>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    return e;
+}
+
+int aggregate_grid_ctas(int dp_max, bool census64) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kAggWarpsPerBlock * 32, 0);
+    const size_t smem = aggregate_smem_bytes(dp_max, census64);
+    if (census64)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aggregate_kernel<uint64_t>,
+                                                      kAggWarpsPerBlock * 32, smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aggregate_kernel<uint32_t>,
+                                                      kAggWarpsPerBlock * 32, smem);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 
-cudaError_t launch_aggregate(const AggVariant& v, const PairDev* d_pairs, const JobDev* d_jobs,
-                             const UnitDev* d_units, int num_units, unsigned* counter,
-                             int grid_ctas, cudaStream_t stream) {
+cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
+                             const JobDev* d_jobs, const UnitDev* d_units, int num_units,
+                             unsigned* counter, int grid_ctas, cudaStream_t stream) {
     if (num_units <= 0) return cudaSuccess;
-    AggKernelFn fn = pick_kernel(v);
-    if (!fn) return cudaErrorInvalidValue;
-    if (grid_ctas <= 0) grid_ctas = aggregate_grid_ctas(v);
+    if (grid_ctas <= 0) grid_ctas = aggregate_grid_ctas(dp_max, census64);
     const int needed = (num_units + kAggWarpsPerBlock - 1) / kAggWarpsPerBlock;
     if (grid_ctas > needed) grid_ctas = needed;
+    const size_t smem = aggregate_smem_bytes(dp_max, census64);
     count_launch();
-    fn<<<grid_ctas, kAggWarpsPerBlock * 32, 0, stream>>>(d_pairs, d_jobs, d_units, num_units,
-                                                         counter);
+    if (census64)
+        aggregate_kernel<uint64_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max);
+    else
+        aggregate_kernel<uint32_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max);
     return cudaGetLastError();
 }
 

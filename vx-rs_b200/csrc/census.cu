@@ -9,9 +9,10 @@
 // Layout: each 32x8 tile of one view is staged once in shared memory with its
 // (rx, ry) apron (clamped coordinates), then every thread builds one
 // descriptor from shared memory. Descriptors are written twice: row-major
-// (read by vertical and diagonal paths) and column-major (read by horizontal
-// paths, so that the 32 scanlines of a warp - 32 consecutive rows - load
-// consecutive words). Output word: u32 when the window has <= 32 bits, else u64.
+// (read by vertical and diagonal paths) and in 32-row bands, x-major inside a
+// band, word (x, y) at ((y/32)*W + x)*32 + y%32 (read by horizontal paths: the
+// 32 scanlines of a warp are the 32 rows of a band, so each column is 128
+// contiguous bytes). Output word: u32 when the window has <= 32 bits, else u64.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -75,7 +76,7 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
     CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
     rm[(size_t)y * W + x] = (CT)bits;
-    cm[(size_t)x * H + y] = (CT)bits;
+    cm[((size_t)(y >> 5) * W + x) * 32 + (y & 31)] = (CT)bits;
 }
 
 }  // namespace

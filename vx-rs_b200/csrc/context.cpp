@@ -77,6 +77,7 @@ vx_status vx_ctx_create(int device_ordinal, vx_ctx** out) {
         uint64_t threshold = UINT64_MAX;
         e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
+
     if (e != cudaSuccess) {
         vx_status s = cuda_fail(e, "vx_ctx_create");
         if (ctx->pool) cudaMemPoolDestroy(ctx->pool);

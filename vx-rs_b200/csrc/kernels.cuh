@@ -13,7 +13,7 @@ struct PairDev {
     size_t left_pitch, right_pitch;
     void* census_l;        // W*H census words, row-major (y*W + x)
     void* census_r;
-    void* census_lt;       // W*H census words, column-major (x*H + y)
+    void* census_lt;       // census words in 32-row bands: ((y/32)*W + x)*32 + y%32
     void* census_rt;
     uint16_t* slabs;       // num_paths slabs of H*W*Dp u16 (pixel-major, d-minor)
     size_t slab_stride;    // elements per slab = H*W*Dp
@@ -51,6 +51,10 @@ struct UnitDev {
 constexpr int kCensusTileW = 32;
 constexpr int kCensusTileH = 8;
 constexpr int kAggWarpsPerBlock = 4;
+// Guard words before and after every row-major census plane: the aggregation
+// kernel stages aligned 16-byte chunks that may extend past the first and last
+// row by up to 256 + 40 words.
+constexpr int kCensusGuardWords = 320;
 constexpr int kWtaThreads = 256;
 // Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).
 constexpr int kMaxWidth = 16384;

@@ -17,26 +17,16 @@ inline void count_launch(uint64_t n = 1) { g_kernel_launches.fetch_add(n, std::m
 cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
                           int max_ry, bool census64, cudaStream_t stream);
 
-// Kernel variant of the path aggregation, chosen per group of units.
-struct AggVariant {
-    int dmax;     // register capacity in disparities: 64, 128, 192, 256
-    bool exact;   // D == dmax for every pair of the group
-    bool census64;
-    bool horizontal;
-    bool operator==(const AggVariant& o) const {
-        return dmax == o.dmax && exact == o.exact && census64 == o.census64 &&
-               horizontal == o.horizontal;
-    }
-};
-
-// Persistent launch over `num_units` warp units; warps pull units from
-// `*counter` (must be zero on entry). grid_ctas = 0 picks SMs x occupancy.
-cudaError_t launch_aggregate(const AggVariant& v, const PairDev* d_pairs, const JobDev* d_jobs,
-                             const UnitDev* d_units, int num_units, unsigned* counter,
-                             int grid_ctas, cudaStream_t stream);
-
-// Number of CTAs a persistent aggregation launch uses for this variant.
-int aggregate_grid_ctas(const AggVariant& v);
+// Path aggregation: one persistent launch over `num_units` warp units of every
+// (pair, path) of a batch; warps pull units from `*counter` (zero on entry).
+// dp_max = largest padded disparity count of the batch (sizes shared memory).
+// grid_ctas = 0 picks SMs x occupancy.
+size_t aggregate_smem_bytes(int dp_max, bool census64);
+cudaError_t prepare_aggregate_kernels();  // raises the shared-memory limit; once per device
+int aggregate_grid_ctas(int dp_max, bool census64);
+cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
+                             const JobDev* d_jobs, const UnitDev* d_units, int num_units,
+                             unsigned* counter, int grid_ctas, cudaStream_t stream);
 
 // WTA + subpixel + optional LR check: one CTA per (pair, row). The kernel keeps
 // three words per pixel of the row in shared memory.

@@ -17,18 +17,6 @@ inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a
 // (vx-vision/src/kernels/sgm.rs:197-200), the rest are the 4/8-path extension.
 const int kDirs[8][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
 
-int pick_dmax(int nd, bool* exact) {
-    for (int v : {64, 128, 192, 256})
-        if (nd == v) {
-            *exact = true;
-            return v;
-        }
-    *exact = false;
-    for (int v : {64, 128, 256})
-        if (nd <= v) return v;
-    return 0;
-}
-
 }  // namespace
 
 int census_bits(const vx_sgm_config& cfg) {
@@ -78,7 +66,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
     pl.pair_data_off.resize(n);
     size_t data = 0;
     int tiles = 0, rows = 0;
-    std::vector<std::vector<UnitDev>> group_units;
+    std::vector<UnitDev> units;
     for (int i = 0; i < n; ++i) {
         const PairSpec& s = specs[i];
         const vx_sgm_config& c = s.cfg;
@@ -118,37 +106,30 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         // Workspace-relative data: 4 census planes then P slabs.
         const size_t npx = (size_t)W * H;
         pl.pair_data_off[i] = data;
-        const size_t cplane = align_up(npx * ct);
-        pd.census_l = reinterpret_cast<void*>(data);
-        pd.census_r = reinterpret_cast<void*>(data + cplane);
+        const size_t guard = kCensusGuardWords * ct;
+        const size_t cplane = align_up(npx * ct + 2 * guard);                  // guarded row-major
+        const size_t bplane = align_up((size_t)((H + 31) / 32) * 32 * W * ct);  // banded copy
+        pd.census_l = reinterpret_cast<void*>(data + guard);
+        pd.census_r = reinterpret_cast<void*>(data + cplane + guard);
         pd.census_lt = reinterpret_cast<void*>(data + 2 * cplane);
-        pd.census_rt = reinterpret_cast<void*>(data + 3 * cplane);
-        data += 4 * cplane;
+        pd.census_rt = reinterpret_cast<void*>(data + 2 * cplane + bplane);
+        data += 2 * cplane + 2 * bplane;
         pd.slab_stride = npx * (size_t)Dp;
         pd.slabs = reinterpret_cast<uint16_t*>(data);
         data += align_up(pd.slab_stride * P * sizeof(uint16_t));
 
-        bool exact = false;
-        const int dmax = pick_dmax(D, &exact);
+        pl.dp_max = std::max(pl.dp_max, Dp);
         for (int p = 0; p < P; ++p) {
             JobDev j{};
             j.pair = i;
             j.path = p;
             j.dx = kDirs[p][0];
             j.dy = kDirs[p][1];
-            const bool horiz = j.dy == 0;
-            j.num_scanlines = horiz ? H : (j.dx == 0 ? W : W + H - 1);
+            j.num_scanlines = j.dy == 0 ? H : (j.dx == 0 ? W : W + H - 1);
             j.k_min = (j.dx > 0 && j.dy != 0) ? -(H - 1) : 0;
             const int job = (int)pl.jobs.size();
             pl.jobs.push_back(j);
-            AggVariant v{dmax, exact, pl.census64, horiz};
-            int g = 0;
-            while (g < (int)pl.groups.size() && !(pl.groups[g].variant == v)) ++g;
-            if (g == (int)pl.groups.size()) {
-                pl.groups.push_back({v, 0, 0});
-                group_units.emplace_back();
-            }
-            for (int k = 0; k < j.num_scanlines; k += 32) group_units[g].push_back({job, k});
+            for (int k = 0; k < j.num_scanlines; k += 32) units.push_back({job, k});
         }
     }
     pl.total_tiles = tiles;
@@ -175,17 +156,12 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         }
         return len * p.nd;
     };
-    for (size_t g = 0; g < pl.groups.size(); ++g) {
-        auto& us = group_units[g];
-        std::vector<std::pair<long long, int>> order(us.size());
-        for (size_t i = 0; i < us.size(); ++i) order[i] = {-unit_cost(us[i]), (int)i};
+    {
+        std::vector<std::pair<long long, int>> order(units.size());
+        for (size_t i = 0; i < units.size(); ++i) order[i] = {-unit_cost(units[i]), (int)i};
         std::sort(order.begin(), order.end());
-        std::vector<UnitDev> sorted(us.size());
-        for (size_t i = 0; i < us.size(); ++i) sorted[i] = us[order[i].second];
-        us.swap(sorted);
-        pl.groups[g].unit_begin = (int)pl.units.size();
-        pl.groups[g].unit_count = (int)us.size();
-        pl.units.insert(pl.units.end(), us.begin(), us.end());
+        pl.units.resize(units.size());
+        for (size_t i = 0; i < units.size(); ++i) pl.units[i] = units[order[i].second];
     }
 
     size_t off = 0;
@@ -196,7 +172,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
     pl.off_units = off;
     off = align_up(off + pl.units.size() * sizeof(UnitDev));
     pl.off_counters = off;
-    off = align_up(off + pl.groups.size() * sizeof(unsigned));
+    off = align_up(off + sizeof(unsigned));
     pl.off_data = off;
     pl.ws_bytes = off + data;
     return VX_OK;
@@ -225,7 +201,7 @@ vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t*
         e = cudaMemcpyAsync(base + pl.off_units, pl.units.data(), pl.units.size() * sizeof(UnitDev),
                             cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
-        e = cudaMemsetAsync(base + pl.off_counters, 0, pl.groups.size() * sizeof(unsigned), stream);
+        e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return cuda_fail(e, "uploading the batch plan");
 
     const PairDev* d_pairs = reinterpret_cast<const PairDev*>(base + pl.off_pairs);
@@ -237,12 +213,9 @@ vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t*
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) cudaEventRecord(ev[1], stream);
-    for (size_t g = 0; g < pl.groups.size(); ++g) {
-        const auto& gr = pl.groups[g];
-        e = launch_aggregate(gr.variant, d_pairs, d_jobs, d_units + gr.unit_begin, gr.unit_count,
-                             counters + g, 0, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
-    }
+    e = launch_aggregate(pl.dp_max, pl.census64, d_pairs, d_jobs, d_units, (int)pl.units.size(),
+                         counters, 0, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) cudaEventRecord(ev[2], stream);
     e = launch_wta(d_pairs, n, pl.total_rows, pl.max_width, stream);
     if (e != cudaSuccess) return cuda_fail(e, "WTA launch");

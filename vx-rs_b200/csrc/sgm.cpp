@@ -71,13 +71,13 @@ vx_status vx_sgm_create(vx_ctx* ctx, vx_sgm** out) {
     // (sgm.rs:73-105); the equivalent check is that this library's sm_100a
     // kernel images load on the device.
     cudaError_t e = prepare_wta_kernel();
+    if (e == cudaSuccess) e = prepare_aggregate_kernels();
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(VX_ERR_SHADER_MISSING, "SGM kernels unavailable on device %d: %s", ctx->device,
                     cudaGetErrorString(e));
     }
-    AggVariant probe{128, true, false, false};
-    if (aggregate_grid_ctas(probe) <= 0) {
+    if (aggregate_grid_ctas(256, true) <= 0) {
         cudaGetLastError();
         return fail(VX_ERR_PIPELINE_COMPILE, "aggregation kernel has no occupancy on device %d",
                     ctx->device);
@@ -118,7 +118,10 @@ size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_conf
     const size_t ct = census_bits(*cfg) > 32 ? 8 : 4;
     const size_t dp = (cfg->num_disparities + 7) / 8 * 8;
     auto al = [](size_t v) { return (v + 255) / 256 * 256; };
-    return 4 * al(npx * ct) + al(npx * dp * cfg->num_paths * sizeof(uint16_t));
+    const size_t banded = (size_t)((height + 31) / 32) * 32 * width * ct;
+    const size_t guard = kCensusGuardWords * ct;
+    return 2 * al(npx * ct + 2 * guard) + 2 * al(banded) +
+           al(npx * dp * cfg->num_paths * sizeof(uint16_t));
 }
 
 vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,

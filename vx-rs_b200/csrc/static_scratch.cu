@@ -22,8 +22,8 @@
 //    different host threads without ordering) race on it. The work-queue
 //    counters that must start at zero are cleared on the stream by every call.
 //  * The first call on a device does the set-up for that device (the
-//    scratch's device address via cudaGetSymbolAddress, the WTA kernel's
-//    shared-memory limit); make that first call before any stream capture.
+//    scratch's device address via cudaGetSymbolAddress, the kernels'
+//    shared-memory limits); make that first call before any stream capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -56,7 +56,8 @@ vx_status scratch_for_current_device(char** out) {
         e = cudaGetSymbolAddress(&p, g_sgm_static_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "locating the static scratch on the device");
         e = prepare_wta_kernel();
-        if (e != cudaSuccess) return cuda_fail(e, "configuring the WTA kernel");
+        if (e == cudaSuccess) e = prepare_aggregate_kernels();
+        if (e != cudaSuccess) return cuda_fail(e, "configuring the SGM kernels");
         g_scratch_addr[dev] = static_cast<char*>(p);
     }
     *out = g_scratch_addr[dev];

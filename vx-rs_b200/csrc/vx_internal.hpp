@@ -87,13 +87,9 @@ int census_bits(const vx_sgm_config& cfg);
 struct Plan {
     std::vector<PairDev> pairs;     // pointers relative to the workspace base until bound
     std::vector<JobDev> jobs;
-    std::vector<UnitDev> units;     // all groups, concatenated
-    struct Group {
-        AggVariant variant;
-        int unit_begin, unit_count;
-    };
-    std::vector<Group> groups;
+    std::vector<UnitDev> units;     // all (pair, path, scanline-group) units, longest first
     bool census64 = false;
+    int dp_max = 8;                 // largest padded disparity count
     int total_tiles = 0, total_rows = 0, max_width = 0, max_rx = 0, max_ry = 0;
     // Workspace layout (byte offsets from the workspace base).
     size_t off_pairs = 0, off_jobs = 0, off_units = 0, off_counters = 0, off_data = 0;

@@ -69,7 +69,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         if (act) {
             const size_t off = ((size_t)y * W + x) * Dp + 8 * c;
             for (int p = 0; p < P; ++p) {
-                const uint4 v = *reinterpret_cast<const uint4*>(pr.slabs + pr.slab_stride * p + off);
+                const uint4 v = __ldcs(reinterpret_cast<const uint4*>(pr.slabs + pr.slab_stride * p + off));
                 s[0] += v.x & 0xFFFFu; s[1] += v.x >> 16;
                 s[2] += v.y & 0xFFFFu; s[3] += v.y >> 16;
                 s[4] += v.z & 0xFFFFu; s[5] += v.z >> 16;
