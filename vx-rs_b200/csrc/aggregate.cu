@@ -25,10 +25,11 @@
 // wrapping add for Lp[d+1] + P1).
 //
 // Mapping. One thread owns one scanline. Its D state values (packed u16 pairs)
-// live in warp-private shared memory as [group of 8 d][lane] 16-byte words, so a
-// warp's access to one group is 512 contiguous bytes (conflict-free) and the
-// per-pixel loop runs over groups with a small loop body and a runtime D: one
-// kernel serves every D of a batch. A warp takes 32 neighbouring scanlines of
+// live in tensor memory (TMEM): the thread's TMEM lane, one 32-bit column per
+// pair, read and written 4 columns (8 disparities) at a time by warp-collective
+// tcgen05.ld/st. The per-pixel loop runs over groups of 8 disparities with a
+// small loop body and a runtime D, so one kernel serves every D of a batch, and
+// shared memory is left almost entirely to L1 for the census windows. A warp takes 32 neighbouring scanlines of
 // one (pair, path):
 //  * vertical / diagonal paths: the 32 lanes sit on 32 consecutive pixels of one
 //    row at every step, so the right-census words they need form one segment of
@@ -70,6 +71,34 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
 __device__ __forceinline__ void cp_async_wait_1() {
     asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+// Tensor-memory (TMEM) access for the per-scanline state. Warp w of the CTA owns
+// TMEM lanes 32w..32w+31 (one lane per thread) and the CTA's allocated columns;
+// the 8 disparities of group g are columns 4g..4g+3 (one u16 pair per column).
+// tcgen05.ld is asynchronous: its registers are threaded through the wait so
+// that no use can be scheduled before the data has arrived.
+__device__ __forceinline__ uint4 tmem_ld4(uint32_t taddr) {
+    uint4 r;
+    __syncwarp();  // .sync.aligned: the whole warp, converged
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "r"(taddr));
+    return r;
+}
+__device__ __forceinline__ void tmem_wait_ld(uint4& r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r.x), "+r"(r.y), "+r"(r.z), "+r"(r.w)::"memory");
+}
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint4 v) {
+    __syncwarp();
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
+                 "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+    __syncwarp();
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // Per-scanline constants of one unit.
@@ -140,17 +169,20 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
     return make_uint4(out[0], out[1], out[2], out[3]);
 }
 
-// One pixel: Lsm = this lane's state words (group g at Lsm[g * 32]).
-// getR(d) = right census at x-d; it is only called with x-d >= 0 when CHECK.
-// prefetch(d) hints the census word at x-d into L1 (horizontal paths).
-// Software pipeline over groups (loop unrolled by two, register sets in
+// One pixel of the 32 scanlines of a warp (all lanes execute it: the TMEM
+// accesses are warp-collective). tstate = this warp's TMEM address (lane field
+// = its first lane, column 0). getR(d) = right census at x-d; only called with
+// x-d >= 0 when CHECK. prefetch(d) hints census words into L1 (horizontal
+// paths). active: this lane's scanline covers the pixel; an idle lane stores
+// nothing to its slab and keeps (or resets to) the zero state a scanline starts
+// from. Software pipeline over groups (loop unrolled by two, register sets in
 // ping-pong): while group g runs its min/add chain, the census words and state
 // of group g+1 are in flight, and g+1's costs are formed right after g's chain,
 // so neither load nor popcount latency sits on the chain.
 template <bool CHECK, typename CT, typename GetR, typename Prefetch>
-__device__ __forceinline__ void sgm_pixel(uint4* __restrict__ Lsm, uint32_t& m, const CT lc,
+__device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
                                           const GetR& getR, const Prefetch& prefetch,
-                                          const int x, const ScanConst& k,
+                                          const int x, const bool active, const ScanConst& k,
                                           uint16_t* __restrict__ dst) {
     PixelState ps;
     const uint32_t o3 = (m + k.P2) & 0xFFFFu;
@@ -167,40 +199,43 @@ __device__ __forceinline__ void sgm_pixel(uint4* __restrict__ Lsm, uint32_t& m, 
             r[i] = (!CHECK || x - d >= 0) ? getR(d) : CT(0);
         }
     };
-    // Slab stores are streaming (evict-first): slabs are written once here and
-    // read once by the WTA kernel, and must not push the census planes, which
-    // every path re-reads, out of L2.
-    auto store = [&](const uint4 o, int g) {
-        Lsm[g * 32] = o;
-        __stcs(reinterpret_cast<uint4*>(dst + 8 * g), o);
+    auto store = [&](uint4 o, int g) {
+        if (active) __stcs(reinterpret_cast<uint4*>(dst + 8 * g), o);
+        else o = make_uint4(0u, 0u, 0u, 0u);
+        tmem_st4(tstate + 4 * g, o);
     };
     CT ra[8], rb[8];
     uint32_t ca[8], cb[8];
     load(ra, 0);
-    uint4 sa = Lsm[0], sb;
+    uint4 sa = tmem_ld4(tstate), sb;
     group_costs<CHECK>(ca, lc, ra, x, 0);
+    tmem_wait_ld(sa);
     int g = 0;
 #pragma unroll 1
     for (; g + 2 < k.G; g += 2) {
-        sb = Lsm[(g + 1) * 32];
+        sb = tmem_ld4(tstate + 4 * (g + 1));
         load(rb, g + 1);
+        tmem_wait_ld(sb);
         store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
         group_costs<CHECK>(cb, lc, rb, x, g + 1);
-        sa = Lsm[(g + 2) * 32];
+        sa = tmem_ld4(tstate + 4 * (g + 2));
         load(ra, g + 2);
+        tmem_wait_ld(sa);
         store(sgm_group<false>(sb, sa.x, cb, k, ps), g + 1);
         group_costs<CHECK>(ca, lc, ra, x, g + 2);
     }
     if (g + 1 < k.G) {
-        sb = Lsm[(g + 1) * 32];
+        sb = tmem_ld4(tstate + 4 * (g + 1));
         load(rb, g + 1);
+        tmem_wait_ld(sb);
         store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
         group_costs<CHECK>(cb, lc, rb, x, g + 1);
         store(sgm_group<true>(sb, 0u, cb, k, ps), g + 1);
     } else {
         store(sgm_group<true>(sa, 0u, ca, k, ps), g);
     }
-    m = min(ps.mn & 0xFFFFu, ps.mn >> 16);
+    tmem_wait_st();            // the next pixel reads this state back
+    m = active ? min(ps.mn & 0xFFFFu, ps.mn >> 16) : 0u;
 }
 
 __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
@@ -214,14 +249,15 @@ __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
     return k;
 }
 
-__device__ __forceinline__ void clear_state(uint4* Lsm, int G) {
-    for (int g = 0; g < G; ++g) Lsm[g * 32] = make_uint4(0u, 0u, 0u, 0u);
+__device__ __forceinline__ void clear_state(uint32_t tstate, int G) {
+    for (int g = 0; g < G; ++g) tmem_st4(tstate + 4 * g, make_uint4(0u, 0u, 0u, 0u));
+    tmem_wait_st();
 }
 
 // Unit = 32 scanlines of a vertical or diagonal path.
 template <typename CT>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
-                                                  uint4* __restrict__ Lsm, CT* __restrict__ stage,
+                                                  uint32_t tstate, CT* __restrict__ stage,
                                                   int seg_words) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
@@ -272,7 +308,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         return (int)(ls - (ls & ~(ptrdiff_t)(kPerChunk - 1)));
     };
 
-    clear_state(Lsm, k.G);
+    clear_state(tstate, k.G);
     uint32_t m = 0u;
     stage_step(t_lo, t_lo & 1);
     CT lc_next = CT(0);
@@ -292,13 +328,11 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         auto getR = [seg](int d) { return seg[-d]; };
         auto no_prefetch = [](int) {};
         const int xb = k0 + dx * t;             // smallest x of the warp
-        if (active) {
-            uint16_t* dst = out + ((size_t)y * W + x) * Dp;
-            if (xb >= Dp - 1)
-                sgm_pixel<false, CT>(Lsm, m, lc, getR, no_prefetch, x, k, dst);
-            else
-                sgm_pixel<true, CT>(Lsm, m, lc, getR, no_prefetch, x, k, dst);
-        }
+        uint16_t* dst = active ? out + ((size_t)y * W + x) * Dp : out;
+        if (xb >= Dp - 1)
+            sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, dst);
+        else
+            sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, dst);
         __syncwarp();
     }
 }
@@ -306,7 +340,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
 // Unit = 32 rows of a horizontal path (column-major census).
 template <typename CT>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job,
-                                                    int first, uint4* __restrict__ Lsm) {
+                                                    int first, uint32_t tstate) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
@@ -324,7 +358,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
     (void)H;
 
-    clear_state(Lsm, k.G);
+    clear_state(tstate, k.G);
     uint32_t m = 0u;
     const int x0 = dx > 0 ? 0 : W - 1;
     CT lc_next = CL[(size_t)x0 * 32];
@@ -344,13 +378,11 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
                         asm volatile("prefetch.global.L1 [%0];" ::"l"(col - 32 * (d0 + i)));
             }
         };
-        if (active) {
-            uint16_t* dst = out + ((size_t)yc * W + x) * Dp;
-            if (x >= Dp - 1)
-                sgm_pixel<false, CT>(Lsm, m, lc, getR, prefetch, x, k, dst);
-            else
-                sgm_pixel<true, CT>(Lsm, m, lc, getR, prefetch, x, k, dst);
-        }
+        uint16_t* dst = out + ((size_t)yc * W + x) * Dp;
+        if (x >= Dp - 1)
+            sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, dst);
+        else
+            sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, dst);
     }
 }
 
@@ -358,15 +390,26 @@ template <typename CT>
 __global__ void __launch_bounds__(kAggWarpsPerBlock * 32)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
-                 int dp_max) {
+                 int dp_max, int tmem_cols) {
     extern __shared__ __align__(16) unsigned char agg_smem[];
+    __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg_words = dp_max + 40;                          // Dp+31 words + alignment
-    const size_t state_bytes = (size_t)dp_max * 64;             // [dp_max/8][32] uint4
-    const size_t warp_bytes = state_bytes + 2 * seg_words * sizeof(CT);
-    unsigned char* base = agg_smem + warp * warp_bytes;
-    uint4* Lsm = reinterpret_cast<uint4*>(base) + lane;
-    CT* stage = reinterpret_cast<CT*>(base + state_bytes);
+    CT* stage = reinterpret_cast<CT*>(agg_smem) + (size_t)warp * 2 * seg_words;
+
+    // TMEM for the state of the CTA's 4 x 32 scanlines: allocated by warp 0 for
+    // the whole persistent loop and released by warp 0 after every warp is done.
+    if (warp == 0) {
+        const unsigned slot = (unsigned)__cvta_generic_to_shared(&tmem_base);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tstate = tmem_base + ((uint32_t)(32 * warp) << 16);
+
     for (;;) {
         int u = 0;
         if (lane == 0) u = (int)atomicAdd(counter, 1u);
@@ -376,10 +419,18 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT>(pr, job, unit.first_scanline, Lsm);
+            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate);
         else
-            run_vertical_unit<CT>(pr, job, unit.first_scanline, Lsm, stage, seg_words);
+            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words);
         __syncwarp();
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(tmem_cols));
     }
 }
 
@@ -387,18 +438,18 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
 
 size_t aggregate_smem_bytes(int dp_max, bool census64) {
     const size_t ct = census64 ? 8 : 4;
-    return (size_t)kAggWarpsPerBlock * ((size_t)dp_max * 64 + 2 * (dp_max + 40) * ct);
+    return (size_t)kAggWarpsPerBlock * 2 * (dp_max + 40) * ct;
 }
 
-cudaError_t prepare_aggregate_kernels() {
-    const int max_bytes = (int)aggregate_smem_bytes(256, true);
-    cudaError_t e = cudaFuncSetAttribute(aggregate_kernel<uint32_t>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(aggregate_kernel<uint64_t>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
-    return e;
+// TMEM columns per CTA: one 32-bit column per u16 pair of the largest D,
+// rounded up to a power of two (the allocation unit), at least 32.
+int aggregate_tmem_cols(int dp_max) {
+    int cols = 32;
+    while (cols < dp_max / 2) cols <<= 1;
+    return cols;
 }
+
+cudaError_t prepare_aggregate_kernels() { return cudaSuccess; }
 
 int aggregate_grid_ctas(int dp_max, bool census64) {
     int dev = 0, sms = 0, per_sm = 0;
@@ -411,7 +462,11 @@ int aggregate_grid_ctas(int dp_max, bool census64) {
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aggregate_kernel<uint32_t>,
                                                       kAggWarpsPerBlock * 32, smem);
-    return sms * (per_sm > 0 ? per_sm : 1);
+    // Never more resident CTAs per SM than the 512 TMEM columns can serve.
+    const int tmem_ctas = 512 / aggregate_tmem_cols(dp_max);
+    per_sm = per_sm > 0 ? per_sm : 1;
+    if (per_sm > tmem_ctas) per_sm = tmem_ctas;
+    return sms * per_sm;
 }
 
 cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
@@ -422,13 +477,14 @@ cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
     const int needed = (num_units + kAggWarpsPerBlock - 1) / kAggWarpsPerBlock;
     if (grid_ctas > needed) grid_ctas = needed;
     const size_t smem = aggregate_smem_bytes(dp_max, census64);
+    const int cols = aggregate_tmem_cols(dp_max);
     count_launch();
     if (census64)
         aggregate_kernel<uint64_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max);
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max, cols);
     else
         aggregate_kernel<uint32_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max);
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max, cols);
     return cudaGetLastError();
 }
 
