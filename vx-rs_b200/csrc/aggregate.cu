@@ -45,6 +45,10 @@
 // into this path's slab.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+
 #include "kernels.cuh"
 #include "launch.hpp"
 
@@ -129,6 +133,24 @@ __device__ __forceinline__ void group_costs(uint32_t (&c)[8], const CT lc, const
     }
 }
 
+// Writes the warp's output tile to the slab: lanes [la, lb] hold the results of
+// one pixel step; lane row p's vector goes to dst0 + p * stride (in u16), and
+// 16-byte word g of it to +8g. Words are distributed over the lanes in address
+// order, so that consecutive lanes write consecutive 16 bytes of a vector
+// (streaming stores: slabs are read once by the WTA kernel and must not push
+// the census planes, which every path re-reads, out of L2).
+__device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int row_words, int G,
+                                           int la, int lb, uint16_t* __restrict__ dst0,
+                                           size_t stride, int lane) {
+    __syncwarp();
+    const int n = (lb - la + 1) * G;
+    for (int c = lane; c < n; c += 32) {
+        const int p = la + c / G, g = c % G;
+        __stcs(reinterpret_cast<uint4*>(dst0 + (size_t)p * stride + 8 * g), tile[p * row_words + g]);
+    }
+    __syncwarp();
+}
+
 // One group of 8 disparities d = 8g..8g+7 of one pixel. cur = old state words of
 // the group, nxt_lo = old Lp[8g+8] in the low half (unused for the last group),
 // c = the group's matching costs. LAST: the group holding d = D-1, whose o2 is
@@ -173,9 +195,9 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
 // accesses are warp-collective). tstate = this warp's TMEM address (lane field
 // = its first lane, column 0). getR(d) = right census at x-d; only called with
 // x-d >= 0 when CHECK. prefetch(d) hints census words into L1 (horizontal
-// paths). active: this lane's scanline covers the pixel; an idle lane stores
-// nothing to its slab and keeps (or resets to) the zero state a scanline starts
-// from. Software pipeline over groups (loop unrolled by two, register sets in
+// paths). active: this lane's scanline covers the pixel; an idle lane keeps (or
+// resets to) the zero state a scanline starts from. otile = this lane's row of
+// the warp's shared-memory output tile (one 16-byte word per group). Software pipeline over groups (loop unrolled by two, register sets in
 // ping-pong): while group g runs its min/add chain, the census words and state
 // of group g+1 are in flight, and g+1's costs are formed right after g's chain,
 // so neither load nor popcount latency sits on the chain.
@@ -183,7 +205,7 @@ template <bool CHECK, typename CT, typename GetR, typename Prefetch>
 __device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
                                           const GetR& getR, const Prefetch& prefetch,
                                           const int x, const bool active, const ScanConst& k,
-                                          uint16_t* __restrict__ dst) {
+                                          uint4* __restrict__ otile) {
     PixelState ps;
     const uint32_t o3 = (m + k.P2) & 0xFFFFu;
     ps.o3x2 = o3 | (o3 << 16);
@@ -199,9 +221,11 @@ __device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, co
             r[i] = (!CHECK || x - d >= 0) ? getR(d) : CT(0);
         }
     };
+    // Results go to this lane's row of the warp's output tile (written to the
+    // slab, coalesced, by flush_tile); idle lanes keep a zero state.
     auto store = [&](uint4 o, int g) {
-        if (active) __stcs(reinterpret_cast<uint4*>(dst + 8 * g), o);
-        else o = make_uint4(0u, 0u, 0u, 0u);
+        otile[g] = o;
+        if (!active) o = make_uint4(0u, 0u, 0u, 0u);
         tmem_st4(tstate + 4 * g, o);
     };
     CT ra[8], rb[8];
@@ -258,7 +282,8 @@ __device__ __forceinline__ void clear_state(uint32_t tstate, int G) {
 template <typename CT>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
                                                   uint32_t tstate, CT* __restrict__ stage,
-                                                  int seg_words) {
+                                                  int seg_words, uint4* __restrict__ tile,
+                                                  int row_words) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
@@ -328,11 +353,18 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         auto getR = [seg](int d) { return seg[-d]; };
         auto no_prefetch = [](int) {};
         const int xb = k0 + dx * t;             // smallest x of the warp
-        uint16_t* dst = active ? out + ((size_t)y * W + x) * Dp : out;
+        uint4* otile = tile + lane * row_words;
         if (xb >= Dp - 1)
-            sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, dst);
+            sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
         else
-            sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, dst);
+            sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
+        // Active lanes are one run of consecutive pixels of row y.
+        const unsigned act = __ballot_sync(kFull, active);
+        if (act) {
+            const int la = __ffs(act) - 1, lb = 31 - __clz(act);
+            flush_tile(tile, row_words, k.G, la, lb, out + ((size_t)y * W + xb) * Dp, (size_t)Dp,
+                       lane);
+        }
         __syncwarp();
     }
 }
@@ -340,7 +372,8 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
 // Unit = 32 rows of a horizontal path (column-major census).
 template <typename CT>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job,
-                                                    int first, uint32_t tstate) {
+                                                    int first, uint32_t tstate,
+                                                    uint4* __restrict__ tile, int row_words) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
@@ -348,10 +381,11 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const int dx = job.dx;
     const int y = first + lane;                 // row of this lane
     const bool active = y < job.num_scanlines;
-    const int yc = active ? y : first;          // keeps idle lanes' addresses in bounds
+    const int nrows = min(32, job.num_scanlines - first);
     // Banded census: word (x, y) at ((y / 32) * W + x) * 32 + y % 32, so the 32
     // rows of this unit (first is a multiple of 32) read 128 contiguous bytes per
-    // column and column x-d sits at a constant offset of -32*d words.
+    // column and column x-d sits at a constant offset of -32*d words. Bands are
+    // allocated whole, so idle lanes (rows >= H) read allocated words.
     const size_t band = (size_t)(first >> 5) * W;
     const CT* __restrict__ CL = static_cast<const CT*>(pr.census_lt) + band * 32 + lane;
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_rt) + band * 32 + lane;
@@ -378,27 +412,42 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
                         asm volatile("prefetch.global.L1 [%0];" ::"l"(col - 32 * (d0 + i)));
             }
         };
-        uint16_t* dst = out + ((size_t)yc * W + x) * Dp;
+        uint4* otile = tile + lane * row_words;
         if (x >= Dp - 1)
-            sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, dst);
+            sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
         else
-            sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, dst);
+            sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
+        // Rows first..first+nrows-1, one vector per row at column x.
+        flush_tile(tile, row_words, k.G, 0, nrows - 1, out + ((size_t)first * W + x) * Dp,
+                   (size_t)W * Dp, lane);
     }
 }
 
+// Shared memory per warp: the census staging buffers (2 x (Dp+40) words) and
+// the output tile (32 rows of Dp/8 + 1 16-byte words; the pad word keeps the
+// rows' 16-byte stores on distinct banks).
+__host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, size_t ct) {
+    return 2 * (size_t)(dp_max + 40) * ct + (size_t)32 * (dp_max / 8 + 1) * 16;
+}
+
 template <typename CT>
-__global__ void __launch_bounds__(kAggWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kAggMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
-                 int dp_max, int tmem_cols) {
+                 int dp_max, int tmem_cols, int wg_cols) {
     extern __shared__ __align__(16) unsigned char agg_smem[];
     __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg_words = dp_max + 40;                          // Dp+31 words + alignment
-    CT* stage = reinterpret_cast<CT*>(agg_smem) + (size_t)warp * 2 * seg_words;
+    const int row_words = dp_max / 8 + 1;                       // tile row: Dp/8 words + pad
+    unsigned char* wbase = agg_smem + (size_t)warp * aggregate_warp_smem(dp_max, sizeof(CT));
+    CT* stage = reinterpret_cast<CT*>(wbase);
+    uint4* tile = reinterpret_cast<uint4*>(wbase + 2 * seg_words * sizeof(CT));
 
-    // TMEM for the state of the CTA's 4 x 32 scanlines: allocated by warp 0 for
-    // the whole persistent loop and released by warp 0 after every warp is done.
+    // TMEM for the state of all the CTA's scanlines, allocated by warp 0 for the
+    // whole persistent loop and released by warp 0 after every warp is done.
+    // Warp w owns TMEM lanes 32*(w%4).. (its lane quarter) and, inside them, the
+    // columns of its warpgroup w/4: [ (w/4)*wg_cols, (w/4+1)*wg_cols ).
     if (warp == 0) {
         const unsigned slot = (unsigned)__cvta_generic_to_shared(&tmem_base);
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
@@ -408,7 +457,8 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tstate = tmem_base + ((uint32_t)(32 * warp) << 16);
+    const uint32_t tstate =
+        tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * wg_cols);
 
     for (;;) {
         int u = 0;
@@ -419,9 +469,10 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate);
+            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate, tile, row_words);
         else
-            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words);
+            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile,
+                                  row_words);
         __syncwarp();
     }
 
@@ -436,55 +487,99 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
 
 }  // namespace
 
-size_t aggregate_smem_bytes(int dp_max, bool census64) {
+// Launch shape of the aggregation kernel for a batch whose largest padded D is
+// dp_max: one CTA per SM (the CUDA occupancy calculator allows one CTA per SM
+// for a kernel that allocates tensor memory) with as many warpgroups as the
+// SM's 512 TMEM columns and registers hold. A warpgroup's 4 warps cover the
+// 128 TMEM lanes and need dp_max/2 columns.
+struct AggShape {
+    int warpgroups;
+    int wg_cols;     // columns per warpgroup
+    int tmem_cols;   // allocation (power of two >= warpgroups * wg_cols)
+    size_t smem;     // census staging
+};
+
+AggShape aggregate_shape(int dp_max, bool census64) {
+    AggShape sh{};
+    sh.wg_cols = dp_max / 2;
+    int by_tmem = 512 / sh.wg_cols;
+    int regs = 80, regs_sm = 65536, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, census64 ? (const void*)aggregate_kernel<uint64_t>
+                                            : (const void*)aggregate_kernel<uint32_t>) ==
+            cudaSuccess &&
+        fa.numRegs > 0)
+        regs = fa.numRegs;
+    cudaGetLastError();
+    const int by_regs = regs_sm / (regs * 128);
     const size_t ct = census64 ? 8 : 4;
-    return (size_t)kAggWarpsPerBlock * 2 * (dp_max + 40) * ct;
+    int smem_sm = 227 * 1024;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int by_smem = (int)(smem_sm / (4 * aggregate_warp_smem(dp_max, ct)));
+    sh.warpgroups = std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
+    int req = kAggDefaultWarpgroups;
+    if (const char* env = std::getenv("VX_SGM_AGG_WARPGROUPS")) req = std::atoi(env);
+    if (req >= 1) sh.warpgroups = std::min(req, sh.warpgroups);
+    sh.tmem_cols = 32;
+    while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
+    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, ct);
+    return sh;
 }
 
-// TMEM columns per CTA: one 32-bit column per u16 pair of the largest D,
-// rounded up to a power of two (the allocation unit), at least 32.
-int aggregate_tmem_cols(int dp_max) {
-    int cols = 32;
-    while (cols < dp_max / 2) cols <<= 1;
-    return cols;
+size_t aggregate_smem_bytes(int dp_max, bool census64) {
+    return aggregate_shape(dp_max, census64).smem;
 }
 
-cudaError_t prepare_aggregate_kernels() { return cudaSuccess; }
+cudaError_t prepare_aggregate_kernels() {
+    // Dynamic shared memory up to the largest staging area, and the smallest
+    // shared-memory carveout: the rest of the SM's L1 caches the census windows.
+    int dev = 0, max_bytes = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaError_t e = cudaSuccess;
+    for (const void* fn : {(const void*)aggregate_kernel<uint32_t>, (const void*)aggregate_kernel<uint64_t>}) {
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+        if (e == cudaSuccess)   // dynamic + static shared memory must fit the opt-in limit
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     max_bytes - (int)fa.sharedSizeBytes);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxL1);
+    }
+    return e;
+}
 
 int aggregate_grid_ctas(int dp_max, bool census64) {
-    int dev = 0, sms = 0, per_sm = 0;
+    (void)dp_max;
+    (void)census64;
+    int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = aggregate_smem_bytes(dp_max, census64);
-    if (census64)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aggregate_kernel<uint64_t>,
-                                                      kAggWarpsPerBlock * 32, smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aggregate_kernel<uint32_t>,
-                                                      kAggWarpsPerBlock * 32, smem);
-    // Never more resident CTAs per SM than the 512 TMEM columns can serve.
-    const int tmem_ctas = 512 / aggregate_tmem_cols(dp_max);
-    per_sm = per_sm > 0 ? per_sm : 1;
-    if (per_sm > tmem_ctas) per_sm = tmem_ctas;
-    return sms * per_sm;
+    return sms;
 }
 
 cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
                              const JobDev* d_jobs, const UnitDev* d_units, int num_units,
                              unsigned* counter, int grid_ctas, cudaStream_t stream) {
     if (num_units <= 0) return cudaSuccess;
+    const AggShape sh = aggregate_shape(dp_max, census64);
+    const int threads = sh.warpgroups * 128;
     if (grid_ctas <= 0) grid_ctas = aggregate_grid_ctas(dp_max, census64);
-    const int needed = (num_units + kAggWarpsPerBlock - 1) / kAggWarpsPerBlock;
+    const int needed = (num_units + threads / 32 - 1) / (threads / 32);
     if (grid_ctas > needed) grid_ctas = needed;
-    const size_t smem = aggregate_smem_bytes(dp_max, census64);
-    const int cols = aggregate_tmem_cols(dp_max);
+    if (std::getenv("VX_SGM_DEBUG"))
+        std::fprintf(stderr, "vx_sgm: aggregation %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
+                     grid_ctas, sh.warpgroups, sh.tmem_cols, sh.smem);
     count_launch();
     if (census64)
-        aggregate_kernel<uint64_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, cols);
+        aggregate_kernel<uint64_t><<<grid_ctas, threads, sh.smem, stream>>>(
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
     else
-        aggregate_kernel<uint32_t><<<grid_ctas, kAggWarpsPerBlock * 32, smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, cols);
+        aggregate_kernel<uint32_t><<<grid_ctas, threads, sh.smem, stream>>>(
+            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
     return cudaGetLastError();
 }
 
