@@ -107,7 +107,7 @@ void vx_sgm_config_new(vx_sgm_config* cfg, uint32_t num_disparities);
 /* Replaces SGMStereo::new(&ctx) (sgm.rs:73-105): checks that the sm_100a
  * kernel images load on the context's device (ShaderMissing otherwise). */
 vx_status vx_sgm_create(vx_ctx* ctx, vx_sgm** out);
-void vx_sgm_destroy(vx_sgm* sgm);
+void vx_sgm_destroy(vx_sgm* sgm);  /* before the context it was created with */
 
 /* Replaces SGMStereo::compute_disparity(&ctx, &left, &right, &output, &cfg)
  * (sgm.rs:108-265). left/right: U8 images of equal size; out_f32: F32 image
@@ -151,6 +151,29 @@ vx_status vx_sgm_compute_disparity_noalloc(const uint8_t* left, size_t left_pitc
                                            vx_stream stream);
 /* Size in bytes of the static scratch used by vx_sgm_compute_disparity_noalloc. */
 size_t vx_sgm_static_scratch_bytes(void);
+
+/* Autotuner (no reference counterpart): runs this batch once per candidate
+ * launch shape of the path-aggregation kernel (warpgroups per CTA), `iterations`
+ * timed runs each (CUDA events on the context's stream, one untimed run first),
+ * and records the fastest for batches with the same key (largest padded D,
+ * census word width, log2 of the queued scanline units). Outputs are written
+ * like vx_sgm_compute_batch. best_* may be NULL. Synchronous. */
+vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
+                                const vx_image* const* right, vx_image* const* out_f32,
+                                vx_image* const* out_i16, const vx_sgm_config* cfgs,
+                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms);
+/* Persist / restore the autotuned table as JSON. */
+vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path);
+vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path);
+
+/* CUDA graphs per shape bucket (no reference counterpart). With max_buckets
+ * > 0, vx_sgm_compute_batch / compute_disparity keep, per bucket (the ordered
+ * list of the pairs' sizes and configs), a resident workspace and a captured
+ * graph of the launch sequence; a call of a known bucket refreshes the pair
+ * table and launches the graph. At most max_buckets buckets are kept (least
+ * recently used first out); 0 disables the cache and frees it. Calls of one
+ * bucket share its workspace, so they must be ordered on one stream. */
+vx_status vx_sgm_set_graph_cache(vx_sgm* sgm, uint32_t max_buckets);
 
 /* Device bytes of intermediate state one pair needs (census + path slabs). */
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg);

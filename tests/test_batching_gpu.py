@@ -1,0 +1,91 @@
+"""Batched path on the GPU: CUDA graphs per shape bucket and the autotuner give
+the same results as the plain batched call (bit for bit)."""
+import os
+
+import numpy as np
+import pytest
+
+import vx_sgm
+from gpu_helpers import assert_disparity_equal, run_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _pairs(n, seed):
+    rng = np.random.default_rng(seed)
+    pairs, cfgs = [], []
+    for i in range(n):
+        w, h = int(rng.choice([96, 160, 211])), int(rng.choice([64, 90, 120]))
+        nd = int(rng.choice([32, 64, 128]))
+        L, R, _ = vx_sgm.synth_pair(i % 3, w, h, 2, nd - 4, seed * 100 + i)
+        pairs.append((L, R))
+        cfgs.append(vx_sgm.SGMStereoConfig(num_disparities=nd, census_radius_x=2, census_radius_y=2,
+                                           num_paths=8, lr_check=True))
+    return pairs, cfgs
+
+
+def _textures(ctx, pairs):
+    tl = [ctx.texture_gray8(L, L.shape[1], L.shape[0]) for L, _ in pairs]
+    tr = [ctx.texture_gray8(R, R.shape[1], R.shape[0]) for _, R in pairs]
+    of = [ctx.texture_output_r32float(L.shape[1], L.shape[0]) for L, _ in pairs]
+    oi = [ctx.texture_output_i16(L.shape[1], L.shape[0]) for L, _ in pairs]
+    return tl, tr, of, oi
+
+
+def test_graph_cache_matches_plain_batch(gpu_ctx):
+    pairs, cfgs = _pairs(6, 7)
+    plain_sgm = vx_sgm.SGMStereo(gpu_ctx)
+    want = run_batch(gpu_ctx, plain_sgm, pairs, cfgs)
+    sgm = vx_sgm.SGMStereo(gpu_ctx)
+    sgm.set_graph_cache(2)
+    tl, tr, of, oi = _textures(gpu_ctx, pairs)
+    for _ in range(3):  # capture, then replays
+        sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)
+        for (f, i), w in zip([(f.read_r32float(), i.download()) for f, i in zip(of, oi)], want):
+            assert_disparity_equal((f, i), w, tol=0.0, what="graph replay")
+    # same bucket, new images and outputs: the pair table is rebound
+    pairs2, _ = _pairs(6, 7)
+    pairs2 = [(np.ascontiguousarray(R), np.ascontiguousarray(L)) for L, R in pairs2]  # other content
+    want2 = run_batch(gpu_ctx, plain_sgm, pairs2, cfgs)
+    tl2, tr2, of2, oi2 = _textures(gpu_ctx, pairs2)
+    sgm.compute_batch(gpu_ctx, tl2, tr2, of2, cfgs, outputs_i16=oi2)
+    for f, i, w in zip(of2, oi2, want2):
+        assert_disparity_equal((f.read_r32float(), i.download()), w, tol=0.0, what="graph rebind")
+    # other buckets evict the least recently used one; results stay exact
+    for seed in (8, 9):
+        p, c = _pairs(3, seed)
+        t = _textures(gpu_ctx, p)
+        sgm.compute_batch(gpu_ctx, t[0], t[1], t[2], c, outputs_i16=t[3])
+        w = run_batch(gpu_ctx, plain_sgm, p, c)
+        for f, i, ww in zip(t[2], t[3], w):
+            assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="evict")
+    sgm.set_graph_cache(0)
+    sgm.close()
+    plain_sgm.close()
+
+
+def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
+    pairs, cfgs = _pairs(5, 11)
+    sgm = vx_sgm.SGMStereo(gpu_ctx)
+    want = run_batch(gpu_ctx, sgm, pairs, cfgs)
+    tl, tr, of, oi = _textures(gpu_ctx, pairs)
+    w, ms = sgm.autotune_batch(gpu_ctx, tl, tr, of, cfgs, oi, iterations=1)
+    assert w >= 1 and ms > 0
+    for f, i, ww in zip(of, oi, want):
+        assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="autotune run")
+    sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)  # uses the tuned shape
+    for f, i, ww in zip(of, oi, want):
+        assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="tuned batch")
+    path = os.path.join(tmp_path, "tuning.json")
+    sgm.tuning_save(path)
+    text = open(path).read()
+    assert f'"warpgroups": {w}' in text
+    other = vx_sgm.SGMStereo(gpu_ctx)
+    other.tuning_load(path)
+    other.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)
+    for f, i, ww in zip(of, oi, want):
+        assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="loaded tuning")
+    with pytest.raises(vx_sgm.VxError):
+        other.tuning_load(os.path.join(tmp_path, "missing.json"))
+    other.close()
+    sgm.close()

@@ -499,13 +499,15 @@ struct AggShape {
     size_t smem;     // census staging
 };
 
-AggShape aggregate_shape(int dp_max, bool census64) {
-    AggShape sh{};
-    sh.wg_cols = dp_max / 2;
-    int by_tmem = 512 / sh.wg_cols;
-    int regs = 80, regs_sm = 65536, dev = 0;
+// Largest number of warpgroups one aggregation CTA can hold for this batch:
+// bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
+int aggregate_max_warpgroups(int dp_max, bool census64) {
+    const int wg_cols = dp_max / 2;
+    const int by_tmem = 512 / wg_cols;
+    int regs = 80, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
     if (cudaFuncGetAttributes(&fa, census64 ? (const void*)aggregate_kernel<uint64_t>
                                             : (const void*)aggregate_kernel<uint32_t>) ==
@@ -514,22 +516,32 @@ AggShape aggregate_shape(int dp_max, bool census64) {
         regs = fa.numRegs;
     cudaGetLastError();
     const int by_regs = regs_sm / (regs * 128);
-    const size_t ct = census64 ? 8 : 4;
-    int smem_sm = 227 * 1024;
-    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int by_smem = (int)(smem_sm / (4 * aggregate_warp_smem(dp_max, ct)));
-    sh.warpgroups = std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
-    int req = kAggDefaultWarpgroups;
-    if (const char* env = std::getenv("VX_SGM_AGG_WARPGROUPS")) req = std::atoi(env);
-    if (req >= 1) sh.warpgroups = std::min(req, sh.warpgroups);
-    sh.tmem_cols = 32;
-    while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
-    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, ct);
-    return sh;
+    const int by_smem = (int)((smem_sm - 1024) / (4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4)));
+    return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
 }
 
-size_t aggregate_smem_bytes(int dp_max, bool census64) {
-    return aggregate_shape(dp_max, census64).smem;
+int aggregate_default_warpgroups(int dp_max, bool census64, int num_units) {
+    // Most warpgroups that still leave every warp ~2.5 units of the queue: a
+    // scanline is serial work, so a crowded SM slows the longest units down and
+    // few units per warp cannot even that out.
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int wmax = aggregate_max_warpgroups(dp_max, census64);
+    int w = 1;
+    while (w < wmax && (double)num_units >= 2.5 * sms * 4 * (w + 1)) ++w;
+    return w;
+}
+
+AggShape aggregate_shape(int dp_max, bool census64, int warpgroups) {
+    AggShape sh{};
+    sh.wg_cols = dp_max / 2;
+    const int wmax = aggregate_max_warpgroups(dp_max, census64);
+    sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
+    sh.tmem_cols = 32;
+    while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
+    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4);
+    return sh;
 }
 
 cudaError_t prepare_aggregate_kernels() {
@@ -561,13 +573,14 @@ int aggregate_grid_ctas(int dp_max, bool census64) {
     return sms;
 }
 
-cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
+cudaError_t launch_aggregate(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs,
                              const JobDev* d_jobs, const UnitDev* d_units, int num_units,
-                             unsigned* counter, int grid_ctas, cudaStream_t stream) {
+                             unsigned* counter, cudaStream_t stream) {
     if (num_units <= 0) return cudaSuccess;
-    const AggShape sh = aggregate_shape(dp_max, census64);
+    if (warpgroups <= 0) warpgroups = aggregate_default_warpgroups(dp_max, census64, num_units);
+    const AggShape sh = aggregate_shape(dp_max, census64, warpgroups);
     const int threads = sh.warpgroups * 128;
-    if (grid_ctas <= 0) grid_ctas = aggregate_grid_ctas(dp_max, census64);
+    int grid_ctas = aggregate_grid_ctas(dp_max, census64);
     const int needed = (num_units + threads / 32 - 1) / (threads / 32);
     if (grid_ctas > needed) grid_ctas = needed;
     if (std::getenv("VX_SGM_DEBUG"))

@@ -1,0 +1,154 @@
+// In-house autotuner of the aggregation launch shape.
+//
+// The path-aggregation kernel runs one CTA per SM holding 1..N warpgroups (each
+// scanline is serial work: more warps per SM raise throughput until the
+// longest scanlines, slowed by a crowded SM, dominate). The best count depends
+// on the batch: its largest disparity count, its census word width and how many
+// 32-scanline units it queues. vx_sgm_autotune_batch times every candidate on
+// a real batch with CUDA events around the aggregation launch and records the
+// fastest in the SGMStereo handle; later batches with the same key use it. The
+// table is saved to / loaded from a small JSON file.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <vector>
+
+#include "vx_internal.hpp"
+
+namespace vxsgm {
+
+TuneKey tune_key(const Plan& plan) {
+    TuneKey k;
+    k.dp_max = plan.dp_max;
+    k.census64 = plan.census64 ? 1 : 0;
+    k.units_log2 = plan.units.empty() ? 0 : (int)std::floor(std::log2((double)plan.units.size()));
+    return k;
+}
+
+}  // namespace vxsgm
+
+using namespace vxsgm;
+
+int vx_sgm::warpgroups_for(const Plan& plan) {
+    std::lock_guard<std::mutex> lk(tune_mu);
+    auto it = tuned.find(tune_key(plan));
+    return it == tuned.end() ? 0 : it->second.warpgroups;
+}
+
+extern "C" {
+
+vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
+                                const vx_image* const* right, vx_image* const* out_f32,
+                                vx_image* const* out_i16, const vx_sgm_config* cfgs,
+                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms) {
+    if (!sgm || !ctx || !n || !left || !right || !out_f32 || !cfgs)
+        return fail(VX_ERR_INVALID_ARGUMENT, "autotune_batch: NULL argument");
+    if (iterations == 0) iterations = 1;
+    std::vector<PairSpec> specs(n);
+    for (uint32_t i = 0; i < n; ++i)
+        specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
+    Plan plan;
+    vx_status st = build_plan(specs, &plan);
+    if (st != VX_OK) return st;
+    DeviceGuard g(ctx->device);
+    char* ws = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes,
+                                            ctx->pool, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
+    }
+    bind_plan(plan, ws);
+    cudaEvent_t ev[4] = {};
+    for (auto& x : ev) cudaEventCreate(&x);
+    const int wmax = aggregate_max_warpgroups(plan.dp_max, plan.census64);
+    int best_w = 0;
+    float best = 0.0f;
+    for (int w = 1; w <= wmax && st == VX_OK; ++w) {
+        double total = 0.0;
+        for (uint32_t it = 0; it <= iterations && st == VX_OK; ++it) {  // first run untimed
+            st = run_plan(plan, ws, ctx->stream, ev, w);
+            if (st != VX_OK) break;
+            e = cudaEventSynchronize(ev[3]);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[1], ev[2]);
+            if (e != cudaSuccess) st = cuda_fail(e, "autotune timing");
+            if (it > 0) total += ms;
+        }
+        const float mean = (float)(total / iterations);
+        if (st == VX_OK && (best_w == 0 || mean < best)) {
+            best_w = w;
+            best = mean;
+        }
+    }
+    cudaFreeAsync(ws, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (st != VX_OK) return st;
+    {
+        std::lock_guard<std::mutex> lk(sgm->tune_mu);
+        sgm->tuned[tune_key(plan)] = {best_w, best};
+    }
+    if (best_warpgroups) *best_warpgroups = (uint32_t)best_w;
+    if (best_ms) *best_ms = best;
+    return VX_OK;
+}
+
+vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path) {
+    if (!sgm || !path) return fail(VX_ERR_INVALID_ARGUMENT, "tuning_save: NULL argument");
+    std::ofstream f(path);
+    if (!f) return fail(VX_ERR_INVALID_ARGUMENT, "tuning_save: cannot open %s", path);
+    std::lock_guard<std::mutex> lk(sgm->tune_mu);
+    f << "{\"version\": 1, \"entries\": [";
+    bool first = true;
+    for (const auto& kv : sgm->tuned) {
+        f << (first ? "" : ", ") << "{\"dp_max\": " << kv.first.dp_max
+          << ", \"census64\": " << kv.first.census64 << ", \"units_log2\": " << kv.first.units_log2
+          << ", \"warpgroups\": " << kv.second.warpgroups
+          << ", \"aggregate_ms\": " << kv.second.aggregate_ms << "}";
+        first = false;
+    }
+    f << "]}\n";
+    return f.good() ? VX_OK : fail(VX_ERR_INVALID_ARGUMENT, "tuning_save: write failed");
+}
+
+// Reads the file written by vx_sgm_tuning_save (a flat list of entries with
+// integer fields; anything else in the file is ignored).
+vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
+    if (!sgm || !path) return fail(VX_ERR_INVALID_ARGUMENT, "tuning_load: NULL argument");
+    std::ifstream f(path);
+    if (!f) return fail(VX_ERR_INVALID_ARGUMENT, "tuning_load: cannot open %s", path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    auto field = [&](size_t from, size_t to, const char* name, double* v) {
+        const std::string key = std::string("\"") + name + "\":";
+        size_t p = text.find(key, from);
+        if (p == std::string::npos || p > to) return false;
+        *v = std::strtod(text.c_str() + p + key.size(), nullptr);
+        return true;
+    };
+    size_t pos = 0;
+    int loaded = 0;
+    std::lock_guard<std::mutex> lk(sgm->tune_mu);
+    while ((pos = text.find('{', pos + 1)) != std::string::npos) {
+        const size_t end = text.find('}', pos);
+        if (end == std::string::npos) break;
+        double dp, c64, ul, wg, ms = 0;
+        if (field(pos, end, "dp_max", &dp) && field(pos, end, "census64", &c64) &&
+            field(pos, end, "units_log2", &ul) && field(pos, end, "warpgroups", &wg)) {
+            field(pos, end, "aggregate_ms", &ms);
+            if (wg >= 1 && dp >= 8) {
+                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul}] = {(int)wg, (float)ms};
+                ++loaded;
+            }
+        }
+        pos = end;
+    }
+    if (!loaded) return fail(VX_ERR_INVALID_CONFIG, "tuning_load: no entries in %s", path);
+    return VX_OK;
+}
+
+}  // extern "C"

@@ -53,8 +53,6 @@ constexpr int kCensusTileH = 8;
 constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
 // Largest aggregation CTA (6 warpgroups); keeps registers per thread <= 85.
 constexpr int kAggMaxThreads = 768;
-// Warpgroups per aggregation CTA (one CTA per SM) unless tuned otherwise.
-constexpr int kAggDefaultWarpgroups = 2;
 // Guard words before and after every row-major census plane: the aggregation
 // kernel stages aligned 16-byte chunks that may extend past the first and last
 // row by up to 256 + 40 words.

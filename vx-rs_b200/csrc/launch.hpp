@@ -19,14 +19,16 @@ cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles
 
 // Path aggregation: one persistent launch over `num_units` warp units of every
 // (pair, path) of a batch; warps pull units from `*counter` (zero on entry).
-// dp_max = largest padded disparity count of the batch (sizes shared memory).
-// grid_ctas = 0 picks SMs x occupancy.
-size_t aggregate_smem_bytes(int dp_max, bool census64);
-cudaError_t prepare_aggregate_kernels();  // raises the shared-memory limit; once per device
+// dp_max = largest padded disparity count of the batch. One CTA per SM with
+// `warpgroups` warpgroups (0 = default for this batch; clamped to what an SM
+// holds), sharing one tensor-memory allocation for the scanline state.
+cudaError_t prepare_aggregate_kernels();  // shared-memory limits; once per device
 int aggregate_grid_ctas(int dp_max, bool census64);
-cudaError_t launch_aggregate(int dp_max, bool census64, const PairDev* d_pairs,
+int aggregate_max_warpgroups(int dp_max, bool census64);
+int aggregate_default_warpgroups(int dp_max, bool census64, int num_units);
+cudaError_t launch_aggregate(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs,
                              const JobDev* d_jobs, const UnitDev* d_units, int num_units,
-                             unsigned* counter, int grid_ctas, cudaStream_t stream);
+                             unsigned* counter, cudaStream_t stream);
 
 // WTA + subpixel + optional LR check: one CTA per (pair, row). The kernel keeps
 // three words per pixel of the row in shared memory.

@@ -189,38 +189,58 @@ void bind_plan(Plan& pl, char* base) {
     }
 }
 
-vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev) {
+vx_status upload_plan(const Plan& pl, char* base, cudaStream_t stream, bool pairs_only) {
     const int n = (int)pl.pairs.size();
     if (n == 0) return VX_OK;
     cudaError_t e = cudaMemcpyAsync(base + pl.off_pairs, pl.pairs.data(), n * sizeof(PairDev),
                                     cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(base + pl.off_jobs, pl.jobs.data(), pl.jobs.size() * sizeof(JobDev),
-                            cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess && !pl.units.empty())
-        e = cudaMemcpyAsync(base + pl.off_units, pl.units.data(), pl.units.size() * sizeof(UnitDev),
-                            cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess)
-        e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned), stream);
-    if (e != cudaSuccess) return cuda_fail(e, "uploading the batch plan");
+    if (!pairs_only) {
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(base + pl.off_jobs, pl.jobs.data(), pl.jobs.size() * sizeof(JobDev),
+                                cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess && !pl.units.empty())
+            e = cudaMemcpyAsync(base + pl.off_units, pl.units.data(),
+                                pl.units.size() * sizeof(UnitDev), cudaMemcpyHostToDevice, stream);
+    }
+    return e == cudaSuccess ? VX_OK : cuda_fail(e, "uploading the batch plan");
+}
 
+vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev,
+                      int warpgroups, bool capturing) {
+    // Under stream capture the timing events become event-record nodes.
+    auto record = [&](cudaEvent_t e) {
+        if (!e) return;
+        if (capturing) cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal);
+        else cudaEventRecord(e, stream);
+    };
+    const int n = (int)pl.pairs.size();
+    if (n == 0) return VX_OK;
+    cudaError_t e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the work counter");
     const PairDev* d_pairs = reinterpret_cast<const PairDev*>(base + pl.off_pairs);
     const JobDev* d_jobs = reinterpret_cast<const JobDev*>(base + pl.off_jobs);
     const UnitDev* d_units = reinterpret_cast<const UnitDev*>(base + pl.off_units);
     unsigned* counters = reinterpret_cast<unsigned*>(base + pl.off_counters);
 
-    if (ev) cudaEventRecord(ev[0], stream);
+    if (ev) record(ev[0]);
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
-    if (ev) cudaEventRecord(ev[1], stream);
-    e = launch_aggregate(pl.dp_max, pl.census64, d_pairs, d_jobs, d_units, (int)pl.units.size(),
-                         counters, 0, stream);
+    if (ev) record(ev[1]);
+    e = launch_aggregate(pl.dp_max, pl.census64, warpgroups, d_pairs, d_jobs, d_units,
+                         (int)pl.units.size(), counters, stream);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
-    if (ev) cudaEventRecord(ev[2], stream);
+    if (ev) record(ev[2]);
     e = launch_wta(d_pairs, n, pl.total_rows, pl.max_width, stream);
     if (e != cudaSuccess) return cuda_fail(e, "WTA launch");
-    if (ev) cudaEventRecord(ev[3], stream);
+    if (ev) record(ev[3]);
     return VX_OK;
+}
+
+vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev,
+                   int warpgroups) {
+    vx_status st = upload_plan(pl, base, stream, false);
+    if (st != VX_OK) return st;
+    return launch_plan(pl, base, stream, ev, warpgroups, false);
 }
 
 }  // namespace vxsgm

@@ -10,8 +10,8 @@ namespace {
 
 // Runs a batch; if keep_ws is non-null the workspace is handed back to the
 // caller (who must free it with cudaFreeAsync) instead of being released.
-vx_status run_batch(vx_ctx* ctx, const std::vector<PairSpec>& specs, cudaStream_t stream,
-                    bool synchronous, char** keep_ws, Plan* plan_out) {
+vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
+                    cudaStream_t stream, bool synchronous, char** keep_ws, Plan* plan_out) {
     Plan plan;
     vx_status st = build_plan(specs, &plan);
     if (st != VX_OK) return st;
@@ -24,7 +24,7 @@ vx_status run_batch(vx_ctx* ctx, const std::vector<PairSpec>& specs, cudaStream_
         return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
     }
     bind_plan(plan, ws);
-    st = run_plan(plan, ws, stream, ctx->next_timing_slot());
+    st = run_plan(plan, ws, stream, ctx->next_timing_slot(), sgm->warpgroups_for(plan));
     if (keep_ws && st == VX_OK) {
         *keep_ws = ws;
     } else {
@@ -96,7 +96,8 @@ vx_status vx_sgm_compute_disparity(vx_sgm* sgm, vx_ctx* ctx, const vx_image* lef
     if (!sgm || !ctx || !cfg) return fail(VX_ERR_INVALID_ARGUMENT, "compute_disparity: NULL argument");
     std::vector<PairSpec> specs{{left, right, out_f32, out_i16, *cfg}};
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    return run_batch(ctx, specs, s, stream == nullptr, nullptr, nullptr);
+    if (sgm->graph_capacity) return run_batch_graph(sgm, ctx, specs, s, stream == nullptr);
+    return run_batch(sgm, ctx, specs, s, stream == nullptr, nullptr, nullptr);
 }
 
 vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
@@ -109,7 +110,8 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
     for (uint32_t i = 0; i < n; ++i)
         specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    return run_batch(ctx, specs, s, stream == nullptr, nullptr, nullptr);
+    if (sgm->graph_capacity) return run_batch_graph(sgm, ctx, specs, s, stream == nullptr);
+    return run_batch(sgm, ctx, specs, s, stream == nullptr, nullptr, nullptr);
 }
 
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg) {
@@ -135,7 +137,7 @@ vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, cons
     std::vector<PairSpec> specs{{left, right, out, nullptr, *cfg}};
     char* ws = nullptr;
     Plan plan;
-    st = run_batch(ctx, specs, ctx->stream, true, &ws, &plan);
+    st = run_batch(sgm, ctx, specs, ctx->stream, true, &ws, &plan);
     if (st == VX_OK) {
         const PairDev& pd = plan.pairs[0];
         const size_t W = pd.width, H = pd.height, D = pd.nd, Dp = pd.nd_pad, P = pd.num_paths;

@@ -4,6 +4,7 @@
 
 #include <cstdarg>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -39,11 +40,6 @@ struct vx_image {
     uint32_t width = 0, height = 0;
     vx_format format = VX_FORMAT_U8;
     bool owned = false;
-};
-
-// The reference's SGMStereo (vx-vision/src/kernels/sgm.rs:62).
-struct vx_sgm {
-    vx_ctx* ctx = nullptr;
 };
 
 namespace vxsgm {
@@ -103,8 +99,66 @@ void bind_plan(Plan& plan, char* base);
 // Issues the whole batch (census, aggregation, WTA) on `stream` with the
 // workspace at `base` (plan must be bound to it).
 // stage_events: null, or 4 events recorded before census, before aggregation,
-// before WTA and after WTA.
+// before WTA and after WTA. warpgroups: aggregation CTA size (0 = default).
 vx_status run_plan(const Plan& plan, char* base, cudaStream_t stream,
-                   cudaEvent_t* stage_events = nullptr);
+                   cudaEvent_t* stage_events = nullptr, int warpgroups = 0);
+// The two halves of run_plan: copy the plan tables into the workspace (all of
+// them, or the pair table alone), and the launch sequence itself (which is
+// what a CUDA graph of the batch captures).
+vx_status upload_plan(const Plan& plan, char* base, cudaStream_t stream, bool pairs_only);
+vx_status launch_plan(const Plan& plan, char* base, cudaStream_t stream, cudaEvent_t* stage_events,
+                      int warpgroups, bool capturing);
+
+// Autotuning key of a batch: the aggregation launch shape depends on the
+// largest padded D, the census word width and the amount of queued work.
+struct TuneKey {
+    int dp_max;
+    int census64;
+    int units_log2;
+    bool operator<(const TuneKey& o) const {
+        if (dp_max != o.dp_max) return dp_max < o.dp_max;
+        if (census64 != o.census64) return census64 < o.census64;
+        return units_log2 < o.units_log2;
+    }
+};
+TuneKey tune_key(const Plan& plan);
 
 }  // namespace vxsgm
+
+struct vx_sgm;
+namespace vxsgm {
+// The batch through the sgm's CUDA-graph cache (graphs.cpp).
+vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
+                          cudaStream_t stream, bool synchronous);
+}  // namespace vxsgm
+
+// The reference's SGMStereo (vx-vision/src/kernels/sgm.rs:62), plus the
+// autotuned launch shapes of the batches it has seen.
+struct vx_sgm {
+    vx_ctx* ctx = nullptr;
+    struct Tuned {
+        int warpgroups;
+        float aggregate_ms;
+    };
+    std::mutex tune_mu;
+    std::map<vxsgm::TuneKey, Tuned> tuned;
+    int warpgroups_for(const vxsgm::Plan& plan);
+
+    // CUDA graphs per shape bucket (see graphs.cpp): a bucket is the list of
+    // every pair's size and config; image pointers may differ between calls.
+    struct GraphEntry {
+        std::string key;
+        vxsgm::Plan plan;           // bound to ws
+        char* ws = nullptr;         // resident workspace of the bucket
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaEvent_t baked[4] = {};  // events the stage-timing nodes were captured with
+        cudaGraphNode_t ev_nodes[4] = {};
+        uint64_t last_use = 0;
+    };
+    std::mutex graph_mu;
+    size_t graph_capacity = 0;
+    uint64_t graph_clock = 0;
+    std::vector<GraphEntry*> graphs;
+    ~vx_sgm();
+};

@@ -91,6 +91,13 @@ _sgm_compute = _sig("vx_sgm_compute_disparity", ctypes.c_int, _P, _P, _P, _P, _P
 _sgm_batch = _sig("vx_sgm_compute_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
                   ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                   ctypes.POINTER(_CConfig), _P)
+_sgm_autotune = _sig("vx_sgm_autotune_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
+                     ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                     ctypes.POINTER(_CConfig), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                     ctypes.POINTER(ctypes.c_float))
+_graph_cache = _sig("vx_sgm_set_graph_cache", ctypes.c_int, _P, ctypes.c_uint32)
+_tuning_save = _sig("vx_sgm_tuning_save", ctypes.c_int, _P, ctypes.c_char_p)
+_tuning_load = _sig("vx_sgm_tuning_load", ctypes.c_int, _P, ctypes.c_char_p)
 _sgm_ws = _sig("vx_sgm_workspace_bytes", ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
                ctypes.POINTER(_CConfig))
 _sgm_noalloc = _sig("vx_sgm_compute_disparity_noalloc", ctypes.c_int, _P, ctypes.c_size_t, _P,
@@ -264,6 +271,7 @@ class SGMStereo:
         h = _P()
         _check(_sgm_create(ctx.handle, ctypes.byref(h)))
         self._h = h
+        self._ctx = ctx  # the handle must be destroyed before its context
 
     @classmethod
     def new(cls, ctx: Context) -> "SGMStereo":
@@ -289,6 +297,29 @@ class SGMStereo:
         oi = arr(outputs_i16) if outputs_i16 is not None else None
         _check(_sgm_batch(self._h, ctx.handle, n, arr(lefts), arr(rights), arr(outputs), oi, cfgs,
                           _P(stream) if stream else None))
+
+    def autotune_batch(self, ctx: Context, lefts, rights, outputs, configs, outputs_i16=None,
+                       iterations: int = 2):
+        """Times every aggregation launch shape on this batch and keeps the fastest
+        for batches like it. Returns (warpgroups, aggregate_ms)."""
+        n = len(lefts)
+        arr = lambda ts: (_P * n)(*[t.handle if t is not None else None for t in ts])
+        cfgs = (_CConfig * n)(*[c.to_c() for c in configs])
+        oi = arr(outputs_i16) if outputs_i16 is not None else None
+        w, ms = ctypes.c_uint32(), ctypes.c_float()
+        _check(_sgm_autotune(self._h, ctx.handle, n, arr(lefts), arr(rights), arr(outputs), oi,
+                             cfgs, iterations, ctypes.byref(w), ctypes.byref(ms)))
+        return int(w.value), float(ms.value)
+
+    def set_graph_cache(self, max_buckets: int):
+        """CUDA graphs per shape bucket for compute_batch / compute_disparity."""
+        _check(_graph_cache(self._h, int(max_buckets)))
+
+    def tuning_save(self, path: str):
+        _check(_tuning_save(self._h, path.encode()))
+
+    def tuning_load(self, path: str):
+        _check(_tuning_load(self._h, path.encode()))
 
     def debug_dump(self, ctx: Context, left: Texture, right: Texture, config: SGMStereoConfig):
         """Census words, per-path costs L_r and summed cost volume S of one pair."""
