@@ -143,10 +143,19 @@ __device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int r
                                            int la, int lb, uint16_t* __restrict__ dst0,
                                            size_t stride, int lane) {
     __syncwarp();
+    // Word c = (p - la) * G + g of the run, walked with a running (p, g) so
+    // that no division is needed per word: lane starts at c = lane, steps 32.
     const int n = (lb - la + 1) * G;
+    const int q = 32 / G, r = 32 % G;
+    int p = la + lane / G, g = lane % G;
     for (int c = lane; c < n; c += 32) {
-        const int p = la + c / G, g = c % G;
         __stcs(reinterpret_cast<uint4*>(dst0 + (size_t)p * stride + 8 * g), tile[p * row_words + g]);
+        g += r;
+        p += q;
+        if (g >= G) {
+            g -= G;
+            ++p;
+        }
     }
     __syncwarp();
 }
