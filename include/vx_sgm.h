@@ -196,6 +196,47 @@ vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, cons
 vx_status vx_ctx_enable_stage_timing(vx_ctx* ctx, int enable);
 vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms, float* wta_ms);
 
+/* ---- Serving loop (no reference counterpart) ----------------------------
+ * Continuous batching of stereo requests of any size and config under a
+ * device-memory budget. submit() copies the images into pinned host memory and
+ * queues the request; a scheduler thread admits queued requests in arrival
+ * order while their device bytes (vx_sgm_workspace_bytes + images + outputs)
+ * fit the budget, batches up to max_batch of them, and runs the batch on one of
+ * max_inflight_batches streams (upload, batched SGM, download); batches on
+ * different streams overlap, and new requests join the next batch as soon as a
+ * stream and memory are free. A request's result does not depend on the other
+ * requests of its batch. A request larger than the whole budget is rejected
+ * with VX_ERR_BUDGET. Device buffers come from the context's resident pool. */
+typedef struct vx_sgm_server vx_sgm_server;
+typedef struct vx_server_config {
+    size_t memory_budget_bytes;
+    uint32_t max_batch;
+    uint32_t max_inflight_batches;
+} vx_server_config;
+typedef struct vx_server_stats {
+    uint64_t submitted, completed, rejected, cancelled, failed, batches;
+    uint64_t queued;                      /* waiting for admission */
+    uint64_t inflight_bytes;              /* budget in use */
+    uint64_t completed_pixel_disparities; /* sum of W*H*D of completed requests */
+} vx_server_stats;
+
+vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config* cfg,
+                               vx_sgm_server** out);
+/* Stops admitting, cancels queued requests, waits for running ones. */
+void vx_sgm_server_destroy(vx_sgm_server* server);
+/* left/right: host u8 planes (host_pitch bytes per row, 0 = width). */
+vx_status vx_sgm_server_submit(vx_sgm_server* server, const uint8_t* left, const uint8_t* right,
+                               uint32_t width, uint32_t height, size_t host_pitch,
+                               const vx_sgm_config* cfg, int want_i16, uint64_t* request_id);
+/* Waits up to timeout_ms (0 = poll: VX_ERR_NOT_READY if not done) and copies the
+ * result (W*H f32, optional W*H i16) and the submit-to-completion latency out;
+ * the request is then forgotten. VX_ERR_TIMEOUT when the wait runs out. */
+vx_status vx_sgm_server_wait(vx_sgm_server* server, uint64_t request_id, float* disparity,
+                             int16_t* disparity_i16, double* latency_ms, uint32_t timeout_ms);
+/* Cancels a request that is still queued (VX_ERR_NOT_READY once it started). */
+vx_status vx_sgm_server_cancel(vx_sgm_server* server, uint64_t request_id);
+vx_status vx_sgm_server_get_stats(vx_sgm_server* server, vx_server_stats* out);
+
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);
 

@@ -1,0 +1,84 @@
+"""Serving loop on the GPU: continuous batching under a memory budget. Each served
+result equals the same pair computed alone; oversize requests are rejected;
+queued requests can be cancelled."""
+import numpy as np
+import pytest
+
+import vx_sgm
+from gpu_helpers import assert_disparity_equal, run_pair
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(160, 120), (320, 240), (211, 97), (400, 150)]
+
+
+def _request(i):
+    w, h = SIZES[i % len(SIZES)]
+    nd = [32, 64, 128][i % 3]
+    L, R, _ = vx_sgm.synth_pair(vx_sgm.SCENE_PLANES, w, h, 2, nd - 4, 500 + i)
+    cfg = vx_sgm.SGMStereoConfig(num_disparities=nd, census_radius_x=2, census_radius_y=2,
+                                 num_paths=8, lr_check=True)
+    return L, R, cfg
+
+
+def test_served_results_equal_solo(gpu_ctx, sgm):
+    reqs = [_request(i) for i in range(14)]
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    # Budget for about three requests at a time: requests queue and batches form.
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=3 * biggest, max_batch=4,
+                        max_inflight_batches=2)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    results = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["batches"] >= 2 and st["failed"] == 0
+    assert st["completed_pixel_disparities"] == sum(L.size * c.num_disparities for L, _, c in reqs)
+    for (L, R, c), (d, di, lat) in zip(reqs, results):
+        assert lat > 0
+        assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
+
+
+def test_oversize_request_is_rejected(gpu_ctx, sgm):
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=1 << 20, max_batch=4)
+    L, R, c = _request(1)
+    with pytest.raises(vx_sgm.VxError) as e:
+        srv.submit(L, R, c)
+    assert e.value.status == 8  # VX_ERR_BUDGET
+    assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_cancel_queued_request(gpu_ctx, sgm):
+    reqs = [_request(i) for i in range(6)]
+    need = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=int(need * 1.5), max_batch=1,
+                        max_inflight_batches=1)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    cancelled = None
+    for rid in reversed(ids):  # the last ones are still queued behind the first
+        try:
+            srv.cancel(rid)
+            cancelled = rid
+            break
+        except vx_sgm.VxError:
+            continue
+    assert cancelled is not None
+    for rid in ids:
+        if rid == cancelled:
+            with pytest.raises(vx_sgm.VxError) as e:
+                srv.wait(rid)
+            assert e.value.status == 12  # VX_ERR_CANCELLED
+        else:
+            d, di, _ = srv.wait(rid)
+            assert d.shape == di.shape
+    assert srv.stats()["cancelled"] == 1
+    srv.close()
+
+
+def test_server_rejects_bad_config(gpu_ctx, sgm):
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=1 << 30)
+    L, R, _ = _request(0)
+    with pytest.raises(vx_sgm.VxError) as e:
+        srv.submit(L, R, vx_sgm.SGMStereoConfig(num_disparities=300))
+    assert e.value.status == 6
+    srv.close()

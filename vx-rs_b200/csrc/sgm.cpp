@@ -40,6 +40,13 @@ vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs
 
 }  // namespace
 
+namespace vxsgm {
+vx_status run_batch_plain(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
+                          cudaStream_t stream) {
+    return run_batch(sgm, ctx, specs, stream, false, nullptr, nullptr);
+}
+}  // namespace vxsgm
+
 extern "C" {
 
 void vx_sgm_config_default(vx_sgm_config* cfg) {

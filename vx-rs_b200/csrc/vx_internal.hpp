@@ -127,6 +127,9 @@ TuneKey tune_key(const Plan& plan);
 
 struct vx_sgm;
 namespace vxsgm {
+// The batch without graphs, asynchronous on `stream` (workspace from the pool).
+vx_status run_batch_plain(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
+                          cudaStream_t stream);
 // The batch through the sgm's CUDA-graph cache (graphs.cpp).
 vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
                           cudaStream_t stream, bool synchronous);

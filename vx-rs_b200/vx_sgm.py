@@ -346,6 +346,92 @@ class SGMStereo:
             pass
 
 
+class _CServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_size_t), ("max_batch", ctypes.c_uint32),
+                ("max_inflight_batches", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("rejected", ctypes.c_uint64), ("cancelled", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("inflight_bytes", ctypes.c_uint64),
+                ("completed_pixel_disparities", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+_srv_create = _sig("vx_sgm_server_create", ctypes.c_int, _P, _P, ctypes.POINTER(_CServerConfig),
+                   ctypes.POINTER(_P))
+_srv_destroy = _sig("vx_sgm_server_destroy", None, _P)
+_srv_submit = _sig("vx_sgm_server_submit", ctypes.c_int, _P, _P, _P, ctypes.c_uint32,
+                   ctypes.c_uint32, ctypes.c_size_t, ctypes.POINTER(_CConfig), ctypes.c_int,
+                   ctypes.POINTER(ctypes.c_uint64))
+_srv_wait = _sig("vx_sgm_server_wait", ctypes.c_int, _P, ctypes.c_uint64, _P, _P,
+                 ctypes.POINTER(ctypes.c_double), ctypes.c_uint32)
+_srv_cancel = _sig("vx_sgm_server_cancel", ctypes.c_int, _P, ctypes.c_uint64)
+_srv_stats = _sig("vx_sgm_server_get_stats", ctypes.c_int, _P, ctypes.POINTER(ServerStats))
+
+
+class Server:
+    """Continuous-batching SGM server under a device-memory budget (see vx_sgm.h)."""
+
+    def __init__(self, sgm: "SGMStereo", ctx: Context, memory_budget_bytes: int,
+                 max_batch: int = 32, max_inflight_batches: int = 2):
+        c = _CServerConfig(int(memory_budget_bytes), int(max_batch), int(max_inflight_batches))
+        h = _P()
+        _check(_srv_create(sgm.handle, ctx.handle, ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+        self._keep = (sgm, ctx)
+        self._shapes = {}
+
+    def submit(self, left: np.ndarray, right: np.ndarray, config: SGMStereoConfig,
+               want_i16: bool = True) -> int:
+        left = np.ascontiguousarray(left, np.uint8)
+        right = np.ascontiguousarray(right, np.uint8)
+        h, w = left.shape
+        c = config.to_c()
+        rid = ctypes.c_uint64()
+        _check(_srv_submit(self._h, left.ctypes.data, right.ctypes.data, w, h, w, ctypes.byref(c),
+                           int(want_i16), ctypes.byref(rid)))
+        self._shapes[rid.value] = (h, w, want_i16)
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = 60000):
+        """(disparity f32, disparity i16 or None, latency_ms); raises VxError."""
+        h, w, want_i16 = self._shapes[rid]
+        d = np.empty((h, w), np.float32)
+        di = np.empty((h, w), np.int16) if want_i16 else None
+        lat = ctypes.c_double()
+        st = _srv_wait(self._h, rid, d.ctypes.data, di.ctypes.data if di is not None else None,
+                       ctypes.byref(lat), int(timeout_ms))
+        if st == 11:  # VX_ERR_NOT_READY (poll)
+            return None
+        del self._shapes[rid]
+        _check(st)
+        return d, di, lat.value
+
+    def cancel(self, rid: int):
+        _check(_srv_cancel(self._h, rid))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_srv_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            _srv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def compute_disparity_noalloc(left: Texture, right: Texture, output: Texture,
                               config: SGMStereoConfig, output_i16: Texture | None = None,
                               stream: int | None = None):
