@@ -145,6 +145,36 @@ def cpu_reference_rate(items, pairs, max_pd, threads):
     return done_pd / secs / 1e9, n, done_pd, secs
 
 
+SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
+
+
+def served(vx_sgm, ctx, sgm, rates, num_requests):
+    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, 40 GB budget."""
+    import loadgen
+    reqs = loadgen.make_requests(48)
+    srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=32,
+                        max_inflight_batches=2)
+    loadgen.run_poisson(srv, reqs, 100.0, 16)  # warm the pool and the planner
+    out = []
+    for r in rates:
+        res = loadgen.run_poisson(srv, reqs, r, num_requests)
+        res["server"] = srv.stats()
+        out.append(res)
+    srv.close()
+    return out
+
+
+def run_serve_sweep(args, local_rank):
+    import vx_sgm
+    ctx = vx_sgm.Context(local_rank)
+    sgm = vx_sgm.SGMStereo(ctx)
+    rates = [float(x) for x in args.serve_sweep.split(",") if x]
+    for res in served(vx_sgm, ctx, sgm, rates, args.serve_requests):
+        print(json.dumps({"metric": "served SGM", "unit": UNIT, "budget_bytes": SERVE_BUDGET,
+                          "workload": "Poisson arrivals, sizes {640x480,1242x375,1280x720,1920x1080} "
+                                      "x D{64,128,192}, 8 paths", **res}), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -181,6 +211,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--workload", default="mixed", choices=["mixed", "profile", "profile-mix"])
+    ap.add_argument("--serve-rate", type=float, default=200.0,
+                    help="Poisson arrival rate of the served measurement (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-sweep", default="",
+                    help="comma-separated arrival rates: run the served sweep and print one JSON "
+                         "line per rate instead of the benchmark")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
@@ -205,6 +241,9 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     import vx_sgm
+    if args.serve_sweep:
+        run_serve_sweep(args, local_rank)
+        return
     items = workload(rank, args.workload)
     pairs = make_pairs(vx_sgm, items)
     cfgs = [sgm_config(vx_sgm, d) for (_, _, d, _) in items]
@@ -321,6 +360,9 @@ def main():
     plain_ms = max_over_ranks(plain_ms / args.plain_steps)
     plain_value = world * total_pd / (plain_ms * 1e-3) / 1e9
 
+    # ---- served: continuous batching under a 40 GB budget, Poisson arrivals ----
+    serve = served(vx_sgm, ctx, sgm, [args.serve_rate], args.serve_requests)[0]
+
     # ---- roofline of the dominant kernel (path aggregation) ----
     peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -347,6 +389,8 @@ def main():
                   "latency_ms_p50": float(np.percentile(lat, 50)),
                   "latency_ms_p99": float(np.percentile(lat, 99)),
                   "batched_over_plain": value / plain_value},
+        "served": {k: serve[k] for k in ("rate_per_s", "requests", "completed", "latency_ms_p50",
+                                          "latency_ms_p99", "throughput_gpd_s", "achieved_rate_per_s")},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms},

@@ -206,7 +206,8 @@ vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms,
  * different streams overlap, and new requests join the next batch as soon as a
  * stream and memory are free. A request's result does not depend on the other
  * requests of its batch. A request larger than the whole budget is rejected
- * with VX_ERR_BUDGET. Device buffers come from the context's resident pool. */
+ * with VX_ERR_BUDGET. Device buffers come from the context's resident pool;
+ * creating the server maps the whole budget into that pool up front. */
 typedef struct vx_sgm_server vx_sgm_server;
 typedef struct vx_server_config {
     size_t memory_budget_bytes;

@@ -38,11 +38,12 @@ double ms_since(Clock::time_point t0, Clock::time_point t1) {
 }
 
 // Pinned host buffers by power-of-two size class, reused across requests.
+// cudaMallocHost is slow and serialises with other CUDA calls, so blocks are
+// carved out of chunks of at least 64 MB (and 8 blocks) per class.
 class PinnedPool {
   public:
     ~PinnedPool() {
-        for (auto& kv : free_)
-            for (void* p : kv.second) cudaFreeHost(p);
+        for (void* c : chunks_) cudaFreeHost(c);
     }
     void* get(size_t bytes, size_t* cls) {
         size_t c = 4096;
@@ -50,16 +51,18 @@ class PinnedPool {
         *cls = c;
         std::lock_guard<std::mutex> lk(mu_);
         auto& v = free_[c];
-        if (!v.empty()) {
-            void* p = v.back();
-            v.pop_back();
-            return p;
+        if (v.empty()) {
+            const size_t n = std::max<size_t>(8, ((size_t)64 << 20) / c);
+            void* chunk = nullptr;
+            if (cudaMallocHost(&chunk, n * c) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            chunks_.push_back(chunk);
+            for (size_t i = 0; i < n; ++i) v.push_back(static_cast<char*>(chunk) + i * c);
         }
-        void* p = nullptr;
-        if (cudaMallocHost(&p, c) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
+        void* p = v.back();
+        v.pop_back();
         return p;
     }
     void put(void* p, size_t cls) {
@@ -71,6 +74,7 @@ class PinnedPool {
   private:
     std::mutex mu_;
     std::map<size_t, std::vector<void*>> free_;
+    std::vector<void*> chunks_;
 };
 
 enum ReqState { kPending, kRunning, kDone, kCancelled, kFailed };
@@ -300,6 +304,17 @@ vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config*
             }
             delete s;
             return st;
+        }
+    }
+    // Keep the budget resident: map it into the context's pool now, so that
+    // admitting requests never waits for the pool to grow.
+    {
+        void* warm = nullptr;
+        if (cudaMallocFromPoolAsync(&warm, s->budget, ctx->pool, s->slots[0].stream) == cudaSuccess) {
+            cudaFreeAsync(warm, s->slots[0].stream);
+            cudaStreamSynchronize(s->slots[0].stream);
+        } else {
+            cudaGetLastError();  // the pool grows on demand instead
         }
     }
     s->worker = std::thread([s] { s->run(); });
