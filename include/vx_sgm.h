@@ -59,6 +59,10 @@ void vx_ctx_destroy(vx_ctx* ctx);
 vx_stream vx_ctx_stream(vx_ctx* ctx);
 /* Blocks until all work on the context's stream has finished. */
 vx_status vx_ctx_synchronize(vx_ctx* ctx);
+/* Largest device workspace one batch call may take (default: 85% of the device
+ * memory free when the context was created). A batch needing more runs as
+ * consecutive sub-batches on the same stream. */
+vx_status vx_ctx_set_workspace_limit(vx_ctx* ctx, size_t bytes);
 
 /* Image formats: R8Unorm input (texture.rs:38 from_gray8), R32Float output
  * (texture.rs:324 output_r32float), and an int16 integer-disparity map. */
@@ -118,6 +122,32 @@ void vx_sgm_destroy(vx_sgm* sgm);  /* before the context it was created with */
 vx_status vx_sgm_compute_disparity(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left,
                                    const vx_image* right, vx_image* out_f32, vx_image* out_i16,
                                    const vx_sgm_config* cfg, vx_stream stream);
+
+/* CameraIntrinsics (vx-vision/src/types_3d.rs:254-267). */
+typedef struct vx_camera_intrinsics {
+    float fx, fy, cx, cy;
+    uint32_t width, height;
+} vx_camera_intrinsics;
+
+/* DepthMap (vx-vision/src/types_3d.rs:384-410): an F32 texture with intrinsics
+ * and a depth range. The texture is owned by the caller (vx_image_destroy). */
+typedef struct vx_depth_map {
+    vx_image* texture;
+    vx_camera_intrinsics intrinsics;
+    float min_depth, max_depth;
+} vx_depth_map;
+
+/* Replaces SGMStereo::compute(&ctx, &left, &right, &config, &intrinsics,
+ * baseline) (sgm.rs:268-288): allocates an F32 output of the left image's size,
+ * computes the disparity into it and returns a DepthMap over it with
+ * min_depth 0 and max_depth FLT_MAX, exactly like the reference (which does
+ * not convert disparity to depth and ignores baseline). Extension: if depth_out
+ * (an F32 image of the same size) is given, the WTA kernel also writes
+ * depth = fx * baseline / disparity there (0 where the disparity is invalid or
+ * <= 0). Synchronous on the context's stream. */
+vx_status vx_sgm_compute(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,
+                         const vx_sgm_config* cfg, const vx_camera_intrinsics* intrinsics,
+                         float baseline, vx_image* depth_out, vx_depth_map* out);
 
 /* Batched form of compute_disparity (no reference counterpart; the
  * reference only has the per-pair call, sgm.rs:108): n independent pairs of

@@ -67,6 +67,11 @@ vx_status vx_ctx_create(int device_ordinal, vx_ctx** out) {
     cudaError_t e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device_ordinal);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
+        size_t free_b = 0, total_b = 0;
+        e = cudaMemGetInfo(&free_b, &total_b);
+        ctx->workspace_limit = free_b / 20 * 17;
+    }
+    if (e == cudaSuccess) {
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
@@ -144,6 +149,12 @@ vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms,
     if (census_ms) *census_ms = (float)(sum[0] / n);
     if (aggregate_ms) *aggregate_ms = (float)(sum[1] / n);
     if (wta_ms) *wta_ms = (float)(sum[2] / n);
+    return VX_OK;
+}
+
+vx_status vx_ctx_set_workspace_limit(vx_ctx* ctx, size_t bytes) {
+    if (!ctx || bytes == 0) return fail(VX_ERR_INVALID_ARGUMENT, "vx_ctx_set_workspace_limit: bad argument");
+    ctx->workspace_limit = bytes;
     return VX_OK;
 }
 

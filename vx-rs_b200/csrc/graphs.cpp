@@ -30,7 +30,7 @@ std::string bucket_key(const std::vector<PairSpec>& specs) {
         k << s.left->width << 'x' << s.left->height << ':' << c.num_disparities << ',' << p1 << ','
           << p2 << ',' << c.census_radius_x << ',' << c.census_radius_y << ',' << c.num_paths
           << ',' << c.subpixel << ',' << c.lr_check << ',' << c.lr_tolerance << ',' << inv << ','
-          << (s.out_i16 ? 1 : 0) << ';';
+          << (s.out_i16 ? 1 : 0) << ',' << (s.out_depth ? 1 : 0) << ';';
     }
     return k.str();
 }
@@ -57,6 +57,10 @@ void rebind_pointers(vxsgm::Plan& plan, const std::vector<PairSpec>& specs) {
         pd.out_f32_pitch = s.out_f32->pitch;
         pd.out_i16 = s.out_i16 ? static_cast<int16_t*>(s.out_i16->ptr) : nullptr;
         pd.out_i16_pitch = s.out_i16 ? s.out_i16->pitch : 0;
+        pd.out_depth = s.out_depth ? static_cast<float*>(s.out_depth->ptr) : nullptr;
+        pd.out_depth_pitch = s.out_depth ? s.out_depth->pitch : 0;
+        pd.depth_scale = s.depth_scale;
+        pd.depth_invalid = s.depth_invalid;
     }
 }
 

@@ -21,6 +21,10 @@ struct PairDev {
     size_t out_f32_pitch;
     int16_t* out_i16;      // optional integer disparity, pitch in bytes
     size_t out_i16_pitch;
+    float* out_depth;      // optional depth fx*B/disparity, pitch in bytes
+    size_t out_depth_pitch;
+    float depth_scale;     // fx * baseline
+    float depth_invalid;   // written where the disparity is invalid or <= 0
     int width, height;
     int nd;                // number of disparities D (1..256)
     int nd_pad;            // Dp = D rounded up to 8

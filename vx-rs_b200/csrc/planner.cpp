@@ -32,9 +32,12 @@ vx_status validate_pair(const PairSpec& p) {
         return fail(VX_ERR_INVALID_ARGUMENT, "output image must be F32");
     if (p.out_i16 && p.out_i16->format != VX_FORMAT_I16)
         return fail(VX_ERR_INVALID_ARGUMENT, "integer output image must be I16");
+    if (p.out_depth && p.out_depth->format != VX_FORMAT_F32)
+        return fail(VX_ERR_INVALID_ARGUMENT, "depth output image must be F32");
     const uint32_t w = p.left->width, h = p.left->height;
     if (p.right->width != w || p.right->height != h || p.out_f32->width != w ||
-        p.out_f32->height != h || (p.out_i16 && (p.out_i16->width != w || p.out_i16->height != h)))
+        p.out_f32->height != h || (p.out_i16 && (p.out_i16->width != w || p.out_i16->height != h)) ||
+        (p.out_depth && (p.out_depth->width != w || p.out_depth->height != h)))
         return fail(VX_ERR_SIZE_MISMATCH, "texture size mismatch");
     if (w > (uint32_t)kMaxWidth)
         return fail(VX_ERR_INVALID_CONFIG, "image width %u exceeds %d", w, kMaxWidth);
@@ -82,6 +85,10 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         pd.out_f32_pitch = s.out_f32->pitch;
         pd.out_i16 = s.out_i16 ? static_cast<int16_t*>(s.out_i16->ptr) : nullptr;
         pd.out_i16_pitch = s.out_i16 ? s.out_i16->pitch : 0;
+        pd.out_depth = s.out_depth ? static_cast<float*>(s.out_depth->ptr) : nullptr;
+        pd.out_depth_pitch = s.out_depth ? s.out_depth->pitch : 0;
+        pd.depth_scale = s.depth_scale;
+        pd.depth_invalid = s.depth_invalid;
         pd.width = W;
         pd.height = H;
         pd.nd = D;

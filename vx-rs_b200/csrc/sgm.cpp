@@ -1,4 +1,5 @@
 // SGMStereo entry points of the vx_sgm C ABI (vx-vision/src/kernels/sgm.rs).
+#include <cfloat>
 #include <cstring>
 #include <vector>
 
@@ -16,6 +17,34 @@ vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs
     vx_status st = build_plan(specs, &plan);
     if (st != VX_OK) return st;
     if (specs.empty()) return VX_OK;
+    if (plan.ws_bytes > ctx->workspace_limit && specs.size() > 1 && !keep_ws) {
+        // Staging: consecutive sub-batches that each fit the workspace limit run
+        // one after another on the stream (each reuses the previous one's
+        // workspace from the pool).
+        std::vector<PairSpec> chunk;
+        size_t bytes = 0;
+        for (size_t i = 0; i <= specs.size(); ++i) {
+            size_t b = 0;
+            if (i < specs.size())
+                b = vx_sgm_workspace_bytes(specs[i].left->width, specs[i].left->height, &specs[i].cfg) +
+                    (64 << 10);
+            if (i == specs.size() || (!chunk.empty() && bytes + b > ctx->workspace_limit)) {
+                st = run_batch(sgm, ctx, chunk, stream, false, nullptr, nullptr);
+                if (st != VX_OK) return st;
+                chunk.clear();
+                bytes = 0;
+            }
+            if (i < specs.size()) {
+                chunk.push_back(specs[i]);
+                bytes += b;
+            }
+        }
+        if (synchronous) {
+            cudaError_t e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "SGM execution");
+        }
+        return VX_OK;
+    }
     DeviceGuard g(ctx->device);
     char* ws = nullptr;
     cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool, stream);
@@ -107,6 +136,33 @@ vx_status vx_sgm_compute_disparity(vx_sgm* sgm, vx_ctx* ctx, const vx_image* lef
     return run_batch(sgm, ctx, specs, s, stream == nullptr, nullptr, nullptr);
 }
 
+vx_status vx_sgm_compute(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,
+                         const vx_sgm_config* cfg, const vx_camera_intrinsics* intrinsics,
+                         float baseline, vx_image* depth_out, vx_depth_map* out) {
+    if (!sgm || !ctx || !left || !right || !cfg || !intrinsics || !out)
+        return fail(VX_ERR_INVALID_ARGUMENT, "compute: NULL argument");
+    std::memset(out, 0, sizeof *out);
+    // sgm.rs:278-287: an R32Float output of the left image's size, the disparity
+    // computation, and a DepthMap over that texture (min 0, max f32::MAX).
+    vx_image* disp = nullptr;
+    vx_status st = vx_image_create(ctx, left->width, left->height, VX_FORMAT_F32, &disp);
+    if (st != VX_OK) return st;
+    std::vector<PairSpec> specs{{left, right, disp, nullptr, *cfg}};
+    specs[0].out_depth = depth_out;
+    specs[0].depth_scale = intrinsics->fx * baseline;
+    specs[0].depth_invalid = 0.0f;
+    st = run_batch(sgm, ctx, specs, ctx->stream, true, nullptr, nullptr);
+    if (st != VX_OK) {
+        vx_image_destroy(disp);
+        return st;
+    }
+    out->texture = disp;
+    out->intrinsics = *intrinsics;
+    out->min_depth = 0.0f;
+    out->max_depth = FLT_MAX;
+    return VX_OK;
+}
+
 vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
                                const vx_image* const* right, vx_image* const* out_f32,
                                vx_image* const* out_i16, const vx_sgm_config* cfgs,
@@ -117,7 +173,12 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
     for (uint32_t i = 0; i < n; ++i)
         specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    if (sgm->graph_capacity) return run_batch_graph(sgm, ctx, specs, s, stream == nullptr);
+    if (sgm->graph_capacity) {
+        size_t total = 0;
+        for (const auto& p : specs)
+            if (p.left) total += vx_sgm_workspace_bytes(p.left->width, p.left->height, &p.cfg);
+        if (total <= ctx->workspace_limit) return run_batch_graph(sgm, ctx, specs, s, stream == nullptr);
+    }
     return run_batch(sgm, ctx, specs, s, stream == nullptr, nullptr, nullptr);
 }
 

@@ -22,6 +22,9 @@ struct vx_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
+    // Largest workspace one batch may take; larger batches run as sequential
+    // sub-batches (set at creation to 85% of the free device memory).
+    size_t workspace_limit = 0;
     // Stage timing: per batch, 4 events bracket census | aggregation | WTA.
     // Batches since the last enable take consecutive slots of the ring.
     static constexpr int kTimingSlots = 256;
@@ -74,6 +77,9 @@ struct PairSpec {
     vx_image* out_f32;
     vx_image* out_i16;
     vx_sgm_config cfg;
+    vx_image* out_depth = nullptr;  // optional: fx * baseline / disparity
+    float depth_scale = 0.0f;
+    float depth_invalid = 0.0f;
 };
 
 vx_status validate_pair(const PairSpec& p);

@@ -9,6 +9,7 @@
 //            (IEEE single precision, correctly rounded division).
 // Extension: right-view WTA dR(x') = first minimum over d of S(x'+d, d) with
 // x'+d < W; a pixel is invalid when x - dL < 0 or |dL - dR(x - dL)| > tol.
+// Optional depth output fx*B/disparity for valid pixels with disparity > 0.
 //
 // Mapping: lanes span disparities (8 per lane = one 16-byte chunk of a u16 slab
 // row) so slab reads are coalesced; a warp covers 32/seg pixels at once. The
@@ -120,6 +121,9 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     int16_t* out_i = pr.out_i16
         ? reinterpret_cast<int16_t*>(reinterpret_cast<char*>(pr.out_i16) + (size_t)y * pr.out_i16_pitch)
         : nullptr;
+    float* out_z = pr.out_depth
+        ? reinterpret_cast<float*>(reinterpret_cast<char*>(pr.out_depth) + (size_t)y * pr.out_depth_pitch)
+        : nullptr;
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
         const int dl = best_d[x];
         bool valid = true;
@@ -129,6 +133,10 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         }
         out[x] = valid ? disp[x] : pr.invalid_value;
         if (out_i) out_i[x] = (int16_t)(valid ? dl : -1);
+        // Depth epilogue: depth = fx * baseline / disparity (the conversion the
+        // reference leaves to its caller, kernels/sgm.rs:284-286).
+        if (out_z)
+            out_z[x] = (valid && disp[x] > 0.0f) ? __fdiv_rn(pr.depth_scale, disp[x]) : pr.depth_invalid;
     }
 }
 

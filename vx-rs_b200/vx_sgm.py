@@ -58,6 +58,39 @@ class _CConfig(ctypes.Structure):
                 ("lr_tolerance", ctypes.c_uint32), ("invalid_value", ctypes.c_float)]
 
 
+class _CIntrinsics(ctypes.Structure):
+    _fields_ = [("fx", ctypes.c_float), ("fy", ctypes.c_float), ("cx", ctypes.c_float),
+                ("cy", ctypes.c_float), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class _CDepthMap(ctypes.Structure):
+    _fields_ = [("texture", _P), ("intrinsics", _CIntrinsics), ("min_depth", ctypes.c_float),
+                ("max_depth", ctypes.c_float)]
+
+
+@dataclass
+class CameraIntrinsics:
+    """vx-vision/src/types_3d.rs:254-267."""
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    width: int
+    height: int
+
+    def to_c(self) -> _CIntrinsics:
+        return _CIntrinsics(self.fx, self.fy, self.cx, self.cy, self.width, self.height)
+
+
+@dataclass
+class DepthMap:
+    """vx-vision/src/types_3d.rs:384-410: the disparity texture with intrinsics and range."""
+    texture: "Texture"
+    intrinsics: CameraIntrinsics
+    min_depth: float
+    max_depth: float
+
+
 def _sig(name, restype, *argtypes):
     fn = getattr(_lib, name)
     fn.restype = restype
@@ -86,6 +119,10 @@ _img_pitch = _sig("vx_image_pitch", ctypes.c_size_t, _P)
 _cfg_default = _sig("vx_sgm_config_default", None, ctypes.POINTER(_CConfig))
 _sgm_create = _sig("vx_sgm_create", ctypes.c_int, _P, ctypes.POINTER(_P))
 _sgm_destroy = _sig("vx_sgm_destroy", None, _P)
+_sgm_compute_depth = _sig("vx_sgm_compute", ctypes.c_int, _P, _P, _P, _P, ctypes.POINTER(_CConfig),
+                          ctypes.POINTER(_CIntrinsics), ctypes.c_float, _P,
+                          ctypes.POINTER(_CDepthMap))
+_ctx_ws_limit = _sig("vx_ctx_set_workspace_limit", ctypes.c_int, _P, ctypes.c_size_t)
 _sgm_compute = _sig("vx_sgm_compute_disparity", ctypes.c_int, _P, _P, _P, _P, _P, _P,
                     ctypes.POINTER(_CConfig), _P)
 _sgm_batch = _sig("vx_sgm_compute_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
@@ -172,6 +209,10 @@ class Context:
 
     def synchronize(self):
         _check(_ctx_sync(self._h))
+
+    def set_workspace_limit(self, nbytes: int):
+        """Batches needing more device workspace run as consecutive sub-batches."""
+        _check(_ctx_ws_limit(self._h, int(nbytes)))
 
     def enable_stage_timing(self, on: bool = True):
         _check(_ctx_timing(self._h, int(bool(on))))
@@ -288,6 +329,22 @@ class SGMStereo:
         _check(_sgm_compute(self._h, ctx.handle, left.handle, right.handle, output.handle,
                             output_i16.handle if output_i16 is not None else None,
                             ctypes.byref(c), _P(stream) if stream else None))
+
+    def compute(self, ctx: Context, left: Texture, right: Texture, config: SGMStereoConfig,
+                intrinsics: CameraIntrinsics, baseline: float,
+                depth_out: Texture | None = None) -> DepthMap:
+        """SGMStereo::compute (kernels/sgm.rs:268-288): a DepthMap over a new F32 disparity
+        texture (no conversion, like the reference); depth_out optionally receives
+        fx * baseline / disparity."""
+        c = config.to_c()
+        ci = intrinsics.to_c()
+        dm = _CDepthMap()
+        _check(_sgm_compute_depth(self._h, ctx.handle, left.handle, right.handle, ctypes.byref(c),
+                                  ctypes.byref(ci), float(baseline),
+                                  depth_out.handle if depth_out is not None else None,
+                                  ctypes.byref(dm)))
+        tex = Texture(ctx, _P(dm.texture), left.width, left.height, FORMAT_F32)
+        return DepthMap(tex, intrinsics, float(dm.min_depth), float(dm.max_depth))
 
     def compute_batch(self, ctx: Context, lefts, rights, outputs, configs, outputs_i16=None,
                       stream: int | None = None):
