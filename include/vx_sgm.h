@@ -228,27 +228,36 @@ vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms,
 
 /* ---- Serving loop (no reference counterpart) ----------------------------
  * Continuous batching of stereo requests of any size and config under a
- * device-memory budget. submit() copies the images into pinned host memory and
- * queues the request; a scheduler thread admits queued requests in arrival
- * order while their device bytes (vx_sgm_workspace_bytes + images + outputs)
- * fit the budget, batches up to max_batch of them, and runs the batch on one of
+ * device-memory budget. Creating the server takes a device arena of exactly
+ * memory_budget_bytes from the context's pool and a pinned host staging arena
+ * of host_staging_bytes (0: budget / 16, clamped to 256 MB .. 4 GB); serving
+ * then allocates from these alone. submit() copies the images into the staging
+ * arena and queues the request; a scheduler thread admits queued requests in
+ * arrival order while an upper bound of their device bytes (workspace + images
+ * + outputs + plan tables) fits the largest free block of the arena, batches up
+ * to max_batch of them into one block, and runs the batch on one of
  * max_inflight_batches streams (upload, batched SGM, download); batches on
  * different streams overlap, and new requests join the next batch as soon as a
  * stream and memory are free. A request's result does not depend on the other
  * requests of its batch. A request larger than the whole budget is rejected
- * with VX_ERR_BUDGET. Device buffers come from the context's resident pool;
- * creating the server maps the whole budget into that pool up front. */
+ * with VX_ERR_BUDGET. */
 typedef struct vx_sgm_server vx_sgm_server;
 typedef struct vx_server_config {
     size_t memory_budget_bytes;
     uint32_t max_batch;
     uint32_t max_inflight_batches;
+    size_t host_staging_bytes;            /* 0 = default */
 } vx_server_config;
 typedef struct vx_server_stats {
     uint64_t submitted, completed, rejected, cancelled, failed, batches;
     uint64_t queued;                      /* waiting for admission */
-    uint64_t inflight_bytes;              /* budget in use */
+    uint64_t inflight_bytes;              /* device arena bytes held by running batches */
     uint64_t completed_pixel_disparities; /* sum of W*H*D of completed requests */
+    uint64_t pool_reserved_bytes;         /* device memory the context's pool holds */
+    uint64_t pinned_bytes;                /* pinned host memory held (arena + overflow) */
+    uint64_t max_launch_us;               /* longest host time to issue one batch */
+    uint64_t max_pinned_alloc_us;         /* longest pinned allocation past the arena */
+    uint64_t staging_overflows;           /* requests staged past the pinned arena */
 } vx_server_stats;
 
 vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config* cfg,

@@ -38,6 +38,41 @@ def test_served_results_equal_solo(gpu_ctx, sgm):
         assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
 
 
+def test_serving_allocates_nothing_after_start(gpu_ctx, sgm):
+    """The device arena and the pinned staging arena are taken at creation; serving a
+    stream of mixed requests grows neither the context's pool nor the pinned memory."""
+    reqs = [_request(i) for i in range(24)]
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=4 * biggest, max_batch=4,
+                        max_inflight_batches=2)
+    st0 = srv.stats()
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    for i in ids:
+        srv.wait(i)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["pool_reserved_bytes"] == st0["pool_reserved_bytes"]
+    assert st["pinned_bytes"] == st0["pinned_bytes"] and st["staging_overflows"] == 0
+    assert st["inflight_bytes"] == 0
+
+
+def test_staging_overflow_still_serves(gpu_ctx, sgm):
+    """A staging arena too small for the queued requests: the excess requests get
+    their own pinned buffers and the results are unchanged."""
+    reqs = [_request(i) for i in range(8)]
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=3 * biggest, max_batch=4,
+                        max_inflight_batches=2, host_staging_bytes=1 << 18)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    results = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["staging_overflows"] > 0
+    for (L, R, c), (d, di, _) in zip(reqs, results):
+        assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="overflow staging")
+
+
 def test_oversize_request_is_rejected(gpu_ctx, sgm):
     srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=1 << 20, max_batch=4)
     L, R, c = _request(1)

@@ -42,7 +42,10 @@
 // Census words of the next group are loaded while the current group is
 // processed. Pixels whose window may reach x-d < 0 take a second body with the
 // border test, picked by a warp-uniform branch. Results leave as 16-byte stores
-// into this path's slab.
+// into this path's slab, one byte per disparity: the values of a vector are
+// bounded by the census cost plus P2 unless the in-place o1 term pulls them
+// below m (then they wrap), so almost every vector fits bytes; one that does
+// not is marked with 0xFF in byte 0 and written exactly to a u16 shadow slab.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,6 +64,12 @@ constexpr unsigned kFull = 0xffffffffu;
 __device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
     uint32_t r;
     asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
 }
 
@@ -120,6 +129,7 @@ struct PixelState {
     uint32_t km;     // Lp = t + C - m
     uint32_t f;      // o1 of the next disparity (low half)
     uint32_t mn;     // running min of the new values (per half)
+    uint32_t mx;     // running max of the new values (per half, d < D)
 };
 
 // Matching costs of one group from its 8 right-census words; x-d < 0 gives 64.
@@ -133,15 +143,13 @@ __device__ __forceinline__ void group_costs(uint32_t (&c)[8], const CT lc, const
     }
 }
 
-// Writes the warp's output tile to the slab: lanes [la, lb] hold the results of
-// one pixel step; lane row p's vector goes to dst0 + p * stride (in u16), and
-// 16-byte word g of it to +8g. Words are distributed over the lanes in address
-// order, so that consecutive lanes write consecutive 16 bytes of a vector
-// (streaming stores: slabs are read once by the WTA kernel and must not push
-// the census planes, which every path re-reads, out of L2).
-__device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int row_words, int G,
-                                           int la, int lb, uint16_t* __restrict__ dst0,
-                                           size_t stride, int lane) {
+// Writes the warp's output tile to a wide (u16) slab: lanes [la, lb] hold the
+// results of one pixel step; row p's vector goes to dst0 + p * stride (in u16),
+// and 16-byte word g of it to +8g. Words are distributed over the lanes in
+// address order, so consecutive lanes write consecutive 16 bytes of a vector.
+__device__ __forceinline__ void flush_tile_wide(const uint4* __restrict__ tile, int row_words, int G,
+                                                int la, int lb, uint16_t* __restrict__ dst0,
+                                                size_t stride, int lane) {
     __syncwarp();
     // Word c = (p - la) * G + g of the run, walked with a running (p, g) so
     // that no division is needed per word: lane starts at c = lane, steps 32.
@@ -156,6 +164,54 @@ __device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int r
             g -= G;
             ++p;
         }
+    }
+    __syncwarp();
+}
+
+// Writes the warp's output tile to the byte slab: lanes [la, lb] hold the
+// results of one pixel step; row p's vector goes to dst0 + p * stride bytes,
+// its 16-byte chunk h holding d = 16h..16h+15 (tile words 2h and 2h+1, the low
+// byte of every u16). A row whose bit is set in em (escaped) gets 0xFF in
+// byte 0 and its exact u16 words at sh0 + p * sstride (in u16) of the shadow.
+// Chunks are distributed over the lanes in address order, so that consecutive
+// lanes write consecutive 16 bytes of a vector (streaming stores: slabs are
+// read once by the WTA kernel and must not push the census planes, which every
+// path re-reads, out of L2).
+__device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int row_words, int G,
+                                           int la, int lb, unsigned em, uint8_t* __restrict__ dst0,
+                                           size_t stride, uint16_t* __restrict__ sh0,
+                                           size_t sstride, int lane) {
+    __syncwarp();
+    // Chunk c = (p - la) * V + h of the run, walked with a running (p, h) so
+    // that no division is needed per chunk: lane starts at c = lane, steps 32.
+    const int V = (G + 1) >> 1;
+    const int n = (lb - la + 1) * V;
+    const int q = 32 / V, r = 32 % V;
+    int p = la + lane / V, h = lane % V;
+    for (int c = lane; c < n; c += 32) {
+        const uint4* row = tile + p * row_words;
+        const uint4 a = row[2 * h];
+        const uint4 b = 2 * h + 1 < G ? row[2 * h + 1] : make_uint4(0u, 0u, 0u, 0u);
+        uint4 o;
+        o.x = __byte_perm(a.x, a.y, 0x6420);
+        o.y = __byte_perm(a.z, a.w, 0x6420);
+        o.z = __byte_perm(b.x, b.y, 0x6420);
+        o.w = __byte_perm(b.z, b.w, 0x6420);
+        if (h == 0 && ((em >> p) & 1u)) o.x |= 0xFFu;
+        __stcs(reinterpret_cast<uint4*>(dst0 + (size_t)p * stride + 16 * h), o);
+        h += r;
+        p += q;
+        if (h >= V) {
+            h -= V;
+            ++p;
+        }
+    }
+    // Escaped vectors (rare): the warp writes their u16 words, one row at a time.
+    while (em) {
+        const int pe = __ffs(em) - 1;              // bit p of em = row p (la <= p <= lb)
+        em &= em - 1;
+        for (int g = lane; g < G; g += 32)
+            __stcs(reinterpret_cast<uint4*>(sh0 + (size_t)pe * sstride + 8 * g), tile[pe * row_words + g]);
     }
     __syncwarp();
 }
@@ -188,13 +244,15 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
     }
     if (!LAST) {
         ps.mn = vmin2(ps.mn, vmin2(vmin2(out[0], out[1]), vmin2(out[2], out[3])));
+        ps.mx = vmax2(ps.mx, vmax2(vmax2(out[0], out[1]), vmax2(out[2], out[3])));
     } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            uint32_t pm = out[j];
-            if (2 * j > k.last_j) pm |= 0x0000FFFFu;   // pads never count
-            if (2 * j + 1 > k.last_j) pm |= 0xFFFF0000u;
+            uint32_t pm = out[j], po = out[j];
+            if (2 * j > k.last_j) { pm |= 0x0000FFFFu; po &= 0xFFFF0000u; }   // pads never count
+            if (2 * j + 1 > k.last_j) { pm |= 0xFFFF0000u; po &= 0x0000FFFFu; }
             ps.mn = vmin2(ps.mn, pm);
+            ps.mx = vmax2(ps.mx, po);
         }
     }
     return make_uint4(out[0], out[1], out[2], out[3]);
@@ -206,12 +264,14 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
 // x-d >= 0 when CHECK. prefetch(d) hints census words into L1 (horizontal
 // paths). active: this lane's scanline covers the pixel; an idle lane keeps (or
 // resets to) the zero state a scanline starts from. otile = this lane's row of
-// the warp's shared-memory output tile (one 16-byte word per group). Software pipeline over groups (loop unrolled by two, register sets in
-// ping-pong): while group g runs its min/add chain, the census words and state
-// of group g+1 are in flight, and g+1's costs are formed right after g's chain,
-// so neither load nor popcount latency sits on the chain.
+// the warp's shared-memory output tile (one 16-byte word per group). Returns
+// whether the new vector escapes the byte slab. Software pipeline over groups
+// (loop unrolled by two, register sets in ping-pong): while group g runs its
+// min/add chain, the census words and state of group g+1 are in flight, and
+// g+1's costs are formed right after g's chain, so neither load nor popcount
+// latency sits on the chain.
 template <bool CHECK, typename CT, typename GetR, typename Prefetch>
-__device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
+__device__ __forceinline__ bool sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
                                           const GetR& getR, const Prefetch& prefetch,
                                           const int x, const bool active, const ScanConst& k,
                                           uint4* __restrict__ otile) {
@@ -222,6 +282,7 @@ __device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, co
     ps.km = 0u - m;
     ps.f = 0xFFFFu;            // o1 at d = 0
     ps.mn = 0xFFFFFFFFu;
+    ps.mx = 0u;
     auto load = [&](CT (&r)[8], int g) {
         prefetch(8 * (g + 2));
 #pragma unroll
@@ -269,6 +330,9 @@ __device__ __forceinline__ void sgm_pixel(const uint32_t tstate, uint32_t& m, co
     }
     tmem_wait_st();            // the next pixel reads this state back
     m = active ? min(ps.mn & 0xFFFFu, ps.mn >> 16) : 0u;
+    // The vector escapes the byte slab when a value is 255 or more, so that a
+    // stored byte vector never holds the marker 0xFF.
+    return max(ps.mx & 0xFFFFu, ps.mx >> 16) >= 0xFFu;
 }
 
 __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
@@ -315,7 +379,9 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
 
     const CT* __restrict__ CL = static_cast<const CT*>(pr.census_l);
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
-    uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+    uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+    uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
+    const int Dv = pr.nd_vec;
 
     // Stage the right-census segment [xb-(Dp-1), xb+31] of the step's row in
     // 16-byte chunks from the aligned word at or below its start. The planes are
@@ -363,16 +429,20 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         auto no_prefetch = [](int) {};
         const int xb = k0 + dx * t;             // smallest x of the warp
         uint4* otile = tile + lane * row_words;
-        if (xb >= Dp - 1)
-            sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
-        else
-            sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
+        const bool esc = xb >= Dp - 1
+                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile)
+                             : sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
         // Active lanes are one run of consecutive pixels of row y.
         const unsigned act = __ballot_sync(kFull, active);
+        const unsigned em = __ballot_sync(kFull, active && esc);
         if (act) {
             const int la = __ffs(act) - 1, lb = 31 - __clz(act);
-            flush_tile(tile, row_words, k.G, la, lb, out + ((size_t)y * W + xb) * Dp, (size_t)Dp,
-                       lane);
+            const size_t pix0 = (size_t)y * W + xb;
+            if (pr.wide_slabs)
+                flush_tile_wide(tile, row_words, k.G, la, lb, shd + pix0 * Dp, (size_t)Dp, lane);
+            else
+                flush_tile(tile, row_words, k.G, la, lb, em, out + pix0 * Dv, (size_t)Dv,
+                           shd + pix0 * Dp, (size_t)Dp, lane);
         }
         __syncwarp();
     }
@@ -398,7 +468,9 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const size_t band = (size_t)(first >> 5) * W;
     const CT* __restrict__ CL = static_cast<const CT*>(pr.census_lt) + band * 32 + lane;
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_rt) + band * 32 + lane;
-    uint16_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+    uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
+    uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
+    const int Dv = pr.nd_vec;
     (void)H;
 
     clear_state(tstate, k.G);
@@ -422,13 +494,17 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
             }
         };
         uint4* otile = tile + lane * row_words;
-        if (x >= Dp - 1)
-            sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
-        else
-            sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
+        const bool esc = x >= Dp - 1
+                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile)
+                             : sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
+        const unsigned em = __ballot_sync(kFull, active && esc);
         // Rows first..first+nrows-1, one vector per row at column x.
-        flush_tile(tile, row_words, k.G, 0, nrows - 1, out + ((size_t)first * W + x) * Dp,
-                   (size_t)W * Dp, lane);
+        const size_t pix0 = (size_t)first * W + x;
+        if (pr.wide_slabs)
+            flush_tile_wide(tile, row_words, k.G, 0, nrows - 1, shd + pix0 * Dp, (size_t)W * Dp, lane);
+        else
+            flush_tile(tile, row_words, k.G, 0, nrows - 1, em, out + pix0 * Dv, (size_t)W * Dv,
+                       shd + pix0 * Dp, (size_t)W * Dp, lane);
     }
 }
 

@@ -45,25 +45,6 @@ void destroy_entry(vx_sgm::GraphEntry* e, cudaStream_t stream) {
 }
 
 // Refreshes the pointer fields of the bucket's pair table for this call.
-void rebind_pointers(vxsgm::Plan& plan, const std::vector<PairSpec>& specs) {
-    for (size_t i = 0; i < specs.size(); ++i) {
-        PairDev& pd = plan.pairs[i];
-        const PairSpec& s = specs[i];
-        pd.left = static_cast<const uint8_t*>(s.left->ptr);
-        pd.right = static_cast<const uint8_t*>(s.right->ptr);
-        pd.left_pitch = s.left->pitch;
-        pd.right_pitch = s.right->pitch;
-        pd.out_f32 = static_cast<float*>(s.out_f32->ptr);
-        pd.out_f32_pitch = s.out_f32->pitch;
-        pd.out_i16 = s.out_i16 ? static_cast<int16_t*>(s.out_i16->ptr) : nullptr;
-        pd.out_i16_pitch = s.out_i16 ? s.out_i16->pitch : 0;
-        pd.out_depth = s.out_depth ? static_cast<float*>(s.out_depth->ptr) : nullptr;
-        pd.out_depth_pitch = s.out_depth ? s.out_depth->pitch : 0;
-        pd.depth_scale = s.depth_scale;
-        pd.depth_invalid = s.depth_invalid;
-    }
-}
-
 }  // namespace
 
 vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,

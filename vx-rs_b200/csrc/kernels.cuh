@@ -6,7 +6,7 @@
 namespace vxsgm {
 
 // One stereo pair of a launch, as the kernels see it. Built on the host by the
-// planner (plan.cpp) and copied into the launch's workspace.
+// planner (planner.cpp) and copied into the launch's workspace.
 struct PairDev {
     const uint8_t* left;   // U8 images, row pitch in bytes
     const uint8_t* right;
@@ -15,8 +15,18 @@ struct PairDev {
     void* census_r;
     void* census_lt;       // census words in 32-row bands: ((y/32)*W + x)*32 + y%32
     void* census_rt;
-    uint16_t* slabs;       // num_paths slabs of H*W*Dp u16 (pixel-major, d-minor)
-    size_t slab_stride;    // elements per slab = H*W*Dp
+    // Per-path costs, pixel-major and d-minor, in one of two formats:
+    //  * byte slabs (wide_slabs = 0): num_paths slabs of H*W vectors of Dv bytes.
+    //    A vector whose values are all <= 254 is stored as bytes; any other has
+    //    byte 0 set to 0xFF (the escape marker) and its exact u16 values in the
+    //    shadow slab at the same pixel.
+    //  * wide slabs (wide_slabs = 1, for configurations whose costs mostly
+    //    exceed a byte): every vector in the shadow slabs; no byte slabs.
+    uint8_t* slabs;
+    size_t slab_stride;    // bytes per slab = H*W*Dv (0 for wide slabs)
+    uint16_t* shadow;      // num_paths slabs of H*W*Dp u16
+    size_t shadow_stride;  // elements per shadow slab = H*W*Dp
+    int wide_slabs;
     float* out_f32;        // subpixel (or integer) disparity, pitch in bytes
     size_t out_f32_pitch;
     int16_t* out_i16;      // optional integer disparity, pitch in bytes
@@ -28,6 +38,7 @@ struct PairDev {
     int width, height;
     int nd;                // number of disparities D (1..256)
     int nd_pad;            // Dp = D rounded up to 8
+    int nd_vec;            // Dv = D rounded up to 16 (bytes per stored vector)
     int num_paths;
     int p1, p2;            // ushort(p1), ushort(p2)
     int rx, ry;            // census radii

@@ -2,6 +2,7 @@
 // queue of (pair, path, scanline-group) units and issues the launches.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "vx_internal.hpp"
@@ -21,6 +22,58 @@ const int kDirs[8][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {1, 
 
 int census_bits(const vx_sgm_config& cfg) {
     return (int)((2 * cfg.census_radius_x + 1) * (2 * cfg.census_radius_y + 1)) - 1;
+}
+
+// Slab format of a configuration. A path cost is at most the matching cost
+// (<= 64: census bits or the border cost) plus P2 unless it wraps below zero,
+// so byte vectors hold nearly every vector when 64 + P2 <= 254; otherwise most
+// vectors would escape and u16 slabs alone are smaller and read faster.
+// VX_SGM_SLAB_FORMAT=bytes|wide forces one format (both are exact for every
+// configuration; the tests run each on the other's configurations).
+bool wide_slabs(const vx_sgm_config& c) {
+    if (const char* f = std::getenv("VX_SGM_SLAB_FORMAT")) {
+        if (std::strcmp(f, "bytes") == 0) return false;
+        if (std::strcmp(f, "wide") == 0) return true;
+    }
+    return 64 + (int)(uint16_t)c.p2 > 254;
+}
+
+size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg,
+                            size_t census_word_bytes) {
+    const size_t npx = (size_t)width * height, ct = census_word_bytes, P = cfg.num_paths;
+    const size_t dp = (cfg.num_disparities + 7) / 8 * 8;
+    const size_t dv = (cfg.num_disparities + 15) / 16 * 16;
+    const size_t banded = (size_t)((height + 31) / 32) * 32 * width * ct;
+    const size_t guard = kCensusGuardWords * ct;
+    const size_t bytes = wide_slabs(cfg) ? 0 : align_up(npx * dv * P);
+    return 2 * align_up(npx * ct + 2 * guard) + 2 * align_up(banded) + bytes +
+           align_up(npx * dp * P * sizeof(uint16_t));
+}
+
+size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
+    const size_t P = cfg.num_paths;
+    const size_t units = P * (((size_t)width + height - 1 + 31) / 32);
+    return sizeof(PairDev) + P * sizeof(JobDev) + units * sizeof(UnitDev) + sizeof(unsigned) +
+           4 * kAlign;
+}
+
+void rebind_pointers(Plan& plan, const std::vector<PairSpec>& specs) {
+    for (size_t i = 0; i < specs.size(); ++i) {
+        PairDev& pd = plan.pairs[i];
+        const PairSpec& s = specs[i];
+        pd.left = static_cast<const uint8_t*>(s.left->ptr);
+        pd.right = static_cast<const uint8_t*>(s.right->ptr);
+        pd.left_pitch = s.left->pitch;
+        pd.right_pitch = s.right->pitch;
+        pd.out_f32 = static_cast<float*>(s.out_f32->ptr);
+        pd.out_f32_pitch = s.out_f32->pitch;
+        pd.out_i16 = s.out_i16 ? static_cast<int16_t*>(s.out_i16->ptr) : nullptr;
+        pd.out_i16_pitch = s.out_i16 ? s.out_i16->pitch : 0;
+        pd.out_depth = s.out_depth ? static_cast<float*>(s.out_depth->ptr) : nullptr;
+        pd.out_depth_pitch = s.out_depth ? s.out_depth->pitch : 0;
+        pd.depth_scale = s.depth_scale;
+        pd.depth_invalid = s.depth_invalid;
+    }
 }
 
 vx_status validate_pair(const PairSpec& p) {
@@ -74,7 +127,8 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         const PairSpec& s = specs[i];
         const vx_sgm_config& c = s.cfg;
         const int W = (int)s.left->width, H = (int)s.left->height;
-        const int D = (int)c.num_disparities, Dp = (D + 7) / 8 * 8, P = (int)c.num_paths;
+        const int D = (int)c.num_disparities, Dp = (D + 7) / 8 * 8, Dv = (D + 15) / 16 * 16;
+        const int P = (int)c.num_paths;
         PairDev& pd = pl.pairs[i];
         std::memset(&pd, 0, sizeof pd);
         pd.left = static_cast<const uint8_t*>(s.left->ptr);
@@ -93,6 +147,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         pd.height = H;
         pd.nd = D;
         pd.nd_pad = Dp;
+        pd.nd_vec = Dv;
         pd.num_paths = P;
         pd.p1 = (int)(uint16_t)c.p1;  // ushort(params.p1), SGMStereo.metal:155
         pd.p2 = (int)(uint16_t)c.p2;
@@ -110,9 +165,11 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         pl.max_rx = std::max(pl.max_rx, pd.rx);
         pl.max_ry = std::max(pl.max_ry, pd.ry);
 
-        // Workspace-relative data: 4 census planes then P slabs.
+        // Workspace-relative data: 4 census planes, P byte slabs, P shadow slabs
+        // (the layout pair_workspace_bytes sizes).
         const size_t npx = (size_t)W * H;
         pl.pair_data_off[i] = data;
+        const size_t data0 = data;
         const size_t guard = kCensusGuardWords * ct;
         const size_t cplane = align_up(npx * ct + 2 * guard);                  // guarded row-major
         const size_t bplane = align_up((size_t)((H + 31) / 32) * 32 * W * ct);  // banded copy
@@ -121,9 +178,15 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         pd.census_lt = reinterpret_cast<void*>(data + 2 * cplane);
         pd.census_rt = reinterpret_cast<void*>(data + 2 * cplane + bplane);
         data += 2 * cplane + 2 * bplane;
-        pd.slab_stride = npx * (size_t)Dp;
-        pd.slabs = reinterpret_cast<uint16_t*>(data);
-        data += align_up(pd.slab_stride * P * sizeof(uint16_t));
+        pd.wide_slabs = wide_slabs(c) ? 1 : 0;
+        pd.slab_stride = pd.wide_slabs ? 0 : npx * (size_t)Dv;
+        pd.slabs = reinterpret_cast<uint8_t*>(data);
+        data += align_up(pd.slab_stride * P);
+        pd.shadow_stride = npx * (size_t)Dp;
+        pd.shadow = reinterpret_cast<uint16_t*>(data);
+        data += align_up(pd.shadow_stride * P * sizeof(uint16_t));
+        if (data - data0 != pair_workspace_bytes((uint32_t)W, (uint32_t)H, c, ct))
+            return fail(VX_ERR_GPU, "planner: pair layout and its size formula disagree");
 
         pl.dp_max = std::max(pl.dp_max, Dp);
         for (int p = 0; p < P; ++p) {
@@ -192,7 +255,8 @@ void bind_plan(Plan& pl, char* base) {
         pd.census_r = data + reinterpret_cast<size_t>(pd.census_r);
         pd.census_lt = data + reinterpret_cast<size_t>(pd.census_lt);
         pd.census_rt = data + reinterpret_cast<size_t>(pd.census_rt);
-        pd.slabs = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.slabs));
+        pd.slabs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.slabs));
+        pd.shadow = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.shadow));
     }
 }
 

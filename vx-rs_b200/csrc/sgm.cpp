@@ -184,14 +184,7 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
 
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg) {
     if (!cfg) return 0;
-    const size_t npx = (size_t)width * height;
-    const size_t ct = census_bits(*cfg) > 32 ? 8 : 4;
-    const size_t dp = (cfg->num_disparities + 7) / 8 * 8;
-    auto al = [](size_t v) { return (v + 255) / 256 * 256; };
-    const size_t banded = (size_t)((height + 31) / 32) * 32 * width * ct;
-    const size_t guard = kCensusGuardWords * ct;
-    return 2 * al(npx * ct + 2 * guard) + 2 * al(banded) +
-           al(npx * dp * cfg->num_paths * sizeof(uint16_t));
+    return pair_workspace_bytes(width, height, *cfg, census_bits(*cfg) > 32 ? 8 : 4);
 }
 
 vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,
@@ -223,16 +216,23 @@ vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, cons
         if (census_left) fetch_census(pd.census_l, census_left);
         if (census_right) fetch_census(pd.census_r, census_right);
         if (path_costs || cost_volume) {
-            std::vector<uint16_t> slabs(pd.slab_stride * P);
-            cudaMemcpy(slabs.data(), pd.slabs, slabs.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+            const size_t Dv = pd.nd_vec;
+            std::vector<uint8_t> slabs(pd.slab_stride * P + 1);
+            std::vector<uint16_t> shadow(pd.shadow_stride * P);
+            if (!pd.wide_slabs) cudaMemcpy(slabs.data(), pd.slabs, slabs.size() - 1, cudaMemcpyDeviceToHost);
+            cudaMemcpy(shadow.data(), pd.shadow, shadow.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost);
             if (cost_volume) std::memset(cost_volume, 0, npx * D * sizeof(uint16_t));
             for (size_t p = 0; p < P; ++p)
-                for (size_t i = 0; i < npx; ++i)
+                for (size_t i = 0; i < npx; ++i) {
+                    const uint8_t* vb = &slabs[p * pd.slab_stride + i * Dv];
+                    const uint16_t* vs = &shadow[p * pd.shadow_stride + i * Dp];
+                    const bool escaped = pd.wide_slabs || vb[0] == 0xFF;   // u16 values in the shadow
                     for (size_t d = 0; d < D; ++d) {
-                        const uint16_t v = slabs[p * pd.slab_stride + i * Dp + d];
+                        const uint16_t v = escaped ? vs[d] : vb[d];
                         if (path_costs) path_costs[(p * npx + i) * D + d] = v;
                         if (cost_volume) cost_volume[i * D + d] = (uint16_t)(cost_volume[i * D + d] + v);
                     }
+                }
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "debug dump copy");

@@ -84,6 +84,7 @@ struct PairSpec {
 
 vx_status validate_pair(const PairSpec& p);
 int census_bits(const vx_sgm_config& cfg);
+bool wide_slabs(const vx_sgm_config& cfg);
 
 // Host-side plan of one batched launch sequence (planner.cpp).
 struct Plan {
@@ -100,6 +101,15 @@ struct Plan {
 };
 
 vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan);
+// Workspace bytes of one pair's census planes and path slabs with census words
+// of census_word_bytes (a batch uses 8-byte words for all its pairs as soon as
+// one needs them), and an upper bound of its share of the plan tables.
+size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg,
+                            size_t census_word_bytes);
+size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg);
+// Points plan.pairs at the images and outputs of specs (same sizes and order
+// as the specs the plan was built from).
+void rebind_pointers(Plan& plan, const std::vector<PairSpec>& specs);
 // Resolves the workspace-relative pointers of plan.pairs against `base`.
 void bind_plan(Plan& plan, char* base);
 // Issues the whole batch (census, aggregation, WTA) on `stream` with the

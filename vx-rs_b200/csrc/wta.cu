@@ -11,8 +11,14 @@
 // x'+d < W; a pixel is invalid when x - dL < 0 or |dL - dR(x - dL)| > tol.
 // Optional depth output fx*B/disparity for valid pixels with disparity > 0.
 //
-// Mapping: lanes span disparities (8 per lane = one 16-byte chunk of a u16 slab
-// row) so slab reads are coalesced; a warp covers 32/seg pixels at once. The
+// Mapping: lanes span disparities (8 per lane: 8 bytes of a byte-slab vector,
+// or 16 bytes of a wide one) so slab reads are coalesced; a warp covers 32/seg
+// pixels at once. Sums are kept as u16 pairs (d, d+1) in 32-bit words and added
+// per half (wrapping modulo 2^16); a byte is widened into its half by a byte
+// permute. The loads of all paths of a pixel group are issued before any is
+// used (the path count is a template parameter). An escaped byte vector (0xFF
+// in byte 0, held by the pixel's first lane) is left out of the byte sum and
+// its exact u16 values are read from the shadow slab instead. The
 // argmin is a min over the key (S << 8 | d), which orders by cost then by d,
 // i.e. the first minimum. The right-view argmin of the row is accumulated in
 // shared memory with atomicMin on the same keys.
@@ -36,13 +42,71 @@ __device__ __forceinline__ int find_pair_by_row(const PairDev* pairs, int n, int
     return lo;
 }
 
-__global__ void __launch_bounds__(kWtaThreads)
+// acc[k] += (d = 2k, d = 2k+1) of 8 byte values (v.x: d 0..3, v.y: d 4..7).
+__device__ __forceinline__ void add_bytes(uint32_t (&acc)[4], const uint2 v) {
+    acc[0] = __vadd2(acc[0], __byte_perm(v.x, 0u, 0x4140));
+    acc[1] = __vadd2(acc[1], __byte_perm(v.x, 0u, 0x4342));
+    acc[2] = __vadd2(acc[2], __byte_perm(v.y, 0u, 0x4140));
+    acc[3] = __vadd2(acc[3], __byte_perm(v.y, 0u, 0x4342));
+}
+// The same for 8 u16 values (already (d, d+1) pairs).
+__device__ __forceinline__ void add_u16(uint32_t (&acc)[4], const uint4 a) {
+    acc[0] = __vadd2(acc[0], a.x);
+    acc[1] = __vadd2(acc[1], a.y);
+    acc[2] = __vadd2(acc[2], a.z);
+    acc[3] = __vadd2(acc[3], a.w);
+}
+
+// Sum over the NP paths of the 8 disparities d = 8c..8c+7 of pixel pix (lanes
+// with act = false contribute nothing but take part in the warp shuffles).
+template <int NP, bool WIDE>
+__device__ __forceinline__ void sum_paths(const PairDev& pr, size_t pix, int c, bool act, int lead,
+                                          uint32_t (&acc)[4]) {
+    const int Dp = pr.nd_pad;
+    const bool in_dp = act && 8 * c < Dp;           // lanes past Dp (Dv = Dp + 8) read no shadow
+    const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+    if (WIDE) {
+        uint4 v[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p)
+            v[p] = in_dp ? __ldcs(reinterpret_cast<const uint4*>(pr.shadow + pr.shadow_stride * p +
+                                                                   pix * Dp + 8 * c))
+                         : z4;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) add_u16(acc, v[p]);
+        return;
+    }
+    const int Dv = pr.nd_vec;
+    uint2 v[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+        v[p] = act ? __ldcs(reinterpret_cast<const uint2*>(pr.slabs + pr.slab_stride * p + pix * Dv + 8 * c))
+                   : make_uint2(0u, 0u);
+    unsigned esc = 0u;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        if ((__shfl_sync(kFull, v[p].x, lead) & 0xFFu) == 0xFFu)
+            esc |= 1u << p;
+        else
+            add_bytes(acc, v[p]);
+    }
+    if (__any_sync(kFull, esc != 0u)) {             // rare: escaped vectors from the shadow
+#pragma unroll
+        for (int p = 0; p < NP; ++p)
+            if (in_dp && ((esc >> p) & 1u))
+                add_u16(acc, __ldcs(reinterpret_cast<const uint4*>(pr.shadow + pr.shadow_stride * p +
+                                                                     pix * Dp + 8 * c)));
+    }
+}
+
+// Five CTAs per SM (at most 51 registers a thread) keep enough slab loads in flight.
+__global__ void __launch_bounds__(kWtaThreads, 5)
 wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint32_t smem[];
     const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
     const PairDev& pr = pairs[pi];
     const int y = blockIdx.x - pr.row_begin;
-    const int W = pr.width, D = pr.nd, Dp = pr.nd_pad, P = pr.num_paths;
+    const int W = pr.width, D = pr.nd, P = pr.num_paths;
     const bool lr = pr.lr_check != 0;
 
     uint32_t* right_key = smem;                               // W keys (LR only)
@@ -53,34 +117,37 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
     __syncthreads();
 
-    const int chunks = Dp / 8;                      // 16-byte chunks per pixel
+    const int chunks = pr.nd_vec / 8;               // 8-disparity chunks per pixel
     int seg = 1;
     while (seg < chunks) seg <<= 1;                 // lanes per pixel (power of two)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
     const int sub = lane / seg, c = lane % seg;
     const int ppw = 32 / seg;
+    const int kind = (P == 2 ? 0 : P == 4 ? 1 : 2) + (pr.wide_slabs ? 3 : 0);
 
     for (int xb = warp * ppw; xb < W; xb += nwarps * ppw) {
         const int x = xb + sub;
         const bool act = x < W && c < chunks;
+        const size_t pix = (size_t)y * W + (act ? x : 0);
+        uint32_t acc[4] = {0u, 0u, 0u, 0u};         // acc[k] = S(8c+2k) | S(8c+2k+1) << 16
+        switch (kind) {                             // uniform over the CTA
+            case 0: sum_paths<2, false>(pr, pix, c, act, sub * seg, acc); break;
+            case 1: sum_paths<4, false>(pr, pix, c, act, sub * seg, acc); break;
+            case 2: sum_paths<8, false>(pr, pix, c, act, sub * seg, acc); break;
+            case 3: sum_paths<2, true>(pr, pix, c, act, sub * seg, acc); break;
+            case 4: sum_paths<4, true>(pr, pix, c, act, sub * seg, acc); break;
+            default: sum_paths<8, true>(pr, pix, c, act, sub * seg, acc); break;
+        }
         uint32_t s[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) s[j] = 0;
-        if (act) {
-            const size_t off = ((size_t)y * W + x) * Dp + 8 * c;
-            for (int p = 0; p < P; ++p) {
-                const uint4 v = __ldcs(reinterpret_cast<const uint4*>(pr.slabs + pr.slab_stride * p + off));
-                s[0] += v.x & 0xFFFFu; s[1] += v.x >> 16;
-                s[2] += v.y & 0xFFFFu; s[3] += v.y >> 16;
-                s[4] += v.z & 0xFFFFu; s[5] += v.z >> 16;
-                s[6] += v.w & 0xFFFFu; s[7] += v.w >> 16;
-            }
+        for (int k = 0; k < 4; ++k) {
+            s[2 * k] = acc[k] & 0xFFFFu;
+            s[2 * k + 1] = acc[k] >> 16;
         }
         uint32_t best = 0xFFFFFFFFu;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            s[j] &= 0xFFFFu;
             const int d = 8 * c + j;
             if (act && d < D) best = min(best, (s[j] << 8) | (uint32_t)d);
         }

@@ -405,7 +405,7 @@ class SGMStereo:
 
 class _CServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_size_t), ("max_batch", ctypes.c_uint32),
-                ("max_inflight_batches", ctypes.c_uint32)]
+                ("max_inflight_batches", ctypes.c_uint32), ("host_staging_bytes", ctypes.c_size_t)]
 
 
 class ServerStats(ctypes.Structure):
@@ -413,7 +413,10 @@ class ServerStats(ctypes.Structure):
                 ("rejected", ctypes.c_uint64), ("cancelled", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
                 ("queued", ctypes.c_uint64), ("inflight_bytes", ctypes.c_uint64),
-                ("completed_pixel_disparities", ctypes.c_uint64)]
+                ("completed_pixel_disparities", ctypes.c_uint64),
+                ("pool_reserved_bytes", ctypes.c_uint64), ("pinned_bytes", ctypes.c_uint64),
+                ("max_launch_us", ctypes.c_uint64), ("max_pinned_alloc_us", ctypes.c_uint64),
+                ("staging_overflows", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -435,8 +438,9 @@ class Server:
     """Continuous-batching SGM server under a device-memory budget (see vx_sgm.h)."""
 
     def __init__(self, sgm: "SGMStereo", ctx: Context, memory_budget_bytes: int,
-                 max_batch: int = 32, max_inflight_batches: int = 2):
-        c = _CServerConfig(int(memory_budget_bytes), int(max_batch), int(max_inflight_batches))
+                 max_batch: int = 32, max_inflight_batches: int = 2, host_staging_bytes: int = 0):
+        c = _CServerConfig(int(memory_budget_bytes), int(max_batch), int(max_inflight_batches),
+                           int(host_staging_bytes))
         h = _P()
         _check(_srv_create(sgm.handle, ctx.handle, ctypes.byref(c), ctypes.byref(h)))
         self._h = h
