@@ -217,6 +217,8 @@ def main():
     ap.add_argument("--serve-sweep", default="",
                     help="comma-separated arrival rates: run the served sweep and print one JSON "
                          "line per rate instead of the benchmark")
+    ap.add_argument("--pairs", type=int, default=0,
+                    help="keep only the first N pairs of the workload (small profiler cases)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
@@ -245,6 +247,8 @@ def main():
         run_serve_sweep(args, local_rank)
         return
     items = workload(rank, args.workload)
+    if args.pairs:
+        items = items[:args.pairs]
     pairs = make_pairs(vx_sgm, items)
     cfgs = [sgm_config(vx_sgm, d) for (_, _, d, _) in items]
     total_pd = sum(w * h * d for (w, h, d, _) in items)

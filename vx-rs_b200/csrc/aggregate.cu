@@ -261,8 +261,7 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
 // One pixel of the 32 scanlines of a warp (all lanes execute it: the TMEM
 // accesses are warp-collective). tstate = this warp's TMEM address (lane field
 // = its first lane, column 0). getR(d) = right census at x-d; only called with
-// x-d >= 0 when CHECK. prefetch(d) hints census words into L1 (horizontal
-// paths). active: this lane's scanline covers the pixel; an idle lane keeps (or
+// x-d >= 0 when CHECK. active: this lane's scanline covers the pixel; an idle lane keeps (or
 // resets to) the zero state a scanline starts from. otile = this lane's row of
 // the warp's shared-memory output tile (one 16-byte word per group). Returns
 // whether the new vector escapes the byte slab. Software pipeline over groups
@@ -270,10 +269,10 @@ __device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_l
 // min/add chain, the census words and state of group g+1 are in flight, and
 // g+1's costs are formed right after g's chain, so neither load nor popcount
 // latency sits on the chain.
-template <bool CHECK, typename CT, typename GetR, typename Prefetch>
+template <bool CHECK, typename CT, typename GetR>
 __device__ __forceinline__ bool sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
-                                          const GetR& getR, const Prefetch& prefetch,
-                                          const int x, const bool active, const ScanConst& k,
+                                          const GetR& getR, const int x, const bool active,
+                                          const ScanConst& k,
                                           uint4* __restrict__ otile) {
     PixelState ps;
     const uint32_t o3 = (m + k.P2) & 0xFFFFu;
@@ -284,7 +283,6 @@ __device__ __forceinline__ bool sgm_pixel(const uint32_t tstate, uint32_t& m, co
     ps.mn = 0xFFFFFFFFu;
     ps.mx = 0u;
     auto load = [&](CT (&r)[8], int g) {
-        prefetch(8 * (g + 2));
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int d = 8 * g + i;
@@ -426,12 +424,11 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         __syncwarp();
         const CT* seg = stage + (t & 1) * seg_words + seg_offset(t) + lane + (Dp - 1);  // seg[-d] = R(x-d)
         auto getR = [seg](int d) { return seg[-d]; };
-        auto no_prefetch = [](int) {};
         const int xb = k0 + dx * t;             // smallest x of the warp
         uint4* otile = tile + lane * row_words;
         const bool esc = xb >= Dp - 1
-                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile)
-                             : sgm_pixel<true, CT>(tstate, m, lc, getR, no_prefetch, x, active, k, otile);
+                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, x, active, k, otile)
+                             : sgm_pixel<true, CT>(tstate, m, lc, getR, x, active, k, otile);
         // Active lanes are one run of consecutive pixels of row y.
         const unsigned act = __ballot_sync(kFull, active);
         const unsigned em = __ballot_sync(kFull, active && esc);
@@ -483,20 +480,10 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
         if (t + 1 < W) lc_next = CL[(size_t)(x + dx) * 32];
         const CT* col = CR + (size_t)x * 32;        // col[-32*d] = R(x-d, y)
         auto getR = [col](int d) { return col[-32 * d]; };
-        // Two groups further ahead: bring the 8 columns of that group into L1
-        // (one line per column of the band; columns left of x = 0 are skipped).
-        auto prefetch = [col, x, Dp](int d0) {
-            if (d0 < Dp) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (x - d0 - i >= 0)
-                        asm volatile("prefetch.global.L1 [%0];" ::"l"(col - 32 * (d0 + i)));
-            }
-        };
         uint4* otile = tile + lane * row_words;
         const bool esc = x >= Dp - 1
-                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile)
-                             : sgm_pixel<true, CT>(tstate, m, lc, getR, prefetch, x, active, k, otile);
+                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, x, active, k, otile)
+                             : sgm_pixel<true, CT>(tstate, m, lc, getR, x, active, k, otile);
         const unsigned em = __ballot_sync(kFull, active && esc);
         // Rows first..first+nrows-1, one vector per row at column x.
         const size_t pix0 = (size_t)first * W + x;
