@@ -25,7 +25,6 @@ same metric and workload, each step a bounded sample of the pairs.
 import argparse
 import json
 import os
-import subprocess
 import sys
 import time
 
@@ -74,56 +73,73 @@ def make_pairs(vx_sgm, items):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """SM clock, power and clock-event (throttle) reasons of the bench's GPU, read
+    through NVML every 10 ms on a background thread while the timed region runs
+    (plus one reading at its start and one at its end). Read-only."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.path = os.path.join("/tmp", f"vx_clocks_{os.getpid()}.csv")
+        self.rows = []
+        self.err = None
+        self.stop = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                          float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                          nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons)))
 
     def __enter__(self):
+        import threading
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-i", str(self.device), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv, self.h = nv, self._handle(nv)
+            self._sample()
+        except Exception as e:  # no NVML: report it instead of clocks
+            self.err = f"nvml unavailable: {type(e).__name__}"
+            return self
+        self.stop = threading.Event()
+
+        def loop():
+            while not self.stop.wait(0.01):
+                try:
+                    self._sample()
+                except Exception:
+                    pass
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        if self.stop is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
+                self._sample()
             except Exception:
-                self.proc.kill()
-            self.fh.close()
+                pass
 
     def summary(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
-            except ValueError:
-                continue
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v == "Active"})
-        return {"sm_mhz": float(np.median([r[0] for r in rows])),
-                "sm_max_mhz": max(r[1] for r in rows),
-                "power_w_max": max(r[2] for r in rows),
-                "samples": len(rows), "reasons": reasons}
+        if self.err or not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no samples"]}
+        reasons = sorted({name for r in self.rows for bit, name in self.REASONS.items() if r[3] & bit})
+        return {"sm_mhz": float(np.median([r[0] for r in self.rows])),
+                "sm_max_mhz": max(r[1] for r in self.rows),
+                "power_w_max": max(r[2] for r in self.rows),
+                "samples": len(self.rows), "source": "nvml", "reasons": reasons}
 
 
 def cpu_reference_rate(items, pairs, max_pd, threads):
@@ -144,6 +160,11 @@ def cpu_reference_rate(items, pairs, max_pd, threads):
             break
     return done_pd / secs / 1e9, n, done_pd, secs
 
+
+# DRAM bytes (read + write) one aggregation launch of the 64-pair workload moved
+# per path-pixel-disparity: 31.75 GB over 8 x 3.738 G path-pd (ncu capture,
+# dram__bytes_read.sum 1.80 GB + dram__bytes_write.sum 29.95 GB).
+AGG_DRAM_BYTES_PER_PATH_PD = 31.75e9 / (8 * 3737760000)
 
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
@@ -374,10 +395,18 @@ def main():
         peak_src = "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
+    # Algorithmic bytes (P2 = 120: byte path slabs, Dv = D rounded up to 16):
+    # aggregation writes one byte per path-pixel-disparity and reads the left
+    # and right census word of every pixel once per path; the pipeline adds the
+    # census pass (images in, row-major and banded planes out) and the WTA
+    # (slabs in, f32 + i16 disparities out).
     census_bytes = 4  # 5x5 census: one u32 word per pixel
-    agg_bytes = sum(8 * (w * h * d * 2 + 2 * w * h * census_bytes) for (w, h, d, _) in items)
+    dv = lambda d: (d + 15) // 16 * 16
+    agg_bytes = sum(8 * (w * h * dv(d) + 2 * w * h * census_bytes) for (w, h, d, _) in items)
     agg_gbs = agg_bytes / (agg_ms * 1e-3) / 1e9
-    pipeline_bytes = sum(4 * 8 * w * h * d + 6 * w * h for (w, h, d, _) in items)
+    pipeline_bytes = sum(2 * 8 * w * h * dv(d) + 2 * w * h + 4 * w * h * census_bytes + 6 * w * h
+                         for (w, h, d, _) in items)
+    slab_bytes = sum(8 * w * h * dv(d) for (w, h, d, _) in items)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -387,8 +416,8 @@ def main():
                                "8 paths, 5x5 census, P1=10 P2=120, subpixel, LR tol 1",
                    "pairs_per_rank": NUM_PAIRS, "pd_per_rank": total_pd, "pixels_per_rank": total_px,
                    "parallelism": f"replicas x{world}",
-                   "l2": "working set larger than L2 (path slabs %.1f GB per step)" % (
-                       sum(8 * w * h * d * 2 for (w, h, d, _) in items) / 1e9)},
+                   "l2": "working set larger than L2 (byte path slabs %.1f GB per step)" % (
+                       slab_bytes / 1e9)},
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_pass": plain_ms,
                   "latency_ms_p50": float(np.percentile(lat, 50)),
                   "latency_ms_p99": float(np.percentile(lat, 99)),
@@ -400,8 +429,13 @@ def main():
         "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
         "roofline": {"bound": "hbm", "kernel": "path aggregation (all pairs, all paths)",
                      "achieved": agg_gbs, "peak": peak, "unit": "GB/s", "frac": agg_gbs / peak,
-                     "peak_source": peak_src, "traffic": None,
-                     "algorithmic_bytes_per_launch": agg_bytes},
+                     "peak_source": peak_src,
+                     "traffic": AGG_DRAM_BYTES_PER_PATH_PD * 8 * total_pd,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "aggregation launch of this workload, per path-pixel-disparity",
+                     "algorithmic_bytes_per_launch": agg_bytes,
+                     "issue_bound": "the recurrence is integer-issue bound (about 19 instructions "
+                                    "per path-pixel-disparity); HBM is not its limit"},
         "pipeline_roofline": {"bytes_per_step": pipeline_bytes,
                               "achieved_gbs": pipeline_bytes / (ms * 1e-3) / 1e9,
                               "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / peak},

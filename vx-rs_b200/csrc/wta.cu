@@ -13,15 +13,16 @@
 //
 // Mapping: lanes span disparities (8 per lane: 8 bytes of a byte-slab vector,
 // or 16 bytes of a wide one) so slab reads are coalesced; a warp covers 32/seg
-// pixels at once. Sums are kept as u16 pairs (d, d+1) in 32-bit words and added
-// per half (wrapping modulo 2^16); a byte is widened into its half by a byte
-// permute. The loads of all paths of a pixel group are issued before any is
-// used (the path count is a template parameter). An escaped byte vector (0xFF
-// in byte 0, held by the pixel's first lane) is left out of the byte sum and
-// its exact u16 values are read from the shadow slab instead. The
-// argmin is a min over the key (S << 8 | d), which orders by cost then by d,
-// i.e. the first minimum. The right-view argmin of the row is accumulated in
-// shared memory with atomicMin on the same keys.
+// pixels at once. Sums are kept as u16 pairs in 32-bit words (wide slabs: added
+// per half, wrapping modulo 2^16; byte slabs: bytes widened by a mask or a byte
+// permute and summed as whole words, see sum_paths). The loads of all paths of
+// a pixel group are issued before any is used (the path count is a template
+// parameter). An escaped byte vector (0xFF in byte 0, held by the pixel's first
+// lane) is taken out of the byte sum and its exact u16 values are read from
+// the shadow slab instead. The argmin is a min over the key (S << 8 | d), which
+// orders by cost then by d, i.e. the first minimum; S(bd-1) and S(bd+1) for the
+// subpixel step come from the lanes that hold them. The right-view argmin of
+// the row is accumulated in shared memory with atomicMin on the same keys.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -42,69 +43,109 @@ __device__ __forceinline__ int find_pair_by_row(const PairDev* pairs, int n, int
     return lo;
 }
 
-// acc[k] += (d = 2k, d = 2k+1) of 8 byte values (v.x: d 0..3, v.y: d 4..7).
-__device__ __forceinline__ void add_bytes(uint32_t (&acc)[4], const uint2 v) {
-    acc[0] = __vadd2(acc[0], __byte_perm(v.x, 0u, 0x4140));
-    acc[1] = __vadd2(acc[1], __byte_perm(v.x, 0u, 0x4342));
-    acc[2] = __vadd2(acc[2], __byte_perm(v.y, 0u, 0x4140));
-    acc[3] = __vadd2(acc[3], __byte_perm(v.y, 0u, 0x4342));
-}
-// The same for 8 u16 values (already (d, d+1) pairs).
-__device__ __forceinline__ void add_u16(uint32_t (&acc)[4], const uint4 a) {
-    acc[0] = __vadd2(acc[0], a.x);
-    acc[1] = __vadd2(acc[1], a.y);
-    acc[2] = __vadd2(acc[2], a.z);
-    acc[3] = __vadd2(acc[3], a.w);
+// Per-lane view of one pair, held in registers for the row loop.
+struct RowView {
+    const uint8_t* slabs;
+    const uint16_t* shadow;
+    size_t slab_stride, shadow_stride;
+    int Dp, Dv;
+};
+
+// The same sums for 8 u16 values (natural (d, d+1) pairs) into lo/hi words
+// that hold (d, d+2) pairs: lo0 = (0, 2), hi0 = (1, 3), lo1 = (4, 6), hi1 = (5, 7).
+__device__ __forceinline__ void add_u16_split(uint32_t (&a)[4], const uint4 v) {
+    a[0] = __vadd2(a[0], __byte_perm(v.x, v.y, 0x5410));
+    a[1] = __vadd2(a[1], __byte_perm(v.x, v.y, 0x7632));
+    a[2] = __vadd2(a[2], __byte_perm(v.z, v.w, 0x5410));
+    a[3] = __vadd2(a[3], __byte_perm(v.z, v.w, 0x7632));
 }
 
-// Sum over the NP paths of the 8 disparities d = 8c..8c+7 of pixel pix (lanes
-// with act = false contribute nothing but take part in the warp shuffles).
+// Sum over the NP paths of the 8 disparities d = 8c..8c+7 of pixel pix, as
+// natural pairs acc[k] = S(8c+2k) | S(8c+2k+1) << 16 (lanes with act = false
+// contribute nothing but take part in the warp shuffles).
+//
+// Byte slabs: a non-escaped byte is at most 254, so 8 of them sum to less than
+// 2^11 and whole 32-bit words can be added: the byte pairs (0, 2) and (1, 3) of
+// a 4-byte word are widened by a mask and a byte permute and summed with plain
+// 3-input adds, no carry reaching the next half. Escaped vectors (marker in the
+// byte 0 of the pixel's lane c = 0) are taken out again and replaced by their
+// exact u16 values from the shadow slab with per-half wrapping adds (rare).
 template <int NP, bool WIDE>
-__device__ __forceinline__ void sum_paths(const PairDev& pr, size_t pix, int c, bool act, int lead,
+__device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, bool act, int lead,
                                           uint32_t (&acc)[4]) {
-    const int Dp = pr.nd_pad;
-    const bool in_dp = act && 8 * c < Dp;           // lanes past Dp (Dv = Dp + 8) read no shadow
+    const bool in_dp = act && 8 * c < rv.Dp;        // lanes past Dp (Dv = Dp + 8) read no shadow
     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
     if (WIDE) {
+        const uint16_t* base = rv.shadow + pix * rv.Dp + 8 * c;
         uint4 v[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p)
-            v[p] = in_dp ? __ldcs(reinterpret_cast<const uint4*>(pr.shadow + pr.shadow_stride * p +
-                                                                   pix * Dp + 8 * c))
-                         : z4;
+            v[p] = in_dp ? __ldcs(reinterpret_cast<const uint4*>(base + rv.shadow_stride * p)) : z4;
 #pragma unroll
-        for (int p = 0; p < NP; ++p) add_u16(acc, v[p]);
+        for (int p = 0; p < NP; ++p) {
+            acc[0] = __vadd2(acc[0], v[p].x);
+            acc[1] = __vadd2(acc[1], v[p].y);
+            acc[2] = __vadd2(acc[2], v[p].z);
+            acc[3] = __vadd2(acc[3], v[p].w);
+        }
         return;
     }
-    const int Dv = pr.nd_vec;
+    const uint8_t* base = rv.slabs + pix * rv.Dv + 8 * c;
     uint2 v[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p)
-        v[p] = act ? __ldcs(reinterpret_cast<const uint2*>(pr.slabs + pr.slab_stride * p + pix * Dv + 8 * c))
-                   : make_uint2(0u, 0u);
-    unsigned esc = 0u;
+        v[p] = act ? __ldcs(reinterpret_cast<const uint2*>(base + rv.slab_stride * p)) : make_uint2(0u, 0u);
+    constexpr uint32_t M = 0x00FF00FFu;
+    uint32_t a[4] = {0u, 0u, 0u, 0u};               // (0,2) (1,3) (4,6) (5,7)
+    unsigned em = 0u;
 #pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        if ((__shfl_sync(kFull, v[p].x, lead) & 0xFFu) == 0xFFu)
-            esc |= 1u << p;
-        else
-            add_bytes(acc, v[p]);
+    for (int p = 0; p < NP; p += 2) {
+        a[0] += (v[p].x & M) + (v[p + 1].x & M);
+        a[1] += __byte_perm(v[p].x, 0u, 0x4341) + __byte_perm(v[p + 1].x, 0u, 0x4341);
+        a[2] += (v[p].y & M) + (v[p + 1].y & M);
+        a[3] += __byte_perm(v[p].y, 0u, 0x4341) + __byte_perm(v[p + 1].y, 0u, 0x4341);
+        em |= ((v[p].x & 0xFFu) == 0xFFu ? 1u : 0u) << p;
+        em |= ((v[p + 1].x & 0xFFu) == 0xFFu ? 1u : 0u) << (p + 1);
     }
-    if (__any_sync(kFull, esc != 0u)) {             // rare: escaped vectors from the shadow
+    em = __shfl_sync(kFull, em, lead);              // the pixel's markers (its lane c = 0)
+    if (__any_sync(kFull, em != 0u)) {
+        // Every escaped byte vector out first (plain subtractions are exact only
+        // while no half has wrapped), then the shadow values in.
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            if (act && ((em >> p) & 1u)) {
+                a[0] -= v[p].x & M;
+                a[1] -= __byte_perm(v[p].x, 0u, 0x4341);
+                a[2] -= v[p].y & M;
+                a[3] -= __byte_perm(v[p].y, 0u, 0x4341);
+            }
+        }
 #pragma unroll
         for (int p = 0; p < NP; ++p)
-            if (in_dp && ((esc >> p) & 1u))
-                add_u16(acc, __ldcs(reinterpret_cast<const uint4*>(pr.shadow + pr.shadow_stride * p +
-                                                                     pix * Dp + 8 * c)));
+            if (in_dp && ((em >> p) & 1u))
+                add_u16_split(a, __ldcs(reinterpret_cast<const uint4*>(rv.shadow + rv.shadow_stride * p +
+                                                                       pix * rv.Dp + 8 * c)));
     }
+    acc[0] = __byte_perm(a[0], a[1], 0x5410);
+    acc[1] = __byte_perm(a[0], a[1], 0x7632);
+    acc[2] = __byte_perm(a[2], a[3], 0x5410);
+    acc[3] = __byte_perm(a[2], a[3], 0x7632);
 }
 
-// Five CTAs per SM (at most 51 registers a thread) keep enough slab loads in flight.
-__global__ void __launch_bounds__(kWtaThreads, 5)
+// s[i] for a lane-dependent i in 0..7 without local memory (select tree).
+__device__ __forceinline__ uint32_t pick8(const uint32_t (&s)[8], int i) {
+    const uint32_t a0 = (i & 1) ? s[1] : s[0], a1 = (i & 1) ? s[3] : s[2];
+    const uint32_t a2 = (i & 1) ? s[5] : s[4], a3 = (i & 1) ? s[7] : s[6];
+    const uint32_t b0 = (i & 2) ? a1 : a0, b1 = (i & 2) ? a3 : a2;
+    return (i & 4) ? b1 : b0;
+}
+
+// Four CTAs per SM (at most 64 registers a thread, no spills) keep enough slab loads in flight.
+__global__ void __launch_bounds__(kWtaThreads, 4)
 wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint32_t smem[];
     const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
-    const PairDev& pr = pairs[pi];
+    const PairDev pr = pairs[pi];                  // fields live in registers
     const int y = blockIdx.x - pr.row_begin;
     const int W = pr.width, D = pr.nd, P = pr.num_paths;
     const bool lr = pr.lr_check != 0;
@@ -125,6 +166,8 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const int sub = lane / seg, c = lane % seg;
     const int ppw = 32 / seg;
     const int kind = (P == 2 ? 0 : P == 4 ? 1 : 2) + (pr.wide_slabs ? 3 : 0);
+    const RowView rv{pr.slabs, pr.shadow, pr.slab_stride, pr.shadow_stride, pr.nd_pad, pr.nd_vec};
+    const bool subpixel = pr.subpixel != 0;
 
     for (int xb = warp * ppw; xb < W; xb += nwarps * ppw) {
         const int x = xb + sub;
@@ -132,12 +175,12 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         const size_t pix = (size_t)y * W + (act ? x : 0);
         uint32_t acc[4] = {0u, 0u, 0u, 0u};         // acc[k] = S(8c+2k) | S(8c+2k+1) << 16
         switch (kind) {                             // uniform over the CTA
-            case 0: sum_paths<2, false>(pr, pix, c, act, sub * seg, acc); break;
-            case 1: sum_paths<4, false>(pr, pix, c, act, sub * seg, acc); break;
-            case 2: sum_paths<8, false>(pr, pix, c, act, sub * seg, acc); break;
-            case 3: sum_paths<2, true>(pr, pix, c, act, sub * seg, acc); break;
-            case 4: sum_paths<4, true>(pr, pix, c, act, sub * seg, acc); break;
-            default: sum_paths<8, true>(pr, pix, c, act, sub * seg, acc); break;
+            case 0: sum_paths<2, false>(rv, pix, c, act, sub * seg, acc); break;
+            case 1: sum_paths<4, false>(rv, pix, c, act, sub * seg, acc); break;
+            case 2: sum_paths<8, false>(rv, pix, c, act, sub * seg, acc); break;
+            case 3: sum_paths<2, true>(rv, pix, c, act, sub * seg, acc); break;
+            case 4: sum_paths<4, true>(rv, pix, c, act, sub * seg, acc); break;
+            default: sum_paths<8, true>(rv, pix, c, act, sub * seg, acc); break;
         }
         uint32_t s[8];
 #pragma unroll
@@ -153,17 +196,11 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         }
         for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
         const int bd = (int)(best & 0xFFu);
-        uint32_t c0 = 0, c2 = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int d = 8 * c + j;
-            if (act && d == bd - 1) c0 = s[j];
-            if (act && d == bd + 1 && d < D) c2 = s[j];
-        }
-        for (int o = seg >> 1; o > 0; o >>= 1) {
-            c0 |= __shfl_xor_sync(kFull, c0, o);
-            c2 |= __shfl_xor_sync(kFull, c2, o);
-        }
+        // S(bd-1) and S(bd+1) from the lanes that hold them (only used when
+        // 0 < bd < D-1, so both exist).
+        const int dm = max(bd - 1, 0), dq = min(bd + 1, D - 1);
+        const uint32_t c0 = __shfl_sync(kFull, pick8(s, dm & 7), sub * seg + (dm >> 3));
+        const uint32_t c2 = __shfl_sync(kFull, pick8(s, dq & 7), sub * seg + (dq >> 3));
         if (lr && act) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -173,7 +210,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         }
         if (c == 0 && x < W) {
             float v = (float)bd;
-            if (pr.subpixel && bd > 0 && bd < D - 1) {
+            if (subpixel && bd > 0 && bd < D - 1) {
                 const float f0 = (float)c0, f1 = (float)(best >> 8), f2 = (float)c2;
                 const float denom = 2.0f * (f0 + f2 - 2.0f * f1);
                 if (fabsf(denom) > 1e-6f) v = __fadd_rn(v, __fdiv_rn(f0 - f2, denom));
