@@ -1,5 +1,5 @@
 // Path aggregation of semi-global matching: every path of every pair of a batch
-// in ONE persistent launch over a work queue of (pair, path, 32-scanline) units.
+// in ONE persistent launch over a work queue of (pair, path, 64-scanline) units.
 //
 // Semantics (vx-vision/shaders/SGMStereo.metal:72-173), per scanline, per pixel,
 // for d = 0..D-1 in increasing order with ONE array Lp[] updated in place:
@@ -16,36 +16,42 @@
 //
 // Evaluation. With A_d = min(o0, o2, o3) (independent of the current pixel) and
 // f_d = u16(Lp[d] + P1) = o1_{d+1}, one pixel is the chain
-//     t_d = min(A_d, f_{d-1});  f_d = u16(t_d + C_d + P1 - m);  Lp[d] = u16(t_d + C_d - m)
-// whose critical path is one min and one add per disparity. u16 values live in
-// the low half of 32-bit registers: min.u16x2 compares halves on their own and a
-// 32-bit add's low half is the u16 sum, so whatever accumulates in the high half
-// never reaches the low half and no masking is needed. A_d is formed two
-// disparities at a time on packed state words (min.u16x2, and a per-half
-// wrapping add for Lp[d+1] + P1).
+//     t_d = min(A_d, f_{d-1});  f_d = u16(t_d + C_d + P1 - m);  Lp[d] = u16(f_d - P1)
+// whose critical path is one min and one add per disparity.
 //
-// Mapping. One thread owns one scanline. Its D state values (packed u16 pairs)
-// live in tensor memory (TMEM): the thread's TMEM lane, one 32-bit column per
-// pair, read and written 4 columns (8 disparities) at a time by warp-collective
-// tcgen05.ld/st. The per-pixel loop runs over groups of 8 disparities with a
-// small loop body and a runtime D, so one kernel serves every D of a batch, and
-// shared memory is left almost entirely to L1 for the census windows. A warp takes 32 neighbouring scanlines of
-// one (pair, path):
-//  * vertical / diagonal paths: the 32 lanes sit on 32 consecutive pixels of one
-//    row at every step, so the right-census words they need form one segment of
-//    Dp+31 words of that row; it is staged in warp-private shared memory with
-//    16-byte cp.async copies one step ahead (double-buffered).
-//  * horizontal paths: the 32 lanes are 32 consecutive rows (one 32-row band)
-//    at the same x and read the banded census copy: each disparity is one
-//    coalesced 128-byte load at a constant offset, and the window of the last D
-//    columns stays in L1.
-// Census words of the next group are loaded while the current group is
-// processed. Pixels whose window may reach x-d < 0 take a second body with the
-// border test, picked by a warp-uniform branch. Results leave as 16-byte stores
-// into this path's slab, one byte per disparity: the values of a vector are
-// bounded by the census cost plus P2 unless the in-place o1 term pulls them
-// below m (then they wrap), so almost every vector fits bytes; one that does
-// not is marked with 0xFF in byte 0 and written exactly to a u16 shadow slab.
+// Scanline pairs. Every thread carries TWO scanlines, their u16 values side by
+// side in the halves of 32-bit words, and every step of the chain is one
+// per-half instruction for both: min.u16x2, the three-way DPX minimum for A_d,
+// and per-half wrapping adds (which are exactly the shader's ushort
+// arithmetic). The state word of disparity d holds (Lp_lo[d], Lp_hi[d]).
+// A scanline that starts at this pixel gets o3 = 0 and m = 0 for its half:
+// then min(o0,o1,o2,o3) = 0 and Lp[d] = C whatever its state held before, so
+// no state is ever cleared and idle halves need no masking.
+//
+// Mapping. The state of a thread (one 32-bit word per disparity) lives in
+// tensor memory (TMEM): the thread's TMEM lane, one column per disparity, read
+// and written 8 columns at a time by warp-collective tcgen05.ld/st. A warp
+// takes 64 neighbouring scanlines of one (pair, path): lane i carries
+// scanlines i (low half) and i + 32 (high half).
+//  * vertical / diagonal paths: the 64 scanlines sit on 64 consecutive pixels
+//    of one row at every step, so the right-census words they need form one
+//    segment of Dp+63 words of that row; it is staged in warp-private shared
+//    memory with 16-byte cp.async copies one step ahead (double-buffered).
+//  * horizontal paths: the 64 scanlines are 64 consecutive rows (two 32-row
+//    bands) at the same x and read the banded census copy: each disparity is
+//    one coalesced 128-byte load per band at a constant offset.
+// Census words of the next group of 8 disparities are loaded while the
+// current group is processed. Pixels whose window may reach x-d < 0 take a
+// second body with the border test, picked by a warp-uniform branch.
+//
+// Output. Each group's results go to a byte tile in shared memory (one row of
+// Dv bytes per scanline); after the pixel the warp writes the rows of its
+// active scanlines to the path's byte slab with coalesced 8-byte stores. The
+// values of a vector are bounded by the census cost plus P2 unless the
+// in-place o1 term pulls them below m (then they wrap), so almost every vector
+// fits bytes; one with a value of 255 or more gets 0xFF in byte 0 and its
+// exact u16 values, read back from TMEM (the state after the pixel is the
+// vector), go to the u16 shadow slab. Wide slabs get every vector that way.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -67,12 +73,6 @@ __device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
     return r;
 }
 
-__device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b) {
-    uint32_t r;
-    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-    return r;
-}
-
 __device__ __forceinline__ uint32_t popc_xor(uint32_t a, uint32_t b) { return __popc(a ^ b); }
 __device__ __forceinline__ uint32_t popc_xor(uint64_t a, uint64_t b) { return __popcll(a ^ b); }
 
@@ -87,304 +87,367 @@ __device__ __forceinline__ void cp_async_wait_1() {
 }
 
 // Tensor-memory (TMEM) access for the per-scanline state. Warp w of the CTA owns
-// TMEM lanes 32w..32w+31 (one lane per thread) and the CTA's allocated columns;
-// the 8 disparities of group g are columns 4g..4g+3 (one u16 pair per column).
-// tcgen05.ld is asynchronous: its registers are threaded through the wait so
-// that no use can be scheduled before the data has arrived.
-__device__ __forceinline__ uint4 tmem_ld4(uint32_t taddr) {
-    uint4 r;
-    __syncwarp();  // .sync.aligned: the whole warp, converged
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+// TMEM lanes 32(w%4)..32(w%4)+31 (one lane per thread) and the columns of its
+// warpgroup; disparity d is column d. tcgen05.ld is asynchronous: its registers
+// are threaded through the wait so that no use can be scheduled before the data
+// has arrived. The callers are warp-converged (uniform control flow).
+struct Words8 {
+    uint32_t w[8];
+};
+__device__ __forceinline__ Words8 tmem_ld8(uint32_t taddr) {
+    Words8 r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3]), "=r"(r.w[4]), "=r"(r.w[5]),
+                   "=r"(r.w[6]), "=r"(r.w[7])
                  : "r"(taddr));
     return r;
 }
-__device__ __forceinline__ void tmem_wait_ld(uint4& r) {
-    __syncwarp();
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r.x), "+r"(r.y), "+r"(r.z), "+r"(r.w)::"memory");
+__device__ __forceinline__ void tmem_wait_ld(Words8& r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r.w[0]), "+r"(r.w[1]), "+r"(r.w[2]), "+r"(r.w[3]), "+r"(r.w[4]), "+r"(r.w[5]),
+                   "+r"(r.w[6]), "+r"(r.w[7])::"memory");
 }
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint4 v) {
-    __syncwarp();
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
-                 "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const Words8& v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v.w[0]), "r"(v.w[1]), "r"(v.w[2]), "r"(v.w[3]), "r"(v.w[4]), "r"(v.w[5]), "r"(v.w[6]),
+                 "r"(v.w[7])
                  : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() {
-    __syncwarp();
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// Per-scanline constants of one unit.
+// Per-scanline constants of one unit (u16 values in both halves).
 struct ScanConst {
-    uint32_t p1x2;        // P1 in both halves
-    uint32_t P1, P2;
+    uint32_t p1x2;        // P1
+    uint32_t np1x2;       // -P1 (mod 2^16)
+    uint32_t p1p1x2;      // P1 + 1: P1 - m = (~m) + P1 + 1
+    uint32_t p2x2;        // P2
     int Dp, G;            // disparities padded to 8, groups of 8
     int last_j;           // position of d = D-1 inside the last group (0..7)
 };
 
-// Per-pixel values shared by the groups of one pixel.
+// Per-pixel values shared by the groups of one pixel (both scanlines).
 struct PixelState {
-    uint32_t o3x2;   // u16(m + P2) in both halves
-    uint32_t kc;     // f = t + C + (P1 - m)
-    uint32_t km;     // Lp = t + C - m
-    uint32_t f;      // o1 of the next disparity (low half)
-    uint32_t mn;     // running min of the new values (per half)
-    uint32_t mx;     // running max of the new values (per half, d < D)
+    uint32_t o3x2;   // u16(m + P2), 0 for a scanline that starts here
+    uint32_t kc2;    // u16(P1 - m)
+    uint32_t f;      // o1 of the next disparity
+    uint32_t mn;     // running min of the new values (d < D)
+    uint32_t mx;     // running max of the new values (d < D)
 };
 
-// Matching costs of one group from its 8 right-census words; x-d < 0 gives 64.
+// Matching costs of one group for both scanlines, packed c_lo | c_hi << 16;
+// x-d < 0 gives 64.
 template <bool CHECK, typename CT>
-__device__ __forceinline__ void group_costs(uint32_t (&c)[8], const CT lc, const CT (&r)[8],
-                                            const int x, const int g) {
+__device__ __forceinline__ void group_costs(uint32_t (&cw)[8], const CT lc_lo, const CT lc_hi,
+                                            const CT (&rl)[8], const CT (&rh)[8], const int x_lo,
+                                            const int x_hi, const int g) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        c[i] = popc_xor(lc, r[i]);
-        if (CHECK && x - (8 * g + i) < 0) c[i] = 64u;
-    }
-}
-
-// Writes the warp's output tile to a wide (u16) slab: lanes [la, lb] hold the
-// results of one pixel step; row p's vector goes to dst0 + p * stride (in u16),
-// and 16-byte word g of it to +8g. Words are distributed over the lanes in
-// address order, so consecutive lanes write consecutive 16 bytes of a vector.
-__device__ __forceinline__ void flush_tile_wide(const uint4* __restrict__ tile, int row_words, int G,
-                                                int la, int lb, uint16_t* __restrict__ dst0,
-                                                size_t stride, int lane) {
-    __syncwarp();
-    // Word c = (p - la) * G + g of the run, walked with a running (p, g) so
-    // that no division is needed per word: lane starts at c = lane, steps 32.
-    const int n = (lb - la + 1) * G;
-    const int q = 32 / G, r = 32 % G;
-    int p = la + lane / G, g = lane % G;
-    for (int c = lane; c < n; c += 32) {
-        __stcs(reinterpret_cast<uint4*>(dst0 + (size_t)p * stride + 8 * g), tile[p * row_words + g]);
-        g += r;
-        p += q;
-        if (g >= G) {
-            g -= G;
-            ++p;
+        uint32_t cl = popc_xor(lc_lo, rl[i]), ch = popc_xor(lc_hi, rh[i]);
+        if (CHECK) {
+            if (x_lo - (8 * g + i) < 0) cl = 64u;
+            if (x_hi - (8 * g + i) < 0) ch = 64u;
         }
+        cw[i] = cl | (ch << 16);
     }
-    __syncwarp();
 }
 
-// Writes the warp's output tile to the byte slab: lanes [la, lb] hold the
-// results of one pixel step; row p's vector goes to dst0 + p * stride bytes,
-// its 16-byte chunk h holding d = 16h..16h+15 (tile words 2h and 2h+1, the low
-// byte of every u16). A row whose bit is set in em (escaped) gets 0xFF in
-// byte 0 and its exact u16 words at sh0 + p * sstride (in u16) of the shadow.
-// Chunks are distributed over the lanes in address order, so that consecutive
-// lanes write consecutive 16 bytes of a vector (streaming stores: slabs are
-// read once by the WTA kernel and must not push the census planes, which every
-// path re-reads, out of L2).
-__device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int row_words, int G,
-                                           int la, int lb, unsigned em, uint8_t* __restrict__ dst0,
-                                           size_t stride, uint16_t* __restrict__ sh0,
-                                           size_t sstride, int lane) {
-    __syncwarp();
-    // Chunk c = (p - la) * V + h of the run, walked with a running (p, h) so
-    // that no division is needed per chunk: lane starts at c = lane, steps 32.
-    const int V = (G + 1) >> 1;
-    const int n = (lb - la + 1) * V;
-    const int q = 32 / V, r = 32 % V;
-    int p = la + lane / V, h = lane % V;
-    for (int c = lane; c < n; c += 32) {
-        const uint4* row = tile + p * row_words;
-        const uint4 a = row[2 * h];
-        const uint4 b = 2 * h + 1 < G ? row[2 * h + 1] : make_uint4(0u, 0u, 0u, 0u);
-        uint4 o;
-        o.x = __byte_perm(a.x, a.y, 0x6420);
-        o.y = __byte_perm(a.z, a.w, 0x6420);
-        o.z = __byte_perm(b.x, b.y, 0x6420);
-        o.w = __byte_perm(b.z, b.w, 0x6420);
-        if (h == 0 && ((em >> p) & 1u)) o.x |= 0xFFu;
-        __stcs(reinterpret_cast<uint4*>(dst0 + (size_t)p * stride + 16 * h), o);
-        h += r;
-        p += q;
-        if (h >= V) {
-            h -= V;
-            ++p;
-        }
-    }
-    // Escaped vectors (rare): the warp writes their u16 words, one row at a time.
-    while (em) {
-        const int pe = __ffs(em) - 1;              // bit p of em = row p (la <= p <= lb)
-        em &= em - 1;
-        for (int g = lane; g < G; g += 32)
-            __stcs(reinterpret_cast<uint4*>(sh0 + (size_t)pe * sstride + 8 * g), tile[pe * row_words + g]);
-    }
-    __syncwarp();
-}
-
-// One group of 8 disparities d = 8g..8g+7 of one pixel. cur = old state words of
-// the group, nxt_lo = old Lp[8g+8] in the low half (unused for the last group),
-// c = the group's matching costs. LAST: the group holding d = D-1, whose o2 is
-// forced to 0xFFFF and whose pads (d >= D) are kept out of the minimum.
+// One group of 8 disparities d = 8g..8g+7 of one pixel of both scanlines, in
+// two parts so that the state of the next group (whose first word only the last
+// disparity needs) can still be in flight during the first: head = d 8g..8g+6,
+// tail = d 8g+7 and the group's minimum and maximum. S = old state words of the
+// group, nxt = old state word of d = 8g+8 (unused for the last group), cw = the
+// group's packed costs; out = the new words. LAST: the group holding d = D-1,
+// whose o2 is forced to 0xFFFF and whose pads (d >= D) are kept out of the
+// minimum and maximum.
+// A_d = min(o0, o2, o3) and w_d = C_d + P1 - m of disparity j of the group:
+// neither depends on the chain, so a whole group of them is formed first and
+// the chain itself is two dependent instructions per disparity.
 template <bool LAST>
-__device__ __forceinline__ uint4 sgm_group(const uint4 cur, const uint32_t nxt_lo,
-                                           const uint32_t (&c)[8], const ScanConst& k,
-                                           PixelState& ps) {
-    const uint32_t w[5] = {cur.x, cur.y, cur.z, cur.w, nxt_lo};
-    uint32_t out[4];
+__device__ __forceinline__ void group_pre(const uint32_t s, const uint32_t sn, const uint32_t c, const int j,
+                                          const ScanConst& k, const PixelState& ps, uint32_t& A, uint32_t& w) {
+    uint32_t o2 = __vadd2(sn, k.p1x2);
+    if (LAST && j == k.last_j) o2 = 0xFFFFFFFFu;
+    A = __vimin3_u16x2(s, o2, ps.o3x2);
+    w = __vadd2(c, ps.kc2);
+}
+// The chain: t = min(A_d, f_{d-1}), f_d = t + w_d, Lp[d] = f_d - P1.
+__device__ __forceinline__ void chain_step(const uint32_t A, const uint32_t w, const ScanConst& k,
+                                           PixelState& ps, uint32_t& o) {
+    ps.f = __vadd2(vmin2(A, ps.f), w);
+    o = __vadd2(ps.f, k.np1x2);
+}
+template <bool LAST>
+__device__ __forceinline__ void sgm_group_head(const Words8& S, const uint32_t (&cw)[8], const ScanConst& k,
+                                               PixelState& ps, Words8& out, uint32_t& w7) {
+    uint32_t A[7], w[7];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        uint32_t o2 = __vadd2(__byte_perm(w[j], w[j + 1], 0x5432), k.p1x2);
-        if (LAST) {
-            if (k.last_j == 2 * j) o2 |= 0x0000FFFFu;
-            if (k.last_j == 2 * j + 1) o2 |= 0xFFFF0000u;
-        }
-        const uint32_t A = vmin2(vmin2(w[j], o2), ps.o3x2);
-        const uint32_t t0 = vmin2(A, ps.f);
-        ps.f = t0 + c[2 * j] + ps.kc;
-        const uint32_t e0 = t0 + c[2 * j] + ps.km;
-        const uint32_t t1 = vmin2(A >> 16, ps.f);
-        ps.f = t1 + c[2 * j + 1] + ps.kc;
-        const uint32_t e1 = t1 + c[2 * j + 1] + ps.km;
-        out[j] = __byte_perm(e0, e1, 0x5410);
-    }
+    for (int j = 0; j < 7; ++j) group_pre<LAST>(S.w[j], S.w[j + 1], cw[j], j, k, ps, A[j], w[j]);
+    w7 = __vadd2(cw[7], ps.kc2);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) chain_step(A[j], w[j], k, ps, out.w[j]);
+}
+template <bool LAST>
+__device__ __forceinline__ void sgm_group_tail(const Words8& S, const uint32_t nxt, const uint32_t w7,
+                                               const ScanConst& k, PixelState& ps, Words8& out) {
+    uint32_t o2 = __vadd2(nxt, k.p1x2);
+    if (LAST && k.last_j == 7) o2 = 0xFFFFFFFFu;
+    chain_step(__vimin3_u16x2(S.w[7], o2, ps.o3x2), w7, k, ps, out.w[7]);
     if (!LAST) {
-        ps.mn = vmin2(ps.mn, vmin2(vmin2(out[0], out[1]), vmin2(out[2], out[3])));
-        ps.mx = vmax2(ps.mx, vmax2(vmax2(out[0], out[1]), vmax2(out[2], out[3])));
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+            ps.mn = __vimin3_u16x2(ps.mn, out.w[j], out.w[j + 1]);
+            ps.mx = __vimax3_u16x2(ps.mx, out.w[j], out.w[j + 1]);
+        }
     } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            uint32_t pm = out[j], po = out[j];
-            if (2 * j > k.last_j) { pm |= 0x0000FFFFu; po &= 0xFFFF0000u; }   // pads never count
-            if (2 * j + 1 > k.last_j) { pm |= 0xFFFF0000u; po &= 0x0000FFFFu; }
-            ps.mn = vmin2(ps.mn, pm);
-            ps.mx = vmax2(ps.mx, po);
+        for (int j = 0; j < 8; ++j) {
+            if (j <= k.last_j) {                   // pads never count
+                ps.mn = vmin2(ps.mn, out.w[j]);
+                ps.mx = __vmaxu2(ps.mx, out.w[j]);
+            }
         }
     }
-    return make_uint4(out[0], out[1], out[2], out[3]);
 }
 
-// One pixel of the 32 scanlines of a warp (all lanes execute it: the TMEM
+// Byte rows of one group: the low bytes of the 8 words' low halves (scanline
+// lo) and of their high halves (scanline hi), d-ascending.
+__device__ __forceinline__ void group_bytes(const Words8& o, uint2& lo, uint2& hi) {
+    const uint32_t t01 = __byte_perm(o.w[0], o.w[1], 0x6420);   // lo0 hi0 lo1 hi1
+    const uint32_t t23 = __byte_perm(o.w[2], o.w[3], 0x6420);
+    const uint32_t t45 = __byte_perm(o.w[4], o.w[5], 0x6420);
+    const uint32_t t67 = __byte_perm(o.w[6], o.w[7], 0x6420);
+    lo.x = __byte_perm(t01, t23, 0x6420);
+    hi.x = __byte_perm(t01, t23, 0x7531);
+    lo.y = __byte_perm(t45, t67, 0x6420);
+    hi.y = __byte_perm(t45, t67, 0x7531);
+}
+
+// One pixel of the 64 scanlines of a warp (all lanes execute it: the TMEM
 // accesses are warp-collective). tstate = this warp's TMEM address (lane field
-// = its first lane, column 0). getR(d) = right census at x-d; only called with
-// x-d >= 0 when CHECK. active: this lane's scanline covers the pixel; an idle lane keeps (or
-// resets to) the zero state a scanline starts from. otile = this lane's row of
-// the warp's shared-memory output tile (one 16-byte word per group). Returns
-// whether the new vector escapes the byte slab. Software pipeline over groups
-// (loop unrolled by two, register sets in ping-pong): while group g runs its
-// min/add chain, the census words and state of group g+1 are in flight, and
-// g+1's costs are formed right after g's chain, so neither load nor popcount
-// latency sits on the chain.
+// = its first lane, column 0). getR(d, lo, hi) = right census words at x-d of
+// the two scanlines; only called with x_hi-d >= 0 when CHECK. m = the previous
+// pixel's minimum per half; start = 0xFFFF in each half whose scanline starts at
+// this pixel. row_lo / row_hi = the two scanlines' rows of the warp's byte tile.
+// Returns the per-half maximum of the new vector (d < D). Software pipeline over
+// groups (loop unrolled by two, register sets in ping-pong): while group g runs
+// its chain, the census words and state of group g+1 are in flight (the state
+// is waited for only before g's last disparity), and g+1's costs are formed
+// right after g's chain.
 template <bool CHECK, typename CT, typename GetR>
-__device__ __forceinline__ bool sgm_pixel(const uint32_t tstate, uint32_t& m, const CT lc,
-                                          const GetR& getR, const int x, const bool active,
-                                          const ScanConst& k,
-                                          uint4* __restrict__ otile) {
+__device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
+                                              const CT lc_lo, const CT lc_hi, const GetR& getR,
+                                              const int x_lo, const int x_hi, const ScanConst& k,
+                                              unsigned char* __restrict__ row_lo,
+                                              unsigned char* __restrict__ row_hi) {
     PixelState ps;
-    const uint32_t o3 = (m + k.P2) & 0xFFFFu;
-    ps.o3x2 = o3 | (o3 << 16);
-    ps.kc = k.P1 - m;
-    ps.km = 0u - m;
-    ps.f = 0xFFFFu;            // o1 at d = 0
+    const uint32_t m0 = m & ~start;
+    ps.o3x2 = __vadd2(m0, k.p2x2) & ~start;
+    ps.kc2 = __vadd2(~m0, k.p1p1x2);
+    ps.f = 0xFFFFFFFFu;            // o1 at d = 0
     ps.mn = 0xFFFFFFFFu;
     ps.mx = 0u;
-    auto load = [&](CT (&r)[8], int g) {
+    auto load = [&](CT (&rl)[8], CT (&rh)[8], int g) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int d = 8 * g + i;
-            r[i] = (!CHECK || x - d >= 0) ? getR(d) : CT(0);
+            if (!CHECK || x_hi - d >= 0) {
+                getR(d, rl[i], rh[i]);
+            } else {
+                rl[i] = CT(0);
+                rh[i] = CT(0);
+            }
         }
     };
-    // Results go to this lane's row of the warp's output tile (written to the
-    // slab, coalesced, by flush_tile); idle lanes keep a zero state.
-    auto store = [&](uint4 o, int g) {
-        otile[g] = o;
-        if (!active) o = make_uint4(0u, 0u, 0u, 0u);
-        tmem_st4(tstate + 4 * g, o);
+    auto store = [&](const Words8& o, int g) {
+        uint2 lo, hi;
+        group_bytes(o, lo, hi);
+        *reinterpret_cast<uint2*>(row_lo + 8 * g) = lo;
+        *reinterpret_cast<uint2*>(row_hi + 8 * g) = hi;
+        tmem_st8(tstate + 8 * g, o);
     };
-    CT ra[8], rb[8];
+    CT ra_l[8], ra_h[8], rb_l[8], rb_h[8];
     uint32_t ca[8], cb[8];
-    load(ra, 0);
-    uint4 sa = tmem_ld4(tstate), sb;
-    group_costs<CHECK>(ca, lc, ra, x, 0);
+    Words8 oa, ob;
+    uint32_t w7;
+    load(ra_l, ra_h, 0);
+    Words8 sa = tmem_ld8(tstate), sb;
+    group_costs<CHECK>(ca, lc_lo, lc_hi, ra_l, ra_h, x_lo, x_hi, 0);
     tmem_wait_ld(sa);
     int g = 0;
 #pragma unroll 1
     for (; g + 2 < k.G; g += 2) {
-        sb = tmem_ld4(tstate + 4 * (g + 1));
-        load(rb, g + 1);
+        sb = tmem_ld8(tstate + 8 * (g + 1));
+        load(rb_l, rb_h, g + 1);
+        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
         tmem_wait_ld(sb);
-        store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
-        group_costs<CHECK>(cb, lc, rb, x, g + 1);
-        sa = tmem_ld4(tstate + 4 * (g + 2));
-        load(ra, g + 2);
+        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
+        store(oa, g);
+        group_costs<CHECK>(cb, lc_lo, lc_hi, rb_l, rb_h, x_lo, x_hi, g + 1);
+        sa = tmem_ld8(tstate + 8 * (g + 2));
+        load(ra_l, ra_h, g + 2);
+        sgm_group_head<false>(sb, cb, k, ps, ob, w7);
         tmem_wait_ld(sa);
-        store(sgm_group<false>(sb, sa.x, cb, k, ps), g + 1);
-        group_costs<CHECK>(ca, lc, ra, x, g + 2);
+        sgm_group_tail<false>(sb, sa.w[0], w7, k, ps, ob);
+        store(ob, g + 1);
+        group_costs<CHECK>(ca, lc_lo, lc_hi, ra_l, ra_h, x_lo, x_hi, g + 2);
     }
     if (g + 1 < k.G) {
-        sb = tmem_ld4(tstate + 4 * (g + 1));
-        load(rb, g + 1);
+        sb = tmem_ld8(tstate + 8 * (g + 1));
+        load(rb_l, rb_h, g + 1);
+        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
         tmem_wait_ld(sb);
-        store(sgm_group<false>(sa, sb.x, ca, k, ps), g);
-        group_costs<CHECK>(cb, lc, rb, x, g + 1);
-        store(sgm_group<true>(sb, 0u, cb, k, ps), g + 1);
+        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
+        store(oa, g);
+        group_costs<CHECK>(cb, lc_lo, lc_hi, rb_l, rb_h, x_lo, x_hi, g + 1);
+        sgm_group_head<true>(sb, cb, k, ps, ob, w7);
+        sgm_group_tail<true>(sb, 0u, w7, k, ps, ob);
+        store(ob, g + 1);
     } else {
-        store(sgm_group<true>(sa, 0u, ca, k, ps), g);
+        sgm_group_head<true>(sa, ca, k, ps, oa, w7);
+        sgm_group_tail<true>(sa, 0u, w7, k, ps, oa);
+        store(oa, g);
     }
     tmem_wait_st();            // the next pixel reads this state back
-    m = active ? min(ps.mn & 0xFFFFu, ps.mn >> 16) : 0u;
-    // The vector escapes the byte slab when a value is 255 or more, so that a
-    // stored byte vector never holds the marker 0xFF.
-    return max(ps.mx & 0xFFFFu, ps.mx >> 16) >= 0xFFu;
+    m = ps.mn;
+    return ps.mx;
 }
 
 __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
     ScanConst k;
-    k.P1 = (uint32_t)pr.p1;
-    k.P2 = (uint32_t)pr.p2;
-    k.p1x2 = k.P1 | (k.P1 << 16);
+    const uint32_t P1 = (uint32_t)pr.p1, P2 = (uint32_t)pr.p2;
+    k.p1x2 = P1 | (P1 << 16);
+    const uint32_t np1 = (0x10000u - P1) & 0xFFFFu;
+    k.np1x2 = np1 | (np1 << 16);
+    const uint32_t p1p1 = (P1 + 1u) & 0xFFFFu;
+    k.p1p1x2 = p1p1 | (p1p1 << 16);
+    k.p2x2 = P2 | (P2 << 16);
     k.Dp = pr.nd_pad;
     k.G = pr.nd_pad / 8;
     k.last_j = (pr.nd - 1) - 8 * (k.G - 1);
     return k;
 }
 
-__device__ __forceinline__ void clear_state(uint32_t tstate, int G) {
-    for (int g = 0; g < G; ++g) tmem_st4(tstate + 4 * g, make_uint4(0u, 0u, 0u, 0u));
-    tmem_wait_st();
+// Writes the rows la..lb (a run of active scanlines, 0..63) of the warp's byte
+// tile to the slab: row r's vector (Dv bytes) goes to dst0 + r * stride. The
+// rows' 8-byte chunks are distributed over the lanes in address order (chunk
+// c = (r - la) * V + h, walked with a running (r, h): no division per chunk),
+// so consecutive lanes write consecutive 8 bytes of a vector. Streaming stores:
+// the slabs are read once by the WTA kernel and must not push the census
+// planes, which every path re-reads, out of L2.
+__device__ __forceinline__ void flush_tile(const unsigned char* __restrict__ tile, int row_bytes, int Dv,
+                                           int la, int lb, unsigned char* __restrict__ dst0, size_t stride,
+                                           int lane) {
+    const int V = Dv / 8;
+    const int n = (lb - la + 1) * V;
+    const int q = 32 / V, rr = 32 % V;
+    int r = la + lane / V, h = lane % V;
+    for (int c = lane; c < n; c += 32) {
+        __stcs(reinterpret_cast<uint2*>(dst0 + (size_t)r * stride + 8 * h),
+               *reinterpret_cast<const uint2*>(tile + r * row_bytes + 8 * h));
+        h += rr;
+        r += q;
+        if (h >= V) {
+            h -= V;
+            ++r;
+        }
+    }
 }
 
-// Unit = 32 scanlines of a vertical or diagonal path.
+// The lanes whose w_lo / w_hi is set write their scanlines' exact u16 vectors,
+// read back from TMEM (the state after the pixel), to sh_lo / sh_hi (in the
+// shadow or wide slab). All lanes take part in the TMEM loads.
+__device__ __forceinline__ void write_u16_vectors(uint32_t tstate, int G, bool w_lo, bool w_hi,
+                                                  uint16_t* __restrict__ sh_lo, uint16_t* __restrict__ sh_hi) {
+    for (int g = 0; g < G; ++g) {
+        Words8 s = tmem_ld8(tstate + 8 * g);
+        tmem_wait_ld(s);
+        if (w_lo) {
+            const uint4 v = make_uint4(__byte_perm(s.w[0], s.w[1], 0x5410), __byte_perm(s.w[2], s.w[3], 0x5410),
+                                       __byte_perm(s.w[4], s.w[5], 0x5410), __byte_perm(s.w[6], s.w[7], 0x5410));
+            __stcs(reinterpret_cast<uint4*>(sh_lo + 8 * g), v);
+        }
+        if (w_hi) {
+            const uint4 v = make_uint4(__byte_perm(s.w[0], s.w[1], 0x7632), __byte_perm(s.w[2], s.w[3], 0x7632),
+                                       __byte_perm(s.w[4], s.w[5], 0x7632), __byte_perm(s.w[6], s.w[7], 0x7632));
+            __stcs(reinterpret_cast<uint4*>(sh_hi + 8 * g), v);
+        }
+    }
+}
+
+// After one pixel step: the escape flags of the two scanlines' vectors (a
+// value of 255 or more), the marker in their byte rows, the byte rows of the
+// active run to the slab, and the u16 vectors that need one (escaped vectors,
+// or every vector of a wide slab). pix_lo / pix_hi = the two scanlines' pixel
+// indices (used only for an active scanline); dst0 / stride = byte slab
+// address of tile row 0 and the row stride.
+__device__ __forceinline__ void finish_pixel(const PairDev& pr, int path, bool wide, int Dv, uint32_t tstate,
+                                             int G, uint32_t mx, bool act_lo, bool act_hi,
+                                             const unsigned char* tile, int row_bytes, unsigned char* row_lo,
+                                             unsigned char* row_hi, unsigned char* dst0, size_t stride,
+                                             size_t pix_lo, size_t pix_hi, int lane) {
+    const bool esc_lo = act_lo && (wide || (mx & 0xFFFFu) >= 0xFFu);
+    const bool esc_hi = act_hi && (wide || (mx >> 16) >= 0xFFu);
+    if (!wide) {
+        if (esc_lo) row_lo[0] = 0xFFu;
+        if (esc_hi) row_hi[0] = 0xFFu;
+    }
+    const unsigned al = __ballot_sync(kFull, act_lo), ah = __ballot_sync(kFull, act_hi);
+    const unsigned e = __ballot_sync(kFull, esc_lo || esc_hi);
+    __syncwarp();
+    if (!wide && (al | ah)) {
+        // The active scanlines are one run of rows: the low and high runs join.
+        const unsigned long long act = (unsigned long long)al | ((unsigned long long)ah << 32);
+        const int la = __ffsll((long long)act) - 1, lb = 63 - __clzll((long long)act);
+        flush_tile(tile, row_bytes, Dv, la, lb, dst0, stride, lane);
+    }
+    if (e) {
+        uint16_t* base = pr.shadow + pr.shadow_stride * (size_t)path;
+        write_u16_vectors(tstate, G, esc_lo, esc_hi, base + pix_lo * pr.nd_pad, base + pix_hi * pr.nd_pad);
+    }
+    __syncwarp();
+}
+
+// Unit = 64 scanlines of a vertical or diagonal path.
 template <typename CT>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
                                                   uint32_t tstate, CT* __restrict__ stage,
-                                                  int seg_words, uint4* __restrict__ tile,
-                                                  int row_words) {
+                                                  int seg_words, unsigned char* __restrict__ tile,
+                                                  int row_bytes) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
-    const int Dp = k.Dp;
+    const int Dp = k.Dp, Dv = pr.nd_vec;
+    const bool wide = pr.wide_slabs != 0;
     const int dx = job.dx, dy = job.dy;
 
-    const int i = first + lane;
-    const int k0 = job.k_min + first;         // scanline index of lane 0
-    const int kk = k0 + lane;
-    // Lane pixel at step t: x = kk + dx*t, y = y0 + dy*t (vertical: dx = 0).
+    const int k0 = job.k_min + first;         // scanline index of tile row 0
+    // This lane's two scanlines (tile rows lane and lane + 32): a scanline's
+    // pixel at step t is x = kk + dx*t, y = y0 + dy*t (vertical: dx = 0).
     const int y0 = dy > 0 ? 0 : H - 1;
-    int tb, te;
-    if (dx == 0) { tb = 0; te = H; }
-    else if (dx > 0) { tb = max(0, -kk); te = min(H, W - kk); }
-    else { tb = max(0, kk - W + 1); te = min(H, kk + 1); }
-    if (i >= job.num_scanlines) { tb = 0x7fffffff; te = -1; }
-    const int t_lo = __reduce_min_sync(kFull, tb);
-    const int t_hi = __reduce_max_sync(kFull, te);
+    auto range = [&](int i, int& tb, int& te) {
+        const int kk = k0 + i;
+        if (first + i >= job.num_scanlines) { tb = 0x7fffffff; te = -1; return; }
+        if (dx == 0) { tb = 0; te = H; }
+        else if (dx > 0) { tb = max(0, -kk); te = min(H, W - kk); }
+        else { tb = max(0, kk - W + 1); te = min(H, kk + 1); }
+    };
+    int tb_lo, te_lo, tb_hi, te_hi;
+    range(lane, tb_lo, te_lo);
+    range(lane + 32, tb_hi, te_hi);
+    const int t_lo = __reduce_min_sync(kFull, min(tb_lo, tb_hi));
+    const int t_hi = __reduce_max_sync(kFull, max(te_lo, te_hi));
     if (t_lo >= t_hi) return;
 
     const CT* __restrict__ CL = static_cast<const CT*>(pr.census_l);
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
-    uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
-    uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
-    const int Dv = pr.nd_vec;
+    unsigned char* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
 
-    // Stage the right-census segment [xb-(Dp-1), xb+31] of the step's row in
+    // Stage the right-census segment [xb-(Dp-1), xb+63] of the step's row in
     // 16-byte chunks from the aligned word at or below its start. The planes are
     // surrounded by guard words (kCensusGuardWords), so the chunks may run past
-    // the row ends: words outside the image are never used for a cost (lanes
+    // the row ends: words outside the image are never used for a cost (halves
     // with x >= W are idle and x-d < 0 takes the border body).
     // The alignment is taken on the plane's linear word index (row starts y*W
     // are not 16-byte aligned in general); the plane base is.
@@ -397,7 +460,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         const ptrdiff_t la = ls & ~(ptrdiff_t)(kPerChunk - 1);
         const CT* src = CR + la;
         CT* dstb = stage + buf * seg_words;
-        const int chunks = (Dp + 31 + (int)(ls - la) + kPerChunk - 1) / kPerChunk;
+        const int chunks = (Dp + 63 + (int)(ls - la) + kPerChunk - 1) / kPerChunk;
         for (int j = lane; j < chunks; j += 32) cp_async16(dstb + j * kPerChunk, src + j * kPerChunk);
         cp_async_commit();
     };
@@ -405,102 +468,102 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         const ptrdiff_t ls = seg_start(t);
         return (int)(ls - (ls & ~(ptrdiff_t)(kPerChunk - 1)));
     };
+    auto left = [&](int t, int i, int tb, int te) -> CT {
+        return (t >= tb && t < te) ? CL[(size_t)(y0 + dy * t) * W + (k0 + i) + dx * t] : CT(0);
+    };
 
-    clear_state(tstate, k.G);
+    unsigned char* row_lo = tile + lane * row_bytes;
+    unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
     stage_step(t_lo, t_lo & 1);
-    CT lc_next = CT(0);
-    if (t_lo >= tb && t_lo < te) lc_next = CL[(size_t)(y0 + dy * t_lo) * W + kk + dx * t_lo];
+    CT lcn_lo = left(t_lo, lane, tb_lo, te_lo), lcn_hi = left(t_lo, lane + 32, tb_hi, te_hi);
     for (int t = t_lo; t < t_hi; ++t) {
         if (t + 1 < t_hi) stage_step(t + 1, (t + 1) & 1);
         else cp_async_commit();                 // keep one group per step
-        const CT lc = lc_next;
-        const bool active = t >= tb && t < te;
-        const int x = kk + dx * t;
+        const CT lc_lo = lcn_lo, lc_hi = lcn_hi;
+        const bool act_lo = t >= tb_lo && t < te_lo, act_hi = t >= tb_hi && t < te_hi;
+        const uint32_t start = (t == tb_lo ? 0x0000FFFFu : 0u) | (t == tb_hi ? 0xFFFF0000u : 0u);
+        const int xb = k0 + dx * t;             // x of tile row 0
         const int y = y0 + dy * t;
-        if (t + 1 < t_hi && t + 1 >= tb && t + 1 < te)
-            lc_next = CL[(size_t)(y + dy) * W + (x + dx)];
+        if (t + 1 < t_hi) {
+            lcn_lo = left(t + 1, lane, tb_lo, te_lo);
+            lcn_hi = left(t + 1, lane + 32, tb_hi, te_hi);
+        }
         cp_async_wait_1();
         __syncwarp();
-        const CT* seg = stage + (t & 1) * seg_words + seg_offset(t) + lane + (Dp - 1);  // seg[-d] = R(x-d)
-        auto getR = [seg](int d) { return seg[-d]; };
-        const int xb = k0 + dx * t;             // smallest x of the warp
-        uint4* otile = tile + lane * row_words;
-        const bool esc = xb >= Dp - 1
-                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, x, active, k, otile)
-                             : sgm_pixel<true, CT>(tstate, m, lc, getR, x, active, k, otile);
-        // Active lanes are one run of consecutive pixels of row y.
-        const unsigned act = __ballot_sync(kFull, active);
-        const unsigned em = __ballot_sync(kFull, active && esc);
-        if (act) {
-            const int la = __ffs(act) - 1, lb = 31 - __clz(act);
-            const size_t pix0 = (size_t)y * W + xb;
-            if (pr.wide_slabs)
-                flush_tile_wide(tile, row_words, k.G, la, lb, shd + pix0 * Dp, (size_t)Dp, lane);
-            else
-                flush_tile(tile, row_words, k.G, la, lb, em, out + pix0 * Dv, (size_t)Dv,
-                           shd + pix0 * Dp, (size_t)Dp, lane);
-        }
-        __syncwarp();
+        const CT* seg = stage + (t & 1) * seg_words + seg_offset(t) + lane + (Dp - 1);  // seg[-d] = R(x_lo-d)
+        auto getR = [seg](int d, CT& lo, CT& hi) {
+            lo = seg[-d];
+            hi = seg[32 - d];
+        };
+        const int x_lo = xb + lane, x_hi = xb + lane + 32;
+        const uint32_t mx = xb >= Dp - 1
+            ? sgm_pixel<false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
+            : sgm_pixel<true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
+        const size_t pix0 = (size_t)y * W + xb;
+        finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
+                     row_hi, out + pix0 * Dv, (size_t)Dv, pix0 + lane, pix0 + lane + 32, lane);
     }
 }
 
-// Unit = 32 rows of a horizontal path (column-major census).
+// Unit = 64 rows of a horizontal path (banded census).
 template <typename CT>
-__device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job,
-                                                    int first, uint32_t tstate,
-                                                    uint4* __restrict__ tile, int row_words) {
+__device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job, int first,
+                                                    uint32_t tstate, unsigned char* __restrict__ tile,
+                                                    int row_bytes) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
-    const int Dp = k.Dp;
+    const int Dp = k.Dp, Dv = pr.nd_vec;
+    const bool wide = pr.wide_slabs != 0;
     const int dx = job.dx;
-    const int y = first + lane;                 // row of this lane
-    const bool active = y < job.num_scanlines;
-    const int nrows = min(32, job.num_scanlines - first);
+    const bool act_lo = first + lane < job.num_scanlines;
+    const bool act_hi = first + 32 + lane < job.num_scanlines;
     // Banded census: word (x, y) at ((y / 32) * W + x) * 32 + y % 32, so the 32
-    // rows of this unit (first is a multiple of 32) read 128 contiguous bytes per
+    // rows of a band (first is a multiple of 64) read 128 contiguous bytes per
     // column and column x-d sits at a constant offset of -32*d words. Bands are
-    // allocated whole, so idle lanes (rows >= H) read allocated words.
-    const size_t band = (size_t)(first >> 5) * W;
-    const CT* __restrict__ CL = static_cast<const CT*>(pr.census_lt) + band * 32 + lane;
-    const CT* __restrict__ CR = static_cast<const CT*>(pr.census_rt) + band * 32 + lane;
-    uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
-    uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
-    const int Dv = pr.nd_vec;
-    (void)H;
+    // allocated whole; the second band of a unit that has none (H <= first+32)
+    // is read from the first one and its rows stay idle.
+    const size_t band_lo = (size_t)(first >> 5) * W;
+    const size_t band_hi = first + 32 < H ? band_lo + W : band_lo;
+    const CT* __restrict__ CLl = static_cast<const CT*>(pr.census_lt) + band_lo * 32 + lane;
+    const CT* __restrict__ CLh = static_cast<const CT*>(pr.census_lt) + band_hi * 32 + lane;
+    const CT* __restrict__ CRl = static_cast<const CT*>(pr.census_rt) + band_lo * 32 + lane;
+    const CT* __restrict__ CRh = static_cast<const CT*>(pr.census_rt) + band_hi * 32 + lane;
+    unsigned char* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
 
-    clear_state(tstate, k.G);
+    unsigned char* row_lo = tile + lane * row_bytes;
+    unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
     const int x0 = dx > 0 ? 0 : W - 1;
-    CT lc_next = CL[(size_t)x0 * 32];
+    CT lcn_lo = CLl[(size_t)x0 * 32], lcn_hi = CLh[(size_t)x0 * 32];
     for (int t = 0; t < W; ++t) {
         const int x = x0 + dx * t;
-        const CT lc = lc_next;
-        if (t + 1 < W) lc_next = CL[(size_t)(x + dx) * 32];
-        const CT* col = CR + (size_t)x * 32;        // col[-32*d] = R(x-d, y)
-        auto getR = [col](int d) { return col[-32 * d]; };
-        uint4* otile = tile + lane * row_words;
-        const bool esc = x >= Dp - 1
-                             ? sgm_pixel<false, CT>(tstate, m, lc, getR, x, active, k, otile)
-                             : sgm_pixel<true, CT>(tstate, m, lc, getR, x, active, k, otile);
-        const unsigned em = __ballot_sync(kFull, active && esc);
-        // Rows first..first+nrows-1, one vector per row at column x.
+        const CT lc_lo = lcn_lo, lc_hi = lcn_hi;
+        if (t + 1 < W) {
+            lcn_lo = CLl[(size_t)(x + dx) * 32];
+            lcn_hi = CLh[(size_t)(x + dx) * 32];
+        }
+        const CT* col_lo = CRl + (size_t)x * 32;   // col[-32*d] = R(x-d, y)
+        const CT* col_hi = CRh + (size_t)x * 32;
+        auto getR = [col_lo, col_hi](int d, CT& lo, CT& hi) {
+            lo = col_lo[-32 * d];
+            hi = col_hi[-32 * d];
+        };
+        const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;
+        const uint32_t mx = x >= Dp - 1
+            ? sgm_pixel<false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
+            : sgm_pixel<true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
+        // Rows first..first+63, one vector per row at column x.
         const size_t pix0 = (size_t)first * W + x;
-        if (pr.wide_slabs)
-            flush_tile_wide(tile, row_words, k.G, 0, nrows - 1, shd + pix0 * Dp, (size_t)W * Dp, lane);
-        else
-            flush_tile(tile, row_words, k.G, 0, nrows - 1, em, out + pix0 * Dv, (size_t)W * Dv,
-                       shd + pix0 * Dp, (size_t)W * Dp, lane);
+        finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
+                     row_hi, out + pix0 * Dv, (size_t)W * Dv, pix0 + (size_t)lane * W,
+                     pix0 + (size_t)(lane + 32) * W, lane);
     }
+    (void)H;
 }
 
-// Shared memory per warp: the census staging buffers (2 x (Dp+40) words) and
-// the output tile (32 rows of Dp/8 + 1 16-byte words; the pad word keeps the
-// rows' 16-byte stores on distinct banks).
-__host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, size_t ct) {
-    return 2 * (size_t)(dp_max + 40) * ct + (size_t)32 * (dp_max / 8 + 1) * 16;
-}
+}  // namespace
 
 template <typename CT>
 __global__ void __launch_bounds__(kAggMaxThreads)
@@ -510,11 +573,11 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     extern __shared__ __align__(16) unsigned char agg_smem[];
     __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int seg_words = dp_max + 40;                          // Dp+31 words + alignment
-    const int row_words = dp_max / 8 + 1;                       // tile row: Dp/8 words + pad
+    const int seg_words = aggregate_seg_words(dp_max);
+    const int row_bytes = aggregate_row_bytes(dp_max);
     unsigned char* wbase = agg_smem + (size_t)warp * aggregate_warp_smem(dp_max, sizeof(CT));
     CT* stage = reinterpret_cast<CT*>(wbase);
-    uint4* tile = reinterpret_cast<uint4*>(wbase + 2 * seg_words * sizeof(CT));
+    unsigned char* tile = wbase + 2 * (size_t)seg_words * sizeof(CT);
 
     // TMEM for the state of all the CTA's scanlines, allocated by warp 0 for the
     // whole persistent loop and released by warp 0 after every warp is done.
@@ -541,10 +604,9 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate, tile, row_words);
+            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
         else
-            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile,
-                                  row_words);
+            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
         __syncwarp();
     }
 
@@ -557,26 +619,23 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     }
 }
 
-}  // namespace
-
 // Launch shape of the aggregation kernel for a batch whose largest padded D is
 // dp_max: one CTA per SM (the CUDA occupancy calculator allows one CTA per SM
 // for a kernel that allocates tensor memory) with as many warpgroups as the
-// SM's 512 TMEM columns and registers hold. A warpgroup's 4 warps cover the
-// 128 TMEM lanes and need dp_max/2 columns.
+// SM's 512 TMEM columns, registers and shared memory hold. A warpgroup's 4
+// warps cover the 128 TMEM lanes (256 scanlines) and need dp_max columns.
 struct AggShape {
     int warpgroups;
     int wg_cols;     // columns per warpgroup
     int tmem_cols;   // allocation (power of two >= warpgroups * wg_cols)
-    size_t smem;     // census staging
+    size_t smem;     // census staging + byte tiles
 };
 
 // Largest number of warpgroups one aggregation CTA can hold for this batch:
 // bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
 int aggregate_max_warpgroups(int dp_max, bool census64) {
-    const int wg_cols = dp_max / 2;
-    const int by_tmem = 512 / wg_cols;
-    int regs = 80, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
+    const int by_tmem = 512 / dp_max;
+    int regs = 128, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -607,7 +666,7 @@ int aggregate_default_warpgroups(int dp_max, bool census64, int num_units) {
 
 AggShape aggregate_shape(int dp_max, bool census64, int warpgroups) {
     AggShape sh{};
-    sh.wg_cols = dp_max / 2;
+    sh.wg_cols = dp_max;
     const int wmax = aggregate_max_warpgroups(dp_max, census64);
     sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
     sh.tmem_cols = 32;

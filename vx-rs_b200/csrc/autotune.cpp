@@ -4,7 +4,7 @@
 // scanline is serial work: more warps per SM raise throughput until the
 // longest scanlines, slowed by a crowded SM, dominate). The best count depends
 // on the batch: its largest disparity count, its census word width and how many
-// 32-scanline units it queues. vx_sgm_autotune_batch times every candidate on
+// 64-scanline units it queues. vx_sgm_autotune_batch times every candidate on
 // a real batch with CUDA events around the aggregation launch and records the
 // fastest in the SGMStereo handle; later batches with the same key use it. The
 // table is saved to / loaded from a small JSON file.

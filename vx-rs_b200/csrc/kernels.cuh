@@ -57,7 +57,7 @@ struct JobDev {
     int k_min;             // scanline index offset (diagonals with dx = +1 start at -(H-1))
 };
 
-// A warp's unit of aggregation work: 32 consecutive scanlines of one job.
+// A warp's unit of aggregation work: kUnitScanlines consecutive scanlines of one job.
 struct UnitDev {
     int job;
     int first_scanline;
@@ -66,12 +66,24 @@ struct UnitDev {
 constexpr int kCensusTileW = 32;
 constexpr int kCensusTileH = 8;
 constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
-// Largest aggregation CTA (6 warpgroups); keeps registers per thread <= 85.
-constexpr int kAggMaxThreads = 768;
+// Scanlines per aggregation work unit (one warp: two scanlines per lane).
+constexpr int kUnitScanlines = 64;
+// Largest aggregation CTA (4 warpgroups); keeps registers per thread <= 128.
+constexpr int kAggMaxThreads = 512;
 // Guard words before and after every row-major census plane: the aggregation
 // kernel stages aligned 16-byte chunks that may extend past the first and last
-// row by up to 256 + 40 words.
-constexpr int kCensusGuardWords = 320;
+// row by up to 256 + 72 words.
+constexpr int kCensusGuardWords = 352;
+
+// Shared memory of one aggregation warp for a batch whose largest padded D is
+// dp_max: two census staging buffers (the Dp+63 words of a step plus up to one
+// 16-byte chunk of alignment) and the byte tile of its 64 scanlines (rows of
+// Dv bytes plus 8, so that the rows' 8-byte stores fall on distinct banks).
+__host__ __device__ constexpr int aggregate_seg_words(int dp_max) { return dp_max + 72; }
+__host__ __device__ constexpr int aggregate_row_bytes(int dp_max) { return (dp_max + 15) / 16 * 16 + 8; }
+__host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, size_t ct) {
+    return 2 * (size_t)aggregate_seg_words(dp_max) * ct + (size_t)kUnitScanlines * aggregate_row_bytes(dp_max);
+}
 constexpr int kWtaThreads = 256;
 // Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).
 constexpr int kMaxWidth = 16384;

@@ -52,7 +52,7 @@ size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config
 
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
     const size_t P = cfg.num_paths;
-    const size_t units = P * (((size_t)width + height - 1 + 31) / 32);
+    const size_t units = P * (((size_t)width + height - 1 + kUnitScanlines - 1) / kUnitScanlines);
     return sizeof(PairDev) + P * sizeof(JobDev) + units * sizeof(UnitDev) + sizeof(unsigned) +
            4 * kAlign;
 }
@@ -199,7 +199,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
             j.k_min = (j.dx > 0 && j.dy != 0) ? -(H - 1) : 0;
             const int job = (int)pl.jobs.size();
             pl.jobs.push_back(j);
-            for (int k = 0; k < j.num_scanlines; k += 32) units.push_back({job, k});
+            for (int k = 0; k < j.num_scanlines; k += kUnitScanlines) units.push_back({job, k});
         }
     }
     pl.total_tiles = tiles;
@@ -213,10 +213,10 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         long long len;
         if (j.dy == 0) len = p.width;
         else if (j.dx == 0) len = p.height;
-        else {  // longest of the unit's 32 diagonals
+        else {  // longest of the unit's diagonals
             len = 0;
             const int k0 = j.k_min + u.first_scanline;
-            const int k1 = j.k_min + std::min(u.first_scanline + 32, j.num_scanlines);
+            const int k1 = j.k_min + std::min(u.first_scanline + kUnitScanlines, j.num_scanlines);
             for (int k = k0; k < k1; ++k) {
                 int tb, te;
                 if (j.dx > 0) { tb = std::max(0, -k); te = std::min(p.height, p.width - k); }
