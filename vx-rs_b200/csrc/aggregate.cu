@@ -229,13 +229,14 @@ __device__ __forceinline__ void group_bytes(const Words8& o, uint2& lo, uint2& h
 // = its first lane, column 0). getR(d, lo, hi) = right census words at x-d of
 // the two scanlines; only called with x_hi-d >= 0 when CHECK. m = the previous
 // pixel's minimum per half; start = 0xFFFF in each half whose scanline starts at
-// this pixel. row_lo / row_hi = the two scanlines' rows of the warp's byte tile.
+// this pixel. row_lo / row_hi = the two scanlines' rows of the warp's output
+// tile (u16 values when WIDE, else bytes).
 // Returns the per-half maximum of the new vector (d < D). Software pipeline over
 // groups (loop unrolled by two, register sets in ping-pong): while group g runs
 // its chain, the census words and state of group g+1 are in flight (the state
 // is waited for only before g's last disparity), and g+1's costs are formed
 // right after g's chain.
-template <bool CHECK, typename CT, typename GetR>
+template <bool CHECK, bool WIDE, typename CT, typename GetR>
 __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
                                               const CT lc_lo, const CT lc_hi, const GetR& getR,
                                               const int x_lo, const int x_hi, const ScanConst& k,
@@ -261,10 +262,19 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
         }
     };
     auto store = [&](const Words8& o, int g) {
-        uint2 lo, hi;
-        group_bytes(o, lo, hi);
-        *reinterpret_cast<uint2*>(row_lo + 8 * g) = lo;
-        *reinterpret_cast<uint2*>(row_hi + 8 * g) = hi;
+        if (WIDE) {             // u16 rows: 8 values (16 bytes) per group
+            *reinterpret_cast<uint4*>(row_lo + 16 * g) = make_uint4(
+                __byte_perm(o.w[0], o.w[1], 0x5410), __byte_perm(o.w[2], o.w[3], 0x5410),
+                __byte_perm(o.w[4], o.w[5], 0x5410), __byte_perm(o.w[6], o.w[7], 0x5410));
+            *reinterpret_cast<uint4*>(row_hi + 16 * g) = make_uint4(
+                __byte_perm(o.w[0], o.w[1], 0x7632), __byte_perm(o.w[2], o.w[3], 0x7632),
+                __byte_perm(o.w[4], o.w[5], 0x7632), __byte_perm(o.w[6], o.w[7], 0x7632));
+        } else {                // byte rows: 8 bytes per group
+            uint2 lo, hi;
+            group_bytes(o, lo, hi);
+            *reinterpret_cast<uint2*>(row_lo + 8 * g) = lo;
+            *reinterpret_cast<uint2*>(row_hi + 8 * g) = hi;
+        }
         tmem_st8(tstate + 8 * g, o);
     };
     CT ra_l[8], ra_h[8], rb_l[8], rb_h[8];
@@ -329,17 +339,17 @@ __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
     return k;
 }
 
-// Writes the rows la..lb (a run of active scanlines, 0..63) of the warp's byte
-// tile to the slab: row r's vector (Dv bytes) goes to dst0 + r * stride. The
+// Writes the rows la..lb (a run of active scanlines, 0..63) of the warp's
+// tile to the slab: row r's vector (vb bytes) goes to dst0 + r * stride. The
 // rows' 8-byte chunks are distributed over the lanes in address order (chunk
 // c = (r - la) * V + h, walked with a running (r, h): no division per chunk),
 // so consecutive lanes write consecutive 8 bytes of a vector. Streaming stores:
 // the slabs are read once by the WTA kernel and must not push the census
 // planes, which every path re-reads, out of L2.
-__device__ __forceinline__ void flush_tile(const unsigned char* __restrict__ tile, int row_bytes, int Dv,
+__device__ __forceinline__ void flush_tile(const unsigned char* __restrict__ tile, int row_bytes, int vb,
                                            int la, int lb, unsigned char* __restrict__ dst0, size_t stride,
                                            int lane) {
-    const int V = Dv / 8;
+    const int V = vb / 8;
     const int n = (lb - la + 1) * V;
     const int q = 32 / V, rr = 32 % V;
     int r = la + lane / V, h = lane % V;
@@ -376,31 +386,37 @@ __device__ __forceinline__ void write_u16_vectors(uint32_t tstate, int G, bool w
     }
 }
 
-// After one pixel step: the escape flags of the two scanlines' vectors (a
-// value of 255 or more), the marker in their byte rows, the byte rows of the
-// active run to the slab, and the u16 vectors that need one (escaped vectors,
-// or every vector of a wide slab). pix_lo / pix_hi = the two scanlines' pixel
-// indices (used only for an active scanline); dst0 / stride = byte slab
-// address of tile row 0 and the row stride.
+// After one pixel step: the rows of the active run go to the path's slab.
+// Byte slabs: a vector with a value of 255 or more (escape) gets the marker in
+// byte 0 of its row, and its exact u16 values are read back from TMEM to the
+// shadow slab. Wide slabs: the tile rows are the u16 vectors. pix0 = pixel of
+// tile row 0; pix_lo / pix_hi = this lane's two scanlines' pixels (used only for
+// an active scanline); pstride = pixel stride between tile rows (1 or W).
 __device__ __forceinline__ void finish_pixel(const PairDev& pr, int path, bool wide, int Dv, uint32_t tstate,
                                              int G, uint32_t mx, bool act_lo, bool act_hi,
                                              const unsigned char* tile, int row_bytes, unsigned char* row_lo,
-                                             unsigned char* row_hi, unsigned char* dst0, size_t stride,
-                                             size_t pix_lo, size_t pix_hi, int lane) {
-    const bool esc_lo = act_lo && (wide || (mx & 0xFFFFu) >= 0xFFu);
-    const bool esc_hi = act_hi && (wide || (mx >> 16) >= 0xFFu);
-    if (!wide) {
-        if (esc_lo) row_lo[0] = 0xFFu;
-        if (esc_hi) row_hi[0] = 0xFFu;
-    }
+                                             unsigned char* row_hi, size_t pix0, size_t pstride, size_t pix_lo,
+                                             size_t pix_hi, int lane) {
+    const bool esc_lo = !wide && act_lo && (mx & 0xFFFFu) >= 0xFFu;
+    const bool esc_hi = !wide && act_hi && (mx >> 16) >= 0xFFu;
+    if (esc_lo) row_lo[0] = 0xFFu;
+    if (esc_hi) row_hi[0] = 0xFFu;
     const unsigned al = __ballot_sync(kFull, act_lo), ah = __ballot_sync(kFull, act_hi);
     const unsigned e = __ballot_sync(kFull, esc_lo || esc_hi);
     __syncwarp();
-    if (!wide && (al | ah)) {
+    if (al | ah) {
         // The active scanlines are one run of rows: the low and high runs join.
         const unsigned long long act = (unsigned long long)al | ((unsigned long long)ah << 32);
         const int la = __ffsll((long long)act) - 1, lb = 63 - __clzll((long long)act);
-        flush_tile(tile, row_bytes, Dv, la, lb, dst0, stride, lane);
+        if (wide) {
+            const int Dp = pr.nd_pad;
+            unsigned char* dst = reinterpret_cast<unsigned char*>(pr.shadow + pr.shadow_stride * (size_t)path +
+                                                                  pix0 * Dp);
+            flush_tile(tile, row_bytes, 2 * Dp, la, lb, dst, pstride * Dp * 2, lane);
+        } else {
+            unsigned char* dst = pr.slabs + pr.slab_stride * (size_t)path + pix0 * Dv;
+            flush_tile(tile, row_bytes, Dv, la, lb, dst, pstride * Dv, lane);
+        }
     }
     if (e) {
         uint16_t* base = pr.shadow + pr.shadow_stride * (size_t)path;
@@ -409,8 +425,9 @@ __device__ __forceinline__ void finish_pixel(const PairDev& pr, int path, bool w
     __syncwarp();
 }
 
-// Unit = 64 scanlines of a vertical or diagonal path.
-template <typename CT>
+// Unit = 64 scanlines of a vertical or diagonal path. WT: the batch has
+// wide-slab pairs (the u16 body is compiled in).
+template <typename CT, bool WT>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
                                                   uint32_t tstate, CT* __restrict__ stage,
                                                   int seg_words, unsigned char* __restrict__ tile,
@@ -419,7 +436,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
     const int Dp = k.Dp, Dv = pr.nd_vec;
-    const bool wide = pr.wide_slabs != 0;
+    const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx, dy = job.dy;
 
     const int k0 = job.k_min + first;         // scanline index of tile row 0
@@ -442,8 +459,6 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
 
     const CT* __restrict__ CL = static_cast<const CT*>(pr.census_l);
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
-    unsigned char* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
-
     // Stage the right-census segment [xb-(Dp-1), xb+63] of the step's row in
     // 16-byte chunks from the aligned word at or below its start. The planes are
     // surrounded by guard words (kCensusGuardWords), so the chunks may run past
@@ -497,17 +512,21 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
             hi = seg[32 - d];
         };
         const int x_lo = xb + lane, x_hi = xb + lane + 32;
-        const uint32_t mx = xb >= Dp - 1
-            ? sgm_pixel<false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
-            : sgm_pixel<true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
+        uint32_t mx;
+        if (xb >= Dp - 1)
+            mx = wide ? sgm_pixel<false, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
+                      : sgm_pixel<false, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
+        else
+            mx = wide ? sgm_pixel<true, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
+                      : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
         const size_t pix0 = (size_t)y * W + xb;
         finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
-                     row_hi, out + pix0 * Dv, (size_t)Dv, pix0 + lane, pix0 + lane + 32, lane);
+                     row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
     }
 }
 
 // Unit = 64 rows of a horizontal path (banded census).
-template <typename CT>
+template <typename CT, bool WT>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job, int first,
                                                     uint32_t tstate, unsigned char* __restrict__ tile,
                                                     int row_bytes) {
@@ -515,7 +534,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
     const int Dp = k.Dp, Dv = pr.nd_vec;
-    const bool wide = pr.wide_slabs != 0;
+    const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx;
     const bool act_lo = first + lane < job.num_scanlines;
     const bool act_hi = first + 32 + lane < job.num_scanlines;
@@ -530,8 +549,6 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const CT* __restrict__ CLh = static_cast<const CT*>(pr.census_lt) + band_hi * 32 + lane;
     const CT* __restrict__ CRl = static_cast<const CT*>(pr.census_rt) + band_lo * 32 + lane;
     const CT* __restrict__ CRh = static_cast<const CT*>(pr.census_rt) + band_hi * 32 + lane;
-    unsigned char* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
-
     unsigned char* row_lo = tile + lane * row_bytes;
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
@@ -551,21 +568,24 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
             hi = col_hi[-32 * d];
         };
         const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;
-        const uint32_t mx = x >= Dp - 1
-            ? sgm_pixel<false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
-            : sgm_pixel<true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
+        uint32_t mx;
+        if (x >= Dp - 1)
+            mx = wide ? sgm_pixel<false, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
+                      : sgm_pixel<false, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
+        else
+            mx = wide ? sgm_pixel<true, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
+                      : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
         // Rows first..first+63, one vector per row at column x.
         const size_t pix0 = (size_t)first * W + x;
         finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
-                     row_hi, out + pix0 * Dv, (size_t)W * Dv, pix0 + (size_t)lane * W,
-                     pix0 + (size_t)(lane + 32) * W, lane);
+                     row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
     }
     (void)H;
 }
 
 }  // namespace
 
-template <typename CT>
+template <typename CT, bool WT>
 __global__ void __launch_bounds__(kAggMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
@@ -574,8 +594,8 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg_words = aggregate_seg_words(dp_max);
-    const int row_bytes = aggregate_row_bytes(dp_max);
-    unsigned char* wbase = agg_smem + (size_t)warp * aggregate_warp_smem(dp_max, sizeof(CT));
+    const int row_bytes = aggregate_row_bytes(dp_max, WT);
+    unsigned char* wbase = agg_smem + (size_t)warp * aggregate_warp_smem(dp_max, sizeof(CT), WT);
     CT* stage = reinterpret_cast<CT*>(wbase);
     unsigned char* tile = wbase + 2 * (size_t)seg_words * sizeof(CT);
 
@@ -604,9 +624,9 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
+            run_horizontal_unit<CT, WT>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
         else
-            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
+            run_vertical_unit<CT, WT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
         __syncwarp();
     }
 
@@ -617,6 +637,13 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                      "r"(tmem_cols));
     }
+}
+
+// The kernel for a batch's census word width and tile format.
+const void* aggregate_kernel_fn(bool census64, bool wide_tiles) {
+    if (census64) return wide_tiles ? (const void*)aggregate_kernel<uint64_t, true>
+                                    : (const void*)aggregate_kernel<uint64_t, false>;
+    return wide_tiles ? (const void*)aggregate_kernel<uint32_t, true> : (const void*)aggregate_kernel<uint32_t, false>;
 }
 
 // Launch shape of the aggregation kernel for a batch whose largest padded D is
@@ -633,45 +660,43 @@ struct AggShape {
 
 // Largest number of warpgroups one aggregation CTA can hold for this batch:
 // bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
-int aggregate_max_warpgroups(int dp_max, bool census64) {
+int aggregate_max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
     const int by_tmem = 512 / dp_max;
     int regs = 128, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, census64 ? (const void*)aggregate_kernel<uint64_t>
-                                            : (const void*)aggregate_kernel<uint32_t>) ==
-            cudaSuccess &&
-        fa.numRegs > 0)
+    if (cudaFuncGetAttributes(&fa, aggregate_kernel_fn(census64, wide_tiles)) == cudaSuccess && fa.numRegs > 0)
         regs = fa.numRegs;
     cudaGetLastError();
     const int by_regs = regs_sm / (regs * 128);
-    const int by_smem = (int)((smem_sm - 1024) / (4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4)));
+    const int by_smem =
+        (int)((smem_sm - 1024) / (4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4, wide_tiles)));
     return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
 }
 
-int aggregate_default_warpgroups(int dp_max, bool census64, int num_units) {
+int aggregate_default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units) {
     // Most warpgroups that still leave every warp ~2.5 units of the queue: a
     // scanline is serial work, so a crowded SM slows the longest units down and
     // few units per warp cannot even that out.
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int wmax = aggregate_max_warpgroups(dp_max, census64);
+    const int wmax = aggregate_max_warpgroups(dp_max, census64, wide_tiles);
     int w = 1;
     while (w < wmax && (double)num_units >= 2.5 * sms * 4 * (w + 1)) ++w;
     return w;
 }
 
-AggShape aggregate_shape(int dp_max, bool census64, int warpgroups) {
+AggShape aggregate_shape(int dp_max, bool census64, bool wide_tiles, int warpgroups) {
     AggShape sh{};
     sh.wg_cols = dp_max;
-    const int wmax = aggregate_max_warpgroups(dp_max, census64);
+    const int wmax = aggregate_max_warpgroups(dp_max, census64, wide_tiles);
     sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
     sh.tmem_cols = 32;
     while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
-    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4);
+    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4, wide_tiles);
     return sh;
 }
 
@@ -682,7 +707,8 @@ cudaError_t prepare_aggregate_kernels() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaError_t e = cudaSuccess;
-    for (const void* fn : {(const void*)aggregate_kernel<uint32_t>, (const void*)aggregate_kernel<uint64_t>}) {
+    for (const void* fn : {aggregate_kernel_fn(false, false), aggregate_kernel_fn(true, false),
+                           aggregate_kernel_fn(false, true), aggregate_kernel_fn(true, true)}) {
         cudaFuncAttributes fa{};
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)   // dynamic + static shared memory must fit the opt-in limit
@@ -704,12 +730,12 @@ int aggregate_grid_ctas(int dp_max, bool census64) {
     return sms;
 }
 
-cudaError_t launch_aggregate(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs,
-                             const JobDev* d_jobs, const UnitDev* d_units, int num_units,
-                             unsigned* counter, cudaStream_t stream) {
+cudaError_t launch_aggregate(int dp_max, bool census64, bool wide_tiles, int warpgroups,
+                             const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
+                             int num_units, unsigned* counter, cudaStream_t stream) {
     if (num_units <= 0) return cudaSuccess;
-    if (warpgroups <= 0) warpgroups = aggregate_default_warpgroups(dp_max, census64, num_units);
-    const AggShape sh = aggregate_shape(dp_max, census64, warpgroups);
+    if (warpgroups <= 0) warpgroups = aggregate_default_warpgroups(dp_max, census64, wide_tiles, num_units);
+    const AggShape sh = aggregate_shape(dp_max, census64, wide_tiles, warpgroups);
     const int threads = sh.warpgroups * 128;
     int grid_ctas = aggregate_grid_ctas(dp_max, census64);
     const int needed = (num_units + threads / 32 - 1) / (threads / 32);
@@ -718,13 +744,10 @@ cudaError_t launch_aggregate(int dp_max, bool census64, int warpgroups, const Pa
         std::fprintf(stderr, "vx_sgm: aggregation %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
                      grid_ctas, sh.warpgroups, sh.tmem_cols, sh.smem);
     count_launch();
-    if (census64)
-        aggregate_kernel<uint64_t><<<grid_ctas, threads, sh.smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
-    else
-        aggregate_kernel<uint32_t><<<grid_ctas, threads, sh.smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
-    return cudaGetLastError();
+    void* args[] = {&d_pairs, &d_jobs, &d_units, &num_units, &counter, &dp_max,
+                    const_cast<int*>(&sh.tmem_cols), const_cast<int*>(&sh.wg_cols)};
+    return cudaLaunchKernel(aggregate_kernel_fn(census64, wide_tiles), dim3(grid_ctas), dim3(threads), args,
+                            sh.smem, stream);
 }
 
 }  // namespace vxsgm

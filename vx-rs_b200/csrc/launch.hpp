@@ -24,11 +24,12 @@ cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles
 // holds), sharing one tensor-memory allocation for the scanline state.
 cudaError_t prepare_aggregate_kernels();  // shared-memory limits; once per device
 int aggregate_grid_ctas(int dp_max, bool census64);
-int aggregate_max_warpgroups(int dp_max, bool census64);
-int aggregate_default_warpgroups(int dp_max, bool census64, int num_units);
-cudaError_t launch_aggregate(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs,
-                             const JobDev* d_jobs, const UnitDev* d_units, int num_units,
-                             unsigned* counter, cudaStream_t stream);
+// wide_tiles: the batch has wide-slab pairs (u16 output tiles).
+int aggregate_max_warpgroups(int dp_max, bool census64, bool wide_tiles);
+int aggregate_default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units);
+cudaError_t launch_aggregate(int dp_max, bool census64, bool wide_tiles, int warpgroups,
+                             const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
+                             int num_units, unsigned* counter, cudaStream_t stream);
 
 // WTA + subpixel + optional LR check: one CTA per (pair, row). The kernel keeps
 // three words per pixel of the row in shared memory.

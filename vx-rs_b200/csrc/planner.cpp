@@ -179,6 +179,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         pd.census_rt = reinterpret_cast<void*>(data + 2 * cplane + bplane);
         data += 2 * cplane + 2 * bplane;
         pd.wide_slabs = wide_slabs(c) ? 1 : 0;
+        if (pd.wide_slabs) pl.wide_tiles = true;
         pd.slab_stride = pd.wide_slabs ? 0 : npx * (size_t)Dv;
         pd.slabs = reinterpret_cast<uint8_t*>(data);
         data += align_up(pd.slab_stride * P);
@@ -297,7 +298,7 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) record(ev[1]);
-    e = launch_aggregate(pl.dp_max, pl.census64, warpgroups, d_pairs, d_jobs, d_units,
+    e = launch_aggregate(pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) record(ev[2]);
