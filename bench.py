@@ -196,6 +196,83 @@ def run_serve_sweep(args, local_rank):
                                       "x D{64,128,192}, 8 paths", **res}), flush=True)
 
 
+# The single-pair and high-resolution configurations of the metric (besides the
+# 64-pair batch): (name, pairs, w, h, D, paths, scene, d_lo, d_hi, description).
+CONFIG_TABLE = [
+    ("c0", 1, 640, 480, 64, 4, "planes", 4, 60, "640x480 D=64, 4 paths, LR tol 1, 5x5 census"),
+    ("c1", 1, 1242, 375, 128, 8, "slanted", 0, 120, "1242x375 D=128, 8 paths, subpixel, LR, 5x5 census"),
+    ("c3", 16, 2048, 1536, 256, 8, "surface", 0, 230,
+     "16 x 2048x1536 D=256, 8 paths, planes + sinusoid + 10% textureless, staged batches"),
+]
+
+
+def run_config_table(args, local_rank):
+    """One JSON line per configuration: the plain per-pair path (one synchronous call per
+    pair, device-resident images, CUDA events; p50/p99 over repeats), the batched path
+    for the multi-pair configuration, and the CPU oracle on one pair of it."""
+    import torch
+
+    import vx_sgm
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    torch.cuda.set_device(local_rank)
+    ctx = vx_sgm.Context(local_rank)
+    sgm = vx_sgm.SGMStereo(ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    scenes = {"planes": vx_sgm.SCENE_PLANES, "slanted": vx_sgm.SCENE_SLANTED, "surface": vx_sgm.SCENE_SURFACE}
+    threads = os.cpu_count() or 1
+    for (name, n, w, h, d, paths, scene, lo, hi, desc) in CONFIG_TABLE:
+        cfg = vx_sgm.SGMStereoConfig(num_disparities=d, p1=10.0, p2=120.0, census_radius_x=2,
+                                     census_radius_y=2, num_paths=paths, subpixel=True,
+                                     lr_check=True, lr_tolerance=1, invalid_value=-1.0)
+        pairs = [vx_sgm.synth_pair(scenes[scene], w, h, lo, hi, 4242 + i)[:2] for i in range(n)]
+        tl = [ctx.texture_gray8(L, w, h) for L, _ in pairs]
+        tr = [ctx.texture_gray8(R, w, h) for _, R in pairs]
+        of = [ctx.texture_output_r32float(w, h) for _ in pairs]
+        oi = [ctx.texture_output_i16(w, h) for _ in pairs]
+        pd = w * h * d
+        # plain: one synchronous call per pair (the reference's call pattern)
+        reps = max(3, 40 // n)
+        for i in range(min(n, 3)):
+            sgm.compute_disparity(ctx, tl[i], tr[i], of[i], cfg, output_i16=oi[i])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lat = []
+        for r in range(reps):
+            i = r % n
+            e0.record(stream)
+            sgm.compute_disparity(ctx, tl[i], tr[i], of[i], cfg, output_i16=oi[i])
+            e1.record(stream)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        line = {"config": name, "workload": desc, "pairs": n, "pd_per_pair": pd,
+                "plain": {"value": pd / (float(np.mean(lat)) * 1e-3) / 1e9, "unit": UNIT,
+                          "latency_ms_p50": float(np.percentile(lat, 50)),
+                          "latency_ms_p99": float(np.percentile(lat, 99)), "calls": reps}}
+        if n > 1:
+            cfgs = [cfg] * n
+            for _ in range(2):
+                sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
+            ctx.synchronize()
+            steps = 3
+            e0.record(stream)
+            for _ in range(steps):
+                sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            line["batched"] = {"value": n * pd / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+                               "workspace_per_pair_bytes": vx_sgm.workspace_bytes(w, h, cfg)}
+        ocfg = oracle.config(num_disparities=d, p1=10, p2=120, census_radius_x=2, census_radius_y=2,
+                             num_paths=paths, subpixel=True, lr_check=True)
+        t0 = time.perf_counter()
+        oracle.sgm(pairs[0][0], pairs[0][1], ocfg, nthreads=threads)
+        secs = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": pd / secs / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"one pair ({pd / 1e6:.1f} M pd, {secs:.2f} s)"}
+        print(json.dumps(line), flush=True)
+        del tl, tr, of, oi
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -240,6 +317,9 @@ def main():
                          "line per rate instead of the benchmark")
     ap.add_argument("--pairs", type=int, default=0,
                     help="keep only the first N pairs of the workload (small profiler cases)")
+    ap.add_argument("--config-table", action="store_true",
+                    help="print one JSON line per single-pair / high-resolution configuration "
+                         "(plain latency, batched throughput, CPU oracle) instead of the benchmark")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
@@ -264,6 +344,9 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     import vx_sgm
+    if args.config_table:
+        run_config_table(args, local_rank)
+        return
     if args.serve_sweep:
         run_serve_sweep(args, local_rank)
         return

@@ -27,6 +27,14 @@ def gpu_ctx():
     ctx.close()
 
 
+@pytest.fixture(params=["single", "pairs"])
+def agg_form(request, monkeypatch):
+    """Runs a test through each aggregation form: the single-scanline kernel (the
+    planner's choice for few units) and the scanline-pair kernel (large batches)."""
+    monkeypatch.setenv("VX_SGM_AGG_FORM", request.param)
+    return request.param
+
+
 @pytest.fixture(scope="session")
 def sgm(gpu_ctx):
     import vx_sgm

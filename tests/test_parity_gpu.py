@@ -10,7 +10,7 @@ from gpu_helpers import assert_disparity_equal, cfg_pair, run_batch, run_pair
 pytestmark = pytest.mark.gpu
 
 
-def test_golden_reference_cases(gpu_ctx, sgm, golden):
+def test_golden_reference_cases(gpu_ctx, sgm, golden, agg_form):
     """Reference configuration (2 paths, subpixel, no LR) reproduces the reference shader's
     census words, cost volume and f32 disparity bit for bit."""
     for c in golden:
@@ -34,7 +34,7 @@ def test_golden_reference_cases(gpu_ctx, sgm, golden):
     (64, 2, 2, 77, 41), (128, 2, 2, 150, 33), (192, 4, 3, 213, 29), (256, 2, 2, 300, 20),
     (48, 4, 3, 61, 37), (100, 1, 1, 90, 31), (7, 2, 2, 19, 13), (1, 1, 1, 9, 7),
 ])
-def test_each_path_bit_exact(gpu_ctx, sgm, nd, rx, ry, w, h):
+def test_each_path_bit_exact(gpu_ctx, sgm, nd, rx, ry, w, h, agg_form):
     """All 8 path directions' L_r, dumped from the path slabs, equal the oracle's."""
     L, R, _ = vx_sgm.synth_pair(0, w, h, 0, max(1, nd - 4), nd * 1000 + w)
     cfg, _ = cfg_pair(num_disparities=nd, census_radius_x=rx, census_radius_y=ry, num_paths=8)
@@ -63,7 +63,7 @@ def test_each_path_bit_exact(gpu_ctx, sgm, nd, rx, ry, w, h):
          census_radius_y=2, num_paths=8, p1=15, p2=300, lr_check=True,
          lr_tolerance=0),                                                      # u16-range values
 ])
-def test_full_pipeline_matches_oracle(gpu_ctx, sgm, case):
+def test_full_pipeline_matches_oracle(gpu_ctx, sgm, case, agg_form):
     case = dict(case)
     scene, w, h, lo, hi = (case.pop(k) for k in ("scene", "w", "h", "lo", "hi"))
     L, R, _ = vx_sgm.synth_pair(scene, w, h, lo, hi, 42)
@@ -73,7 +73,7 @@ def test_full_pipeline_matches_oracle(gpu_ctx, sgm, case):
     assert_disparity_equal(got, (d, di), what=str(case))
 
 
-def test_edge_shapes(gpu_ctx, sgm):
+def test_edge_shapes(gpu_ctx, sgm, agg_form):
     for (w, h, nd) in [(1, 1, 1), (1, 17, 8), (23, 1, 16), (5, 9, 64), (16384, 2, 8), (2, 300, 256)]:
         L, R, _ = vx_sgm.synth_pair(0, w, h, 0, max(0, min(nd - 1, w - 1)), w * 7 + h)
         cfg, ocfg = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2,
@@ -83,7 +83,7 @@ def test_edge_shapes(gpu_ctx, sgm):
         assert_disparity_equal(got, (d, di), what=f"{w}x{h} D={nd}")
 
 
-def test_batch_equals_solo(gpu_ctx, sgm):
+def test_batch_equals_solo(gpu_ctx, sgm, agg_form):
     rng = np.random.default_rng(1)
     pairs, cfgs = [], []
     for i in range(9):

@@ -36,7 +36,7 @@ def _escape_stats(Lk):
 
 @pytest.mark.parametrize("fmt", FORMATS)
 @pytest.mark.parametrize("case", CASES)
-def test_paths_bit_exact_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt, case):
+def test_paths_bit_exact_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt, case, agg_form):
     w, h, nd, rx, ry, p1, p2, seed = case
     monkeypatch.setenv("VX_SGM_SLAB_FORMAT", fmt)
     L, R, _ = vx_sgm.synth_pair(0, w, h, 2, max(1, nd - 4), seed)
@@ -64,7 +64,7 @@ def test_paths_bit_exact_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt, case):
 
 @pytest.mark.parametrize("fmt", FORMATS)
 @pytest.mark.parametrize("case", CASES)
-def test_disparity_matches_oracle_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt, case):
+def test_disparity_matches_oracle_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt, case, agg_form):
     """WTA reads escaped vectors from the shadow (byte slabs) or every vector (wide)."""
     w, h, nd, rx, ry, p1, p2, seed = case
     monkeypatch.setenv("VX_SGM_SLAB_FORMAT", fmt)
@@ -77,7 +77,7 @@ def test_disparity_matches_oracle_in_both_formats(gpu_ctx, sgm, monkeypatch, fmt
 
 
 @pytest.mark.parametrize("fmt", FORMATS)
-def test_golden_cases_in_both_formats(gpu_ctx, sgm, golden, monkeypatch, fmt):
+def test_golden_cases_in_both_formats(gpu_ctx, sgm, golden, monkeypatch, fmt, agg_form):
     """The reference's own outputs (f32 disparity bits, cost volume) in either format."""
     monkeypatch.setenv("VX_SGM_SLAB_FORMAT", fmt)
     for c in golden:

@@ -1,5 +1,8 @@
-// Path aggregation of semi-global matching: every path of every pair of a batch
-// in ONE persistent launch over a work queue of (pair, path, 64-scanline) units.
+// Path aggregation of semi-global matching, scanline-pair form: every path of
+// every pair of a batch in ONE persistent launch over a work queue of (pair,
+// path, 64-scanline) units. Large batches run this form (fewer instructions per
+// path-pixel-disparity); plans with few units run the single-scanline form
+// (aggregate_single.cu).
 //
 // Semantics (vx-vision/shaders/SGMStereo.metal:72-173), per scanline, per pixel,
 // for d = 0..D-1 in increasing order with ONE array Lp[] updated in place:
@@ -62,6 +65,7 @@
 #include "launch.hpp"
 
 namespace vxsgm {
+namespace pairs {
 
 namespace {
 
@@ -660,7 +664,7 @@ struct AggShape {
 
 // Largest number of warpgroups one aggregation CTA can hold for this batch:
 // bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
-int aggregate_max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
+int max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
     const int by_tmem = 512 / dp_max;
     int regs = 128, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
@@ -676,23 +680,23 @@ int aggregate_max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
     return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
 }
 
-int aggregate_default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units) {
+int default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units) {
     // Most warpgroups that still leave every warp ~2.5 units of the queue: a
     // scanline is serial work, so a crowded SM slows the longest units down and
     // few units per warp cannot even that out.
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int wmax = aggregate_max_warpgroups(dp_max, census64, wide_tiles);
+    const int wmax = max_warpgroups(dp_max, census64, wide_tiles);
     int w = 1;
     while (w < wmax && (double)num_units >= 2.5 * sms * 4 * (w + 1)) ++w;
     return w;
 }
 
-AggShape aggregate_shape(int dp_max, bool census64, bool wide_tiles, int warpgroups) {
+static AggShape shape_for(int dp_max, bool census64, bool wide_tiles, int warpgroups) {
     AggShape sh{};
     sh.wg_cols = dp_max;
-    const int wmax = aggregate_max_warpgroups(dp_max, census64, wide_tiles);
+    const int wmax = max_warpgroups(dp_max, census64, wide_tiles);
     sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
     sh.tmem_cols = 32;
     while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
@@ -700,7 +704,7 @@ AggShape aggregate_shape(int dp_max, bool census64, bool wide_tiles, int warpgro
     return sh;
 }
 
-cudaError_t prepare_aggregate_kernels() {
+cudaError_t prepare() {
     // Dynamic shared memory up to the largest staging area, and the smallest
     // shared-memory carveout: the rest of the SM's L1 caches the census windows.
     int dev = 0, max_bytes = 227 * 1024;
@@ -721,7 +725,7 @@ cudaError_t prepare_aggregate_kernels() {
     return e;
 }
 
-int aggregate_grid_ctas(int dp_max, bool census64) {
+static int grid_ctas_for(int dp_max, bool census64) {
     (void)dp_max;
     (void)census64;
     int dev = 0, sms = 0;
@@ -730,24 +734,46 @@ int aggregate_grid_ctas(int dp_max, bool census64) {
     return sms;
 }
 
-cudaError_t launch_aggregate(int dp_max, bool census64, bool wide_tiles, int warpgroups,
-                             const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                             int num_units, unsigned* counter, cudaStream_t stream) {
+cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
+                   const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
+                   cudaStream_t stream) {
     if (num_units <= 0) return cudaSuccess;
-    if (warpgroups <= 0) warpgroups = aggregate_default_warpgroups(dp_max, census64, wide_tiles, num_units);
-    const AggShape sh = aggregate_shape(dp_max, census64, wide_tiles, warpgroups);
+    if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, census64, wide_tiles, num_units);
+    const AggShape sh = shape_for(dp_max, census64, wide_tiles, warpgroups);
     const int threads = sh.warpgroups * 128;
-    int grid_ctas = aggregate_grid_ctas(dp_max, census64);
+    int grid_ctas = grid_ctas_for(dp_max, census64);
     const int needed = (num_units + threads / 32 - 1) / (threads / 32);
     if (grid_ctas > needed) grid_ctas = needed;
     if (std::getenv("VX_SGM_DEBUG"))
-        std::fprintf(stderr, "vx_sgm: aggregation %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
+        std::fprintf(stderr, "vx_sgm: aggregation (pairs) %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
                      grid_ctas, sh.warpgroups, sh.tmem_cols, sh.smem);
     count_launch();
     void* args[] = {&d_pairs, &d_jobs, &d_units, &num_units, &counter, &dp_max,
                     const_cast<int*>(&sh.tmem_cols), const_cast<int*>(&sh.wg_cols)};
     return cudaLaunchKernel(aggregate_kernel_fn(census64, wide_tiles), dim3(grid_ctas), dim3(threads), args,
                             sh.smem, stream);
+}
+
+}  // namespace pairs
+
+// Both forms, dispatched on the plan's unit size (launch.hpp).
+cudaError_t prepare_aggregate_kernels() {
+    cudaError_t e = pairs::prepare();
+    return e == cudaSuccess ? single::prepare() : e;
+}
+
+int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool wide_tiles) {
+    return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, census64, wide_tiles)
+                                            : single::max_warpgroups(dp_max, census64);
+}
+
+cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, int warpgroups,
+                             const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
+                             int num_units, unsigned* counter, cudaStream_t stream) {
+    if (unit_scanlines == kUnitScanlines)
+        return pairs::launch(dp_max, census64, wide_tiles, warpgroups, d_pairs, d_jobs, d_units, num_units,
+                             counter, stream);
+    return single::launch(dp_max, census64, warpgroups, d_pairs, d_jobs, d_units, num_units, counter, stream);
 }
 
 }  // namespace vxsgm

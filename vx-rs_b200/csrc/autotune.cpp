@@ -25,6 +25,7 @@ TuneKey tune_key(const Plan& plan) {
     k.census64 = plan.census64 ? 1 : 0;
     k.units_log2 = plan.units.empty() ? 0 : (int)std::floor(std::log2((double)plan.units.size()));
     k.wide = plan.wide_tiles ? 1 : 0;
+    k.unit_scanlines = plan.unit_scanlines;
     return k;
 }
 
@@ -64,7 +65,7 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
     bind_plan(plan, ws);
     cudaEvent_t ev[4] = {};
     for (auto& x : ev) cudaEventCreate(&x);
-    const int wmax = aggregate_max_warpgroups(plan.dp_max, plan.census64, plan.wide_tiles);
+    const int wmax = aggregate_max_warpgroups(plan.unit_scanlines, plan.dp_max, plan.census64, plan.wide_tiles);
     int best_w = 0;
     float best = 0.0f;
     for (int w = 1; w <= wmax && st == VX_OK; ++w) {
@@ -107,7 +108,7 @@ vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path) {
     for (const auto& kv : sgm->tuned) {
         f << (first ? "" : ", ") << "{\"dp_max\": " << kv.first.dp_max
           << ", \"census64\": " << kv.first.census64 << ", \"units_log2\": " << kv.first.units_log2
-          << ", \"wide\": " << kv.first.wide
+          << ", \"wide\": " << kv.first.wide << ", \"unit_scanlines\": " << kv.first.unit_scanlines
           << ", \"warpgroups\": " << kv.second.warpgroups
           << ", \"aggregate_ms\": " << kv.second.aggregate_ms << "}";
         first = false;
@@ -138,13 +139,14 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
     while ((pos = text.find('{', pos + 1)) != std::string::npos) {
         const size_t end = text.find('}', pos);
         if (end == std::string::npos) break;
-        double dp, c64, ul, wg, ms = 0, wide = 0;
+        double dp, c64, ul, wg, ms = 0, wide = 0, us = 32;
         if (field(pos, end, "dp_max", &dp) && field(pos, end, "census64", &c64) &&
             field(pos, end, "units_log2", &ul) && field(pos, end, "warpgroups", &wg)) {
             field(pos, end, "aggregate_ms", &ms);
             field(pos, end, "wide", &wide);
+            field(pos, end, "unit_scanlines", &us);
             if (wg >= 1 && dp >= 8) {
-                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide}] = {(int)wg, (float)ms};
+                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide, (int)us}] = {(int)wg, (float)ms};
                 ++loaded;
             }
         }

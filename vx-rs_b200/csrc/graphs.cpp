@@ -10,6 +10,7 @@
 // goes back to the context's pool. All calls of one bucket must be ordered on
 // one stream (they share its workspace).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
@@ -32,6 +33,10 @@ std::string bucket_key(const std::vector<PairSpec>& specs) {
           << ',' << c.subpixel << ',' << c.lr_check << ',' << c.lr_tolerance << ',' << inv << ','
           << (s.out_i16 ? 1 : 0) << ',' << (s.out_depth ? 1 : 0) << ';';
     }
+    // The planner's overrides of the slab format and the aggregation form
+    // change the plan for the same shapes.
+    for (const char* v : {"VX_SGM_SLAB_FORMAT", "VX_SGM_AGG_FORM"})
+        if (const char* e = std::getenv(v)) k << v << '=' << e << ';';
     return k.str();
 }
 

@@ -66,8 +66,11 @@ struct UnitDev {
 constexpr int kCensusTileW = 32;
 constexpr int kCensusTileH = 8;
 constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
-// Scanlines per aggregation work unit (one warp: two scanlines per lane).
+// Scanlines per aggregation work unit of the scanline-pair kernel (one warp:
+// two scanlines per lane); the single-scanline kernel takes 32.
 constexpr int kUnitScanlines = 64;
+// Fewest 64-scanline units for which a batch runs the scanline-pair kernel.
+constexpr long long kPairKernelMinUnits = 2048;
 // Largest aggregation CTA (4 warpgroups); keeps registers per thread <= 128.
 constexpr int kAggMaxThreads = 512;
 // Guard words before and after every row-major census plane: the aggregation

@@ -52,7 +52,7 @@ size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config
 
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
     const size_t P = cfg.num_paths;
-    const size_t units = P * (((size_t)width + height - 1 + kUnitScanlines - 1) / kUnitScanlines);
+    const size_t units = P * (((size_t)width + height - 1 + 31) / 32);     // 32-scanline units at most
     return sizeof(PairDev) + P * sizeof(JobDev) + units * sizeof(UnitDev) + sizeof(unsigned) +
            4 * kAlign;
 }
@@ -198,13 +198,27 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
             j.dy = kDirs[p][1];
             j.num_scanlines = j.dy == 0 ? H : (j.dx == 0 ? W : W + H - 1);
             j.k_min = (j.dx > 0 && j.dy != 0) ? -(H - 1) : 0;
-            const int job = (int)pl.jobs.size();
             pl.jobs.push_back(j);
-            for (int k = 0; k < j.num_scanlines; k += kUnitScanlines) units.push_back({job, k});
         }
     }
     pl.total_tiles = tiles;
     pl.total_rows = rows;
+
+    // Unit size, i.e. aggregation form: a batch with enough 64-scanline units to
+    // give every warp of the GPU several runs the scanline-pair kernel; fewer
+    // units (a single pair, small batches) run the single-scanline kernel on
+    // 32-scanline units, twice the parallelism for the same work.
+    long long units64 = 0;
+    for (const JobDev& j : pl.jobs) units64 += (j.num_scanlines + kUnitScanlines - 1) / kUnitScanlines;
+    pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines : 32;
+    // VX_SGM_AGG_FORM=pairs|single forces one form (both are exact; the tests run
+    // every case through each).
+    if (const char* f = std::getenv("VX_SGM_AGG_FORM")) {
+        if (std::strcmp(f, "pairs") == 0) pl.unit_scanlines = kUnitScanlines;
+        if (std::strcmp(f, "single") == 0) pl.unit_scanlines = 32;
+    }
+    for (int job = 0; job < (int)pl.jobs.size(); ++job)
+        for (int k = 0; k < pl.jobs[job].num_scanlines; k += pl.unit_scanlines) units.push_back({job, k});
 
     // Longest work first inside each persistent launch (LPT order): a unit's
     // cost is its longest scanline times D.
@@ -217,7 +231,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
         else {  // longest of the unit's diagonals
             len = 0;
             const int k0 = j.k_min + u.first_scanline;
-            const int k1 = j.k_min + std::min(u.first_scanline + kUnitScanlines, j.num_scanlines);
+            const int k1 = j.k_min + std::min(u.first_scanline + pl.unit_scanlines, j.num_scanlines);
             for (int k = k0; k < k1; ++k) {
                 int tb, te;
                 if (j.dx > 0) { tb = std::max(0, -k); te = std::min(p.height, p.width - k); }
@@ -298,7 +312,7 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) record(ev[1]);
-    e = launch_aggregate(pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
+    e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) record(ev[2]);

@@ -113,10 +113,10 @@ vx_status vx_sgm_create(vx_ctx* ctx, vx_sgm** out) {
         return fail(VX_ERR_SHADER_MISSING, "SGM kernels unavailable on device %d: %s", ctx->device,
                     cudaGetErrorString(e));
     }
-    if (aggregate_grid_ctas(256, true) <= 0) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess || sms <= 0) {
         cudaGetLastError();
-        return fail(VX_ERR_PIPELINE_COMPILE, "aggregation kernel has no occupancy on device %d",
-                    ctx->device);
+        return fail(VX_ERR_PIPELINE_COMPILE, "no multiprocessors on device %d", ctx->device);
     }
     auto* s = new vx_sgm;
     s->ctx = ctx;

@@ -93,6 +93,7 @@ struct Plan {
     std::vector<UnitDev> units;     // all (pair, path, scanline-group) units, longest first
     bool census64 = false;
     bool wide_tiles = false;        // some pair has wide (u16) slabs
+    int unit_scanlines = 32;        // 64: scanline-pair kernel, 32: single-scanline kernel
     int dp_max = 8;                 // largest padded disparity count
     int total_tiles = 0, total_rows = 0, max_width = 0, max_rx = 0, max_ry = 0;
     // Workspace layout (byte offsets from the workspace base).
@@ -127,14 +128,16 @@ vx_status launch_plan(const Plan& plan, char* base, cudaStream_t stream, cudaEve
                       int warpgroups, bool capturing);
 
 // Autotuning key of a batch: the aggregation launch shape depends on the
-// largest padded D, the census word width, the tile format and the amount of
-// queued work.
+// kernel form (unit size), the largest padded D, the census word width, the
+// tile format and the amount of queued work.
 struct TuneKey {
     int dp_max;
     int census64;
     int units_log2;
     int wide;
+    int unit_scanlines;
     bool operator<(const TuneKey& o) const {
+        if (unit_scanlines != o.unit_scanlines) return unit_scanlines < o.unit_scanlines;
         if (dp_max != o.dp_max) return dp_max < o.dp_max;
         if (census64 != o.census64) return census64 < o.census64;
         if (wide != o.wide) return wide < o.wide;
