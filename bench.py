@@ -49,6 +49,8 @@ def workload(rank: int, name: str = "mixed"):
         return [(1242, 375, 128, 1_000_003 * (rank + 1) + i) for i in range(2)]
     if name == "profile-mix":  # 32 pairs of 320x240, D cycling 64/128/192: 5 GB of slabs
         return [(320, 240, DISPARITIES[i % 3], 1_000_003 * (rank + 1) + i) for i in range(32)]
+    if name == "profile-wide":  # 8 pairs of 1280x720, D=64: few border (x < D) pixels
+        return [(1280, 720, 64, 1_000_003 * (rank + 1) + i) for i in range(8)]
     rng = np.random.default_rng(20261203 + 7919 * rank)
     items = []
     for i in range(NUM_PAIRS):
@@ -308,7 +310,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile", "profile-mix"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile", "profile-mix", "profile-wide"])
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served measurement (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=300)
@@ -382,7 +384,7 @@ def main():
         sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
 
     # ---- autotune the aggregation launch shape on this batch, then graph it ----
-    tuned_wg, tuned_ms = sgm.autotune_batch(ctx, tl, tr, of, cfgs, oi, iterations=1)
+    tuned_wg, tuned_ms, tuned_unit = sgm.autotune_batch(ctx, tl, tr, of, cfgs, oi, iterations=1)
     sgm.set_graph_cache(2)
 
     # ---- device-resident batched steps (headline value) ----
@@ -413,6 +415,7 @@ def main():
                               "workload": args.workload, "stages_ms": {
                                   "census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
                               "autotuned_warpgroups": tuned_wg, "autotune_aggregate_ms": tuned_ms,
+                              "autotuned_unit_scanlines": tuned_unit,
                               "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
@@ -524,7 +527,9 @@ def main():
                               "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / peak},
         "gpu_launches": launches,
         "batching": {"persistent_aggregation_launch": True, "cuda_graph_per_bucket": True,
-                     "autotuned_warpgroups_per_cta": tuned_wg, "autotune_aggregate_ms": tuned_ms},
+                     "autotuned_warpgroups_per_cta": tuned_wg, "autotune_aggregate_ms": tuned_ms,
+                     "autotuned_form": "scanline pairs, 64-scanline units" if tuned_unit == 64
+                                       else "single scanline, 32-scanline units"},
         "clocks": clocks.summary(),
     }
 

@@ -183,16 +183,18 @@ vx_status vx_sgm_compute_disparity_noalloc(const uint8_t* left, size_t left_pitc
 size_t vx_sgm_static_scratch_bytes(void);
 
 /* Autotuner (no reference counterpart): runs this batch once per candidate
- * launch shape of the path-aggregation kernel (warpgroups per CTA), `iterations`
- * timed runs each (CUDA events on the context's stream, one untimed run first),
- * and records the fastest for batches with the same key (aggregation form,
- * largest padded D, census word width, slab format, log2 of the queued
- * scanline units). Outputs are written like vx_sgm_compute_batch. best_* may be
- * NULL. Synchronous. */
+ * of the path-aggregation launch - both forms (32-scanline units on the
+ * single-scanline kernel, 64-scanline units on the scanline-pair kernel) and
+ * every warpgroups-per-CTA shape of each - `iterations` timed runs each (CUDA
+ * events on the context's stream, one untimed run first), and records the
+ * fastest for batches with the same key (largest padded D, census word width,
+ * slab format, log2 of the queued 32-scanline units). Outputs are written like
+ * vx_sgm_compute_batch. best_* may be NULL. Synchronous. */
 vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
                                 const vx_image* const* right, vx_image* const* out_f32,
                                 vx_image* const* out_i16, const vx_sgm_config* cfgs,
-                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms);
+                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms,
+                                uint32_t* best_unit_scanlines);
 /* Persist / restore the autotuned table as JSON. */
 vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path);
 vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path);

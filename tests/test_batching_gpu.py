@@ -69,8 +69,8 @@ def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
     sgm = vx_sgm.SGMStereo(gpu_ctx)
     want = run_batch(gpu_ctx, sgm, pairs, cfgs)
     tl, tr, of, oi = _textures(gpu_ctx, pairs)
-    w, ms = sgm.autotune_batch(gpu_ctx, tl, tr, of, cfgs, oi, iterations=1)
-    assert w >= 1 and ms > 0
+    w, ms, unit = sgm.autotune_batch(gpu_ctx, tl, tr, of, cfgs, oi, iterations=1)
+    assert w >= 1 and ms > 0 and unit in (32, 64)
     for f, i, ww in zip(of, oi, want):
         assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="autotune run")
     sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)  # uses the tuned shape
@@ -79,7 +79,7 @@ def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
     path = os.path.join(tmp_path, "tuning.json")
     sgm.tuning_save(path)
     text = open(path).read()
-    assert f'"warpgroups": {w}' in text
+    assert f'"warpgroups": {w}' in text and f'"unit_scanlines": {unit}' in text
     other = vx_sgm.SGMStereo(gpu_ctx)
     other.tuning_load(path)
     other.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)

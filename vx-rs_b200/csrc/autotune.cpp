@@ -10,6 +10,7 @@
 // table is saved to / loaded from a small JSON file.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -23,9 +24,8 @@ TuneKey tune_key(const Plan& plan) {
     TuneKey k;
     k.dp_max = plan.dp_max;
     k.census64 = plan.census64 ? 1 : 0;
-    k.units_log2 = plan.units.empty() ? 0 : (int)std::floor(std::log2((double)plan.units.size()));
+    k.units_log2 = plan.units32 <= 0 ? 0 : (int)std::floor(std::log2((double)plan.units32));
     k.wide = plan.wide_tiles ? 1 : 0;
-    k.unit_scanlines = plan.unit_scanlines;
     return k;
 }
 
@@ -33,10 +33,26 @@ TuneKey tune_key(const Plan& plan) {
 
 using namespace vxsgm;
 
+vx_status vx_sgm::plan_batch(const std::vector<PairSpec>& specs, Plan* plan) {
+    vx_status st = build_plan(specs, plan);
+    if (st != VX_OK) return st;
+    int unit = 0;
+    {
+        std::lock_guard<std::mutex> lk(tune_mu);
+        auto it = tuned.find(tune_key(*plan));
+        if (it != tuned.end()) unit = it->second.unit_scanlines;
+    }
+    if (unit != 0 && unit != plan->unit_scanlines && !std::getenv("VX_SGM_AGG_FORM")) {
+        *plan = Plan();
+        st = build_plan(specs, plan, unit);
+    }
+    return st;
+}
+
 int vx_sgm::warpgroups_for(const Plan& plan) {
     std::lock_guard<std::mutex> lk(tune_mu);
     auto it = tuned.find(tune_key(plan));
-    return it == tuned.end() ? 0 : it->second.warpgroups;
+    return it == tuned.end() || it->second.unit_scanlines != plan.unit_scanlines ? 0 : it->second.warpgroups;
 }
 
 extern "C" {
@@ -44,57 +60,71 @@ extern "C" {
 vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
                                 const vx_image* const* right, vx_image* const* out_f32,
                                 vx_image* const* out_i16, const vx_sgm_config* cfgs,
-                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms) {
+                                uint32_t iterations, uint32_t* best_warpgroups, float* best_ms,
+                                uint32_t* best_unit_scanlines) {
     if (!sgm || !ctx || !n || !left || !right || !out_f32 || !cfgs)
         return fail(VX_ERR_INVALID_ARGUMENT, "autotune_batch: NULL argument");
     if (iterations == 0) iterations = 1;
     std::vector<PairSpec> specs(n);
     for (uint32_t i = 0; i < n; ++i)
         specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
-    Plan plan;
-    vx_status st = build_plan(specs, &plan);
-    if (st != VX_OK) return st;
     DeviceGuard g(ctx->device);
-    char* ws = nullptr;
-    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes,
-                                            ctx->pool, ctx->stream);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
-    }
-    bind_plan(plan, ws);
     cudaEvent_t ev[4] = {};
     for (auto& x : ev) cudaEventCreate(&x);
-    const int wmax = aggregate_max_warpgroups(plan.unit_scanlines, plan.dp_max, plan.census64, plan.wide_tiles);
-    int best_w = 0;
+    vx_status st = VX_OK;
+    int best_w = 0, best_unit = 0;
     float best = 0.0f;
-    for (int w = 1; w <= wmax && st == VX_OK; ++w) {
-        double total = 0.0;
-        for (uint32_t it = 0; it <= iterations && st == VX_OK; ++it) {  // first run untimed
-            st = run_plan(plan, ws, ctx->stream, ev, w);
-            if (st != VX_OK) break;
-            e = cudaEventSynchronize(ev[3]);
-            float ms = 0.0f;
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[1], ev[2]);
-            if (e != cudaSuccess) st = cuda_fail(e, "autotune timing");
-            if (it > 0) total += ms;
+    TuneKey key{};
+    // Both aggregation forms (32-scanline units on the single-scanline kernel,
+    // 64-scanline units on the scanline-pair kernel), every launch shape each.
+    for (int unit : {32, kUnitScanlines}) {
+        if (const char* f = std::getenv("VX_SGM_AGG_FORM"))
+            if ((unit == 32) != (std::strcmp(f, "single") == 0)) continue;
+        Plan plan;
+        st = build_plan(specs, &plan, unit);
+        if (st != VX_OK) break;
+        key = tune_key(plan);
+        char* ws = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool,
+                                                ctx->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
+            break;
         }
-        const float mean = (float)(total / iterations);
-        if (st == VX_OK && (best_w == 0 || mean < best)) {
-            best_w = w;
-            best = mean;
+        bind_plan(plan, ws);
+        const int wmax = aggregate_max_warpgroups(plan.unit_scanlines, plan.dp_max, plan.census64,
+                                                  plan.wide_tiles);
+        for (int w = 1; w <= wmax && st == VX_OK; ++w) {
+            double total = 0.0;
+            for (uint32_t it = 0; it <= iterations && st == VX_OK; ++it) {  // first run untimed
+                st = run_plan(plan, ws, ctx->stream, ev, w);
+                if (st != VX_OK) break;
+                e = cudaEventSynchronize(ev[3]);
+                float ms = 0.0f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[1], ev[2]);
+                if (e != cudaSuccess) st = cuda_fail(e, "autotune timing");
+                if (it > 0) total += ms;
+            }
+            const float mean = (float)(total / iterations);
+            if (st == VX_OK && (best_w == 0 || mean < best)) {
+                best_w = w;
+                best_unit = unit;
+                best = mean;
+            }
         }
+        cudaFreeAsync(ws, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
     }
-    cudaFreeAsync(ws, ctx->stream);
-    cudaStreamSynchronize(ctx->stream);
     for (auto& x : ev) cudaEventDestroy(x);
     if (st != VX_OK) return st;
     {
         std::lock_guard<std::mutex> lk(sgm->tune_mu);
-        sgm->tuned[tune_key(plan)] = {best_w, best};
+        sgm->tuned[key] = {best_unit, best_w, best};
     }
     if (best_warpgroups) *best_warpgroups = (uint32_t)best_w;
     if (best_ms) *best_ms = best;
+    if (best_unit_scanlines) *best_unit_scanlines = (uint32_t)best_unit;
     return VX_OK;
 }
 
@@ -108,7 +138,7 @@ vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path) {
     for (const auto& kv : sgm->tuned) {
         f << (first ? "" : ", ") << "{\"dp_max\": " << kv.first.dp_max
           << ", \"census64\": " << kv.first.census64 << ", \"units_log2\": " << kv.first.units_log2
-          << ", \"wide\": " << kv.first.wide << ", \"unit_scanlines\": " << kv.first.unit_scanlines
+          << ", \"wide\": " << kv.first.wide << ", \"unit_scanlines\": " << kv.second.unit_scanlines
           << ", \"warpgroups\": " << kv.second.warpgroups
           << ", \"aggregate_ms\": " << kv.second.aggregate_ms << "}";
         first = false;
@@ -145,8 +175,8 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
             field(pos, end, "aggregate_ms", &ms);
             field(pos, end, "wide", &wide);
             field(pos, end, "unit_scanlines", &us);
-            if (wg >= 1 && dp >= 8) {
-                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide, (int)us}] = {(int)wg, (float)ms};
+            if (wg >= 1 && dp >= 8 && (us == 32 || us == kUnitScanlines)) {
+                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide}] = {(int)us, (int)wg, (float)ms};
                 ++loaded;
             }
         }

@@ -70,7 +70,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
     if (!entry) {
         auto* e = new vx_sgm::GraphEntry;
         e->key = key;
-        st = build_plan(specs, &e->plan);
+        st = sgm->plan_batch(specs, &e->plan);
         if (st == VX_OK) {
             err = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&e->ws), e->plan.ws_bytes, ctx->pool,
                                           stream);

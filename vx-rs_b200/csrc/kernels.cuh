@@ -69,8 +69,10 @@ constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
 // Scanlines per aggregation work unit of the scanline-pair kernel (one warp:
 // two scanlines per lane); the single-scanline kernel takes 32.
 constexpr int kUnitScanlines = 64;
-// Fewest 64-scanline units for which a batch runs the scanline-pair kernel.
-constexpr long long kPairKernelMinUnits = 2048;
+// Fewest 64-scanline units for which a batch whose key was not autotuned runs
+// the scanline-pair kernel (on B200 the forms cross over between 6 000 and
+// 8 000 units; the autotuner times both).
+constexpr long long kPairKernelMinUnits = 7500;
 // Largest aggregation CTA (4 warpgroups); keeps registers per thread <= 128.
 constexpr int kAggMaxThreads = 512;
 // Guard words before and after every row-major census plane: the aggregation

@@ -107,7 +107,7 @@ vx_status validate_pair(const PairSpec& p) {
     return VX_OK;
 }
 
-vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines) {
     Plan& pl = *plan;
     pl = Plan{};
     const int n = (int)specs.size();
@@ -209,8 +209,15 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan) {
     // units (a single pair, small batches) run the single-scanline kernel on
     // 32-scanline units, twice the parallelism for the same work.
     long long units64 = 0;
-    for (const JobDev& j : pl.jobs) units64 += (j.num_scanlines + kUnitScanlines - 1) / kUnitScanlines;
-    pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines : 32;
+    pl.units32 = 0;
+    for (const JobDev& j : pl.jobs) {
+        units64 += (j.num_scanlines + kUnitScanlines - 1) / kUnitScanlines;
+        pl.units32 += (j.num_scanlines + 31) / 32;
+    }
+    if (unit_scanlines == kUnitScanlines || unit_scanlines == 32)
+        pl.unit_scanlines = unit_scanlines;        // the autotuned form
+    else
+        pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines : 32;
     // VX_SGM_AGG_FORM=pairs|single forces one form (both are exact; the tests run
     // every case through each).
     if (const char* f = std::getenv("VX_SGM_AGG_FORM")) {

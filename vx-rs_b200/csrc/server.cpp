@@ -262,7 +262,7 @@ void vx_sgm_server::launch(Slot& s, std::vector<Request*>& batch) {
         buf_total += buffer_bytes(r->w, r->h, r->want_i16);
     }
     Plan plan;
-    vx_status st = build_plan(specs, &plan);
+    vx_status st = sgm->plan_batch(specs, &plan);
     if (st == VX_OK) {
         s.block_bytes = buf_total + plan.ws_bytes;
         s.block_off = dev_alloc.alloc(s.block_bytes);

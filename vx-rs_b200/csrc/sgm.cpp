@@ -14,7 +14,7 @@ namespace {
 vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs,
                     cudaStream_t stream, bool synchronous, char** keep_ws, Plan* plan_out) {
     Plan plan;
-    vx_status st = build_plan(specs, &plan);
+    vx_status st = sgm->plan_batch(specs, &plan);
     if (st != VX_OK) return st;
     if (specs.empty()) return VX_OK;
     if (plan.ws_bytes > ctx->workspace_limit && specs.size() > 1 && !keep_ws) {

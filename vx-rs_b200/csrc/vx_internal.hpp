@@ -94,6 +94,7 @@ struct Plan {
     bool census64 = false;
     bool wide_tiles = false;        // some pair has wide (u16) slabs
     int unit_scanlines = 32;        // 64: scanline-pair kernel, 32: single-scanline kernel
+    long long units32 = 0;          // units the plan has at 32 scanlines (tuning key)
     int dp_max = 8;                 // largest padded disparity count
     int total_tiles = 0, total_rows = 0, max_width = 0, max_rx = 0, max_ry = 0;
     // Workspace layout (byte offsets from the workspace base).
@@ -102,7 +103,9 @@ struct Plan {
     std::vector<size_t> pair_data_off;  // per pair: census + slabs
 };
 
-vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan);
+// unit_scanlines: 32 or 64 forces the aggregation form (the autotuner's
+// choice); 0 picks it from the amount of work.
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines = 0);
 // Workspace bytes of one pair's census planes and path slabs with census words
 // of census_word_bytes (a batch uses 8-byte words for all its pairs as soon as
 // one needs them), and an upper bound of its share of the plan tables.
@@ -127,17 +130,15 @@ vx_status upload_plan(const Plan& plan, char* base, cudaStream_t stream, bool pa
 vx_status launch_plan(const Plan& plan, char* base, cudaStream_t stream, cudaEvent_t* stage_events,
                       int warpgroups, bool capturing);
 
-// Autotuning key of a batch: the aggregation launch shape depends on the
-// kernel form (unit size), the largest padded D, the census word width, the
-// tile format and the amount of queued work.
+// Autotuning key of a batch: the best aggregation form and launch shape depend
+// on the largest padded D, the census word width, the tile format and the
+// amount of queued work (log2 of its 32-scanline units).
 struct TuneKey {
     int dp_max;
     int census64;
     int units_log2;
     int wide;
-    int unit_scanlines;
     bool operator<(const TuneKey& o) const {
-        if (unit_scanlines != o.unit_scanlines) return unit_scanlines < o.unit_scanlines;
         if (dp_max != o.dp_max) return dp_max < o.dp_max;
         if (census64 != o.census64) return census64 < o.census64;
         if (wide != o.wide) return wide < o.wide;
@@ -163,11 +164,15 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
 struct vx_sgm {
     vx_ctx* ctx = nullptr;
     struct Tuned {
+        int unit_scanlines;   // aggregation form: 32 single-scanline, 64 scanline pairs
         int warpgroups;
         float aggregate_ms;
     };
     std::mutex tune_mu;
     std::map<vxsgm::TuneKey, Tuned> tuned;
+    // Plan of a batch in the autotuned form (the planner's heuristic when the
+    // batch's key was not tuned), and the tuned launch shape (0 = default).
+    vx_status plan_batch(const std::vector<vxsgm::PairSpec>& specs, vxsgm::Plan* plan);
     int warpgroups_for(const vxsgm::Plan& plan);
 
     // CUDA graphs per shape bucket (see graphs.cpp): a bucket is the list of

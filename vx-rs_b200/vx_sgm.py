@@ -131,7 +131,7 @@ _sgm_batch = _sig("vx_sgm_compute_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
 _sgm_autotune = _sig("vx_sgm_autotune_batch", ctypes.c_int, _P, _P, ctypes.c_uint32,
                      ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                      ctypes.POINTER(_CConfig), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
-                     ctypes.POINTER(ctypes.c_float))
+                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32))
 _graph_cache = _sig("vx_sgm_set_graph_cache", ctypes.c_int, _P, ctypes.c_uint32)
 _tuning_save = _sig("vx_sgm_tuning_save", ctypes.c_int, _P, ctypes.c_char_p)
 _tuning_load = _sig("vx_sgm_tuning_load", ctypes.c_int, _P, ctypes.c_char_p)
@@ -357,16 +357,18 @@ class SGMStereo:
 
     def autotune_batch(self, ctx: Context, lefts, rights, outputs, configs, outputs_i16=None,
                        iterations: int = 2):
-        """Times every aggregation launch shape on this batch and keeps the fastest
-        for batches like it. Returns (warpgroups, aggregate_ms)."""
+        """Times both aggregation forms and every launch shape on this batch and keeps
+        the fastest for batches like it. Returns (warpgroups, aggregate_ms,
+        unit_scanlines) of the winner (unit_scanlines 32: single-scanline kernel,
+        64: scanline-pair kernel)."""
         n = len(lefts)
         arr = lambda ts: (_P * n)(*[t.handle if t is not None else None for t in ts])
         cfgs = (_CConfig * n)(*[c.to_c() for c in configs])
         oi = arr(outputs_i16) if outputs_i16 is not None else None
-        w, ms = ctypes.c_uint32(), ctypes.c_float()
+        w, ms, us = ctypes.c_uint32(), ctypes.c_float(), ctypes.c_uint32()
         _check(_sgm_autotune(self._h, ctx.handle, n, arr(lefts), arr(rights), arr(outputs), oi,
-                             cfgs, iterations, ctypes.byref(w), ctypes.byref(ms)))
-        return int(w.value), float(ms.value)
+                             cfgs, iterations, ctypes.byref(w), ctypes.byref(ms), ctypes.byref(us)))
+        return int(w.value), float(ms.value), int(us.value)
 
     def set_graph_cache(self, max_buckets: int):
         """CUDA graphs per shape bucket for compute_batch / compute_disparity."""
