@@ -274,6 +274,39 @@ def run_config_table(args, local_rank):
         print(json.dumps(line), flush=True)
         del tl, tr, of, oi
 
+    # Post-filters of the depth chain (DepthFilter) on a 1920x1080 disparity map
+    # (25 % invalid = -1): per-call device time over 50 calls, and bytes moved
+    # per pixel (4 read + 4 written) against the HBM peak.
+    w, h = 1920, 1080
+    rng = np.random.default_rng(5)
+    d = (rng.random((h, w)) * 120).astype(np.float32)
+    d[rng.random((h, w)) < 0.25] = -1.0
+    tin = ctx.texture_r32float(d, w, h)
+    tout = ctx.texture_output_r32float(w, h)
+    filt = vx_sgm.DepthFilter(ctx)
+    peak = float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+        if os.path.exists(os.path.join(REPO, "MEASURED_PEAKS.json")) else 6650.0
+    for name, run in (("median r=1", lambda: filt.apply_median(ctx, tin, tout, vx_sgm.DepthMedianConfig(1),
+                                                               stream=ctx.stream)),
+                      ("median r=2", lambda: filt.apply_median(ctx, tin, tout, vx_sgm.DepthMedianConfig(2),
+                                                               stream=ctx.stream)),
+                      ("bilateral r=3", lambda: filt.apply_bilateral(ctx, tin, tout, vx_sgm.DepthFilterConfig(),
+                                                                     stream=ctx.stream))):
+        for _ in range(5):
+            run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(50):
+            run()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 50
+        gbs = 8 * w * h / (ms * 1e-3) / 1e9
+        print(json.dumps({"config": "post-filter", "filter": name, "map": f"{w}x{h} f32, 25% invalid",
+                          "ms_per_call": ms, "gpx_per_s": w * h / (ms * 1e-3) / 1e9,
+                          "hbm_gbs": gbs, "hbm_frac": gbs / peak}), flush=True)
+    filt.close()
+
 
 def run_reference(args, rank, world):
     if rank != 0:

@@ -280,6 +280,43 @@ vx_status vx_sgm_server_wait(vx_sgm_server* server, uint64_t request_id, float* 
 vx_status vx_sgm_server_cancel(vx_sgm_server* server, uint64_t request_id);
 vx_status vx_sgm_server_get_stats(vx_sgm_server* server, vx_server_stats* out);
 
+/* ---- Depth-map post-filters (vx-vision/src/kernels/depth_filter.rs) -------
+ * The step after WTA in vx-vision's depth chain. Both read an F32 image and
+ * write another F32 image of the same size (they must differ); NULL stream =
+ * the context's stream, synchronous (the reference's apply_* wait for their
+ * command buffer); otherwise asynchronous on that stream (encode_*). */
+/* DepthFilterConfig (depth_filter.rs:19-49): defaults radius 3, sigma_spatial
+ * 5.0, sigma_depth 0.05. Validated: radius 0..32, sigmas finite and > 0. */
+typedef struct vx_depth_filter_config {
+    int32_t radius;
+    float sigma_spatial;
+    float sigma_depth;
+} vx_depth_filter_config;
+/* DepthMedianConfig (depth_filter.rs:51-63): default radius 1 (3x3).
+ * Validated: radius 0..5 (the shader's window array holds 121 values). */
+typedef struct vx_depth_median_config {
+    int32_t radius;
+} vx_depth_median_config;
+void vx_depth_filter_config_default(vx_depth_filter_config* cfg);
+void vx_depth_median_config_default(vx_depth_median_config* cfg);
+typedef struct vx_depth_filter vx_depth_filter;
+/* Replaces DepthFilter::new(&ctx) (depth_filter.rs:76-100). */
+vx_status vx_depth_filter_create(vx_ctx* ctx, vx_depth_filter** out);
+void vx_depth_filter_destroy(vx_depth_filter* filter);
+/* Replaces DepthFilter::apply_median / encode_median (depth_filter.rs:140-232):
+ * per pixel, the median (upper middle for an even count) of the window's
+ * values > 0, clamped coordinates; 0 where none is valid
+ * (DepthFilter.metal:84-120). Invalid SGM pixels (value <= 0) are left out. */
+vx_status vx_depth_filter_apply_median(vx_depth_filter* filter, vx_ctx* ctx, const vx_image* in,
+                                       vx_image* out, const vx_depth_median_config* cfg,
+                                       vx_stream stream);
+/* Replaces DepthFilter::apply_bilateral / encode_bilateral (depth_filter.rs:
+ * 102-203): edge-preserving weighted mean of the valid neighbours
+ * (DepthFilter.metal:20-66); 0 where the centre is <= 0. */
+vx_status vx_depth_filter_apply_bilateral(vx_depth_filter* filter, vx_ctx* ctx, const vx_image* in,
+                                          vx_image* out, const vx_depth_filter_config* cfg,
+                                          vx_stream stream);
+
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);
 

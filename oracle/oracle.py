@@ -142,3 +142,60 @@ def reference_sgm(left, right, nd, p1=10.0, p2=120.0, rx=4, ry=3, nthreads=0):
         raise ValueError("ref_sgm_compute rejected its arguments")
     as64 = lambda c: c[..., 0].astype(np.uint64) | (c[..., 1].astype(np.uint64) << np.uint64(32))
     return as64(cl), as64(cr), S, disp
+
+
+# ---- depth-map post-filters (vx-vision/shaders/DepthFilter.metal) ----
+
+REF_DEPTH_SO = os.path.join(HERE, "_ref", "libdepth_ref.so")
+
+
+def ref_depth_available() -> bool:
+    return os.path.exists(REF_DEPTH_SO)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def depth_median(depth: np.ndarray, radius: int = 1) -> np.ndarray:
+    """Restatement of depth_median (DepthFilter.metal:84-120)."""
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.empty_like(d)
+    if lib().oracle_depth_median(_P(d.ctypes.data), _P(out.ctypes.data), w, h, int(radius)) != 0:
+        raise ValueError("oracle_depth_median rejected its arguments")
+    return out
+
+
+def depth_bilateral(depth: np.ndarray, radius: int = 3, sigma_spatial: float = 5.0,
+                    sigma_depth: float = 0.05) -> np.ndarray:
+    """Restatement of depth_bilateral (DepthFilter.metal:20-66)."""
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.empty_like(d)
+    f = lib().oracle_depth_bilateral
+    f.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float]
+    if f(_P(d.ctypes.data), _P(out.ctypes.data), w, h, int(radius), float(sigma_spatial),
+         float(sigma_depth)) != 0:
+        raise ValueError("oracle_depth_bilateral rejected its arguments")
+    return out
+
+
+def ref_depth_median(depth: np.ndarray, radius: int = 1) -> np.ndarray:
+    """The reference shader itself (tier 1, built where the reference is mounted)."""
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.empty_like(d)
+    ctypes.CDLL(REF_DEPTH_SO).ref_depth_median(_P(d.ctypes.data), _P(out.ctypes.data), w, h, int(radius))
+    return out
+
+
+def ref_depth_bilateral(depth: np.ndarray, radius: int, sigma_spatial: float,
+                        sigma_depth: float) -> np.ndarray:
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.empty_like(d)
+    f = ctypes.CDLL(REF_DEPTH_SO).ref_depth_bilateral
+    f.argtypes = [_P, _P, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, ctypes.c_float, ctypes.c_float]
+    f(_P(d.ctypes.data), _P(out.ctypes.data), w, h, int(radius), float(sigma_spatial), float(sigma_depth))
+    return out

@@ -57,6 +57,11 @@ int oracle_sgm(const uint8_t* left, size_t lpitch, const uint8_t* right, size_t 
 int oracle_wta(const uint16_t* S, int w, int h, const oracle_config* cfg, float* disparity,
                int16_t* disparity_i16, int nthreads);
 
+// Depth-map post-filters (vx-vision/shaders/DepthFilter.metal), depth_oracle.cpp.
+int oracle_depth_median(const float* in, float* out, int w, int h, int radius);
+int oracle_depth_bilateral(const float* in, float* out, int w, int h, int radius, float sigma_s,
+                           float sigma_d);
+
 #ifdef __cplusplus
 }
 #endif

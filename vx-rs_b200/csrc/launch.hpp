@@ -55,4 +55,13 @@ cudaError_t prepare_wta_kernel();
 cudaError_t launch_wta(const PairDev* d_pairs, int num_pairs, int total_rows, int max_width,
                        cudaStream_t stream);
 
+// Depth-map post-filters (depth_filter.cu) on pitched F32 planes; radius of the
+// median 0..5, of the bilateral 0..kMaxBilateralRadius.
+constexpr int kMaxMedianRadius = 5;
+constexpr int kMaxBilateralRadius = 32;
+cudaError_t launch_depth_median(const float* in, size_t in_pitch, float* out, size_t out_pitch, int W, int H,
+                                int radius, cudaStream_t stream);
+cudaError_t launch_depth_bilateral(const float* in, size_t in_pitch, float* out, size_t out_pitch, int W, int H,
+                                   int radius, float sigma_s, float sigma_d, cudaStream_t stream);
+
 }  // namespace vxsgm

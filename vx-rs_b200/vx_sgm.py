@@ -242,6 +242,12 @@ class Context:
     def texture_output_r32float(self, width: int, height: int) -> "Texture":
         return Texture.create(self, width, height, FORMAT_F32)
 
+    def texture_r32float(self, data, width: int, height: int) -> "Texture":
+        """Context::texture_r32float (an F32 image from host data)."""
+        t = Texture.create(self, width, height, FORMAT_F32)
+        t.upload(np.asarray(data, dtype=np.float32).reshape(height, width))
+        return t
+
     def texture_output_i16(self, width: int, height: int) -> "Texture":
         return Texture.create(self, width, height, FORMAT_I16)
 
@@ -396,6 +402,76 @@ class SGMStereo:
     def close(self):
         if self._h:
             _sgm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _CDepthFilterConfig(ctypes.Structure):
+    _fields_ = [("radius", ctypes.c_int32), ("sigma_spatial", ctypes.c_float),
+                ("sigma_depth", ctypes.c_float)]
+
+
+class _CDepthMedianConfig(ctypes.Structure):
+    _fields_ = [("radius", ctypes.c_int32)]
+
+
+_df_create = _sig("vx_depth_filter_create", ctypes.c_int, _P, ctypes.POINTER(_P))
+_df_destroy = _sig("vx_depth_filter_destroy", None, _P)
+_df_median = _sig("vx_depth_filter_apply_median", ctypes.c_int, _P, _P, _P, _P,
+                  ctypes.POINTER(_CDepthMedianConfig), _P)
+_df_bilateral = _sig("vx_depth_filter_apply_bilateral", ctypes.c_int, _P, _P, _P, _P,
+                     ctypes.POINTER(_CDepthFilterConfig), _P)
+
+
+class DepthFilterConfig:
+    """DepthFilterConfig (depth_filter.rs:19-49): bilateral window and sigmas."""
+
+    def __init__(self, radius: int = 3, sigma_spatial: float = 5.0, sigma_depth: float = 0.05):
+        self.radius, self.sigma_spatial, self.sigma_depth = radius, sigma_spatial, sigma_depth
+
+    @classmethod
+    def new(cls, radius: int, sigma_spatial: float, sigma_depth: float) -> "DepthFilterConfig":
+        return cls(radius, sigma_spatial, sigma_depth)
+
+
+class DepthMedianConfig:
+    """DepthMedianConfig (depth_filter.rs:51-63): radius 1 = 3x3, 2 = 5x5."""
+
+    def __init__(self, radius: int = 1):
+        self.radius = radius
+
+
+class DepthFilter:
+    """DepthFilter (depth_filter.rs): median and bilateral depth-map filters."""
+
+    def __init__(self, ctx: Context):
+        h = _P()
+        _check(_df_create(ctx.handle, ctypes.byref(h)))
+        self._h, self._ctx = h, ctx
+
+    @classmethod
+    def new(cls, ctx: Context) -> "DepthFilter":
+        return cls(ctx)
+
+    def apply_median(self, ctx: Context, input: Texture, output: Texture,
+                     config: DepthMedianConfig = None, stream=None):
+        c = _CDepthMedianConfig((config or DepthMedianConfig()).radius)
+        _check(_df_median(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c), stream))
+
+    def apply_bilateral(self, ctx: Context, input: Texture, output: Texture,
+                        config: DepthFilterConfig = None, stream=None):
+        cfg = config or DepthFilterConfig()
+        c = _CDepthFilterConfig(cfg.radius, cfg.sigma_spatial, cfg.sigma_depth)
+        _check(_df_bilateral(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c), stream))
+
+    def close(self):
+        if self._h:
+            _df_destroy(self._h)
             self._h = None
 
     def __del__(self):
