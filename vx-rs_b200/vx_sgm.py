@@ -461,13 +461,15 @@ class DepthFilter:
     def apply_median(self, ctx: Context, input: Texture, output: Texture,
                      config: DepthMedianConfig = None, stream=None):
         c = _CDepthMedianConfig((config or DepthMedianConfig()).radius)
-        _check(_df_median(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c), stream))
+        _check(_df_median(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c),
+                         _P(stream) if stream else None))
 
     def apply_bilateral(self, ctx: Context, input: Texture, output: Texture,
                         config: DepthFilterConfig = None, stream=None):
         cfg = config or DepthFilterConfig()
         c = _CDepthFilterConfig(cfg.radius, cfg.sigma_spatial, cfg.sigma_depth)
-        _check(_df_bilateral(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c), stream))
+        _check(_df_bilateral(self._h, ctx.handle, input.handle, output.handle, ctypes.byref(c),
+                         _P(stream) if stream else None))
 
     def close(self):
         if self._h:
