@@ -308,6 +308,99 @@ def run_config_table(args, local_rank):
     filt.close()
 
 
+# Sparse ORB stereo matching (StereoMatcher): the reference example's size
+# (examples/orb_stereo_benchmark.rs: <= 512 keypoints per side, EuRoC
+# intrinsics), a SLAM front end's 2048, and 16384 per side as a throughput case.
+STEREO_WORKLOADS = [
+    ("euroc-512", 512, 512, dict(fx=458.654, fy=457.296, cx=367.215, cy=248.375, baseline=0.110),
+     "512 x 512 ORB keypoints, 752x480 frame, EuRoC intrinsics (the reference example's configuration)"),
+    ("slam-2048", 2048, 2048, {}, "2048 x 2048 ORB keypoints, 752x480 frame, StereoConfig::default"),
+    ("dense-16384", 16384, 16384, {}, "16384 x 16384 ORB keypoints, 752x480 frame, StereoConfig::default"),
+]
+
+
+def run_stereo_match(args, local_rank):
+    """One JSON line per workload: keypoint pairs (n_left x n_right, the
+    reference's distance-matrix size) per second through the host-buffer entry
+    point (end to end, host copies inside), through the device-buffer entry
+    point (kernels only, CUDA events), and on the CPU (the oracle on every host
+    thread; the reference shader compiled as C++, one thread, where built)."""
+    import torch
+
+    import vx_sgm
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    torch.cuda.set_device(local_rank)
+    ctx = vx_sgm.Context(local_rank)
+    matcher = vx_sgm.StereoMatcher(ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    threads = os.cpu_count() or 1
+    dev = torch.device("cuda", local_rank)
+    for (name, nl, nr, cfgd, desc) in STEREO_WORKLOADS:
+        lk, rk, ld, rd = vx_sgm.synth_orb_stereo(nl, nr, 9000 + nl)
+        cfg = vx_sgm.StereoConfig(**cfgd)
+        pairs = nl * nr
+        # end to end: the reference's call (host slices in, Vec of matches out)
+        for _ in range(args.warmup):
+            n_match = len(matcher.run(ctx, lk, rk, ld, rd, cfg).matches)
+        lat = []
+        for _ in range(max(args.steps, 50)):
+            t0 = time.perf_counter()
+            matcher.run(ctx, lk, rk, ld, rd, cfg)
+            lat.append(time.perf_counter() - t0)
+        # device resident: the kernels alone
+        t_lk = torch.from_numpy(lk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_rk = torch.from_numpy(rk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_ld = torch.from_numpy(ld["desc"].view(np.int32).copy()).to(dev)
+        t_rd = torch.from_numpy(rd["desc"].view(np.int32).copy()).to(dev)
+        t_out = torch.empty((nl, 7), dtype=torch.int32, device=dev)
+        t_cnt = torch.empty((1,), dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+
+        def call():
+            matcher.run_device(ctx, t_lk.data_ptr(), nl, t_rk.data_ptr(), nr, t_ld.data_ptr(), t_rd.data_ptr(),
+                               cfg, t_out.data_ptr(), t_cnt.data_ptr(), stream=ctx.stream)
+        for _ in range(args.warmup):
+            call()
+        reps = max(args.steps, 200)
+        launches0 = vx_sgm.kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms = e0.elapsed_time(e1) / reps
+        launches = (vx_sgm.kernel_launch_count() - launches0) / reps
+        assert int(t_cnt.item()) == n_match
+        # CPU: the oracle on every host thread (median of 3), the reference shader on one
+        secs = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            oracle.stereo_match(lk, rk, ld["desc"], rd["desc"], dict(oracle.STEREO_DEFAULTS, **cfgd),
+                                nthreads=threads)
+            secs.append(time.perf_counter() - t0)
+        cpu = pairs / float(np.median(secs)) / 1e9
+        line = {"config": "stereo-match", "workload": name, "desc": desc, "n_left": nl, "n_right": nr,
+                "matches": n_match, "metric": "keypoint pairs/s", "unit": "G pairs/s",
+                "device": {"value": pairs / (dev_ms * 1e-3) / 1e9, "ms_per_call": dev_ms,
+                           "gpu_launches_per_call": launches},
+                "e2e": {"value": pairs / float(np.mean(lat)) / 1e9, "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+                        "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)),
+                        "h2d_bytes_per_call": 48 * (nl + nr), "d2h_bytes_per_call": 16 + 28 * nl},
+                "cpu_baseline": {"value": cpu, "unit": "G pairs/s", "cores": threads, "kind": "port",
+                                 "sample": f"the whole workload, median of 3 ({float(np.median(secs)) * 1e3:.2f} ms)"},
+                "inputs": "device-resident and L2-sized (48 B per keypoint); the kernel is issue-bound"}
+        if oracle.ref_stereo_available() and pairs <= 2048 * 2048:
+            t0 = time.perf_counter()
+            oracle.ref_stereo_match(lk, rk, ld["desc"], rd["desc"], dict(oracle.STEREO_DEFAULTS, **cfgd))
+            rs = time.perf_counter() - t0
+            line["cpu_reference"] = {"value": pairs / rs / 1e9, "unit": "G pairs/s", "cores": 1,
+                                     "kind": "reference", "sample": f"the whole workload once ({rs * 1e3:.1f} ms)"}
+        print(json.dumps(line), flush=True)
+    matcher.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -355,6 +448,9 @@ def main():
     ap.add_argument("--config-table", action="store_true",
                     help="print one JSON line per single-pair / high-resolution configuration "
                          "(plain latency, batched throughput, CPU oracle) instead of the benchmark")
+    ap.add_argument("--stereo-match", action="store_true",
+                    help="print one JSON line per sparse ORB stereo workload (device, end to end, "
+                         "CPU) instead of the benchmark")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
@@ -384,6 +480,9 @@ def main():
         return
     if args.serve_sweep:
         run_serve_sweep(args, local_rank)
+        return
+    if args.stereo_match:
+        run_stereo_match(args, local_rank)
         return
     items = workload(rank, args.workload)
     if args.pairs:

@@ -317,6 +317,78 @@ vx_status vx_depth_filter_apply_bilateral(vx_depth_filter* filter, vx_ctx* ctx, 
                                           vx_image* out, const vx_depth_filter_config* cfg,
                                           vx_stream stream);
 
+/* ---- Sparse ORB stereo matching (vx-vision/src/kernels/stereomatch.rs) -----
+ * For each left keypoint, the right keypoint with the smallest Hamming distance
+ * between their 256-bit ORB descriptors among those passing the epipolar test
+ * |yl - yr| <= max_epipolar and min_disparity <= xl - xr <= max_disparity; the
+ * first in right index order on ties (StereoMatch.metal:32-93). Accepted when
+ * the distance is <= max_hamming cast to 16 bits (StereoMatch.metal:96; the
+ * Lowe ratio test there is commented out, so ratio_thresh is carried but
+ * unused), then triangulated: Z = fx*baseline/d, X = Z*(xl-cx)/fx,
+ * Y = Z*(yl-cy)/fy in IEEE single precision, that operation order. A left
+ * keypoint with no candidate is matched to right index 0 only when max_hamming
+ * is 0xFFFF (the shader's initial best). Matches come out in ascending left
+ * index (the reference's atomic append leaves their order unspecified).
+ * Calls on one matcher must be ordered (one stream, or synchronised between):
+ * they share its scratch. */
+/* CornerPoint (vx-vision/src/types.rs:8-12): 16 bytes. */
+typedef struct vx_corner_point {
+    float position[2];
+    float response;
+    uint32_t pyramid_level;
+} vx_corner_point;
+/* ORBOutput (types.rs:36-39): 256-bit descriptor and angle, 36 bytes. */
+typedef struct vx_orb_output {
+    uint32_t desc[8];
+    float angle;
+} vx_orb_output;
+/* StereoMatchResult as the reference's host reads it (types.rs:64-70), 28 bytes;
+ * _pad is 0. */
+typedef struct vx_stereo_match_result {
+    uint32_t left_idx;
+    uint32_t right_idx;
+    float disparity;
+    float point_3d[3];
+    float _pad;
+} vx_stereo_match_result;
+/* StereoConfig (stereomatch.rs:19-69). Defaults: max_epipolar 2, min_disparity
+ * 1, max_disparity 120, max_hamming 50, ratio_thresh 0.8, fx = fy = 600,
+ * cx 320, cy 240, baseline 0.12. Every value is accepted, as the reference does. */
+typedef struct vx_stereo_config {
+    float max_epipolar;
+    float min_disparity;
+    float max_disparity;
+    uint32_t max_hamming;
+    float ratio_thresh;
+    float fx, fy, cx, cy;
+    float baseline;
+} vx_stereo_config;
+void vx_stereo_config_default(vx_stereo_config* cfg);
+typedef struct vx_stereo_matcher vx_stereo_matcher;
+/* Replaces StereoMatcher::new(&ctx) (stereomatch.rs:84-112). */
+vx_status vx_stereo_matcher_create(vx_ctx* ctx, vx_stereo_matcher** out);
+void vx_stereo_matcher_destroy(vx_stereo_matcher* matcher);
+/* Replaces StereoMatcher::run (stereomatch.rs:115-249): host arrays in, host
+ * array out, synchronous. Keypoint and descriptor counts must agree per side
+ * (the reference asserts), capacity >= n_left_kpts; at most 2^26 left and
+ * 2^23 - 1 right keypoints. *n_matches receives the number of records. */
+vx_status vx_stereo_matcher_run(vx_stereo_matcher* matcher, vx_ctx* ctx, const vx_corner_point* left_kpts,
+                                size_t n_left_kpts, const vx_corner_point* right_kpts, size_t n_right_kpts,
+                                const vx_orb_output* left_descs, size_t n_left_descs,
+                                const vx_orb_output* right_descs, size_t n_right_descs,
+                                const vx_stereo_config* cfg, vx_stereo_match_result* matches, size_t capacity,
+                                size_t* n_matches);
+/* The same on device memory, for pipelines whose keypoints and descriptors
+ * are already on the GPU (the buffers run() uploads, stereomatch.rs:144-169):
+ * descriptors as 8 words per keypoint; keypoints and descriptors 16-byte
+ * aligned; matches has room for n_left records; *match_count (device) gets
+ * their number. NULL stream = the context's stream, synchronous. */
+vx_status vx_stereo_matcher_run_device(vx_stereo_matcher* matcher, vx_ctx* ctx, const vx_corner_point* left_kpts,
+                                       uint32_t n_left, const vx_corner_point* right_kpts, uint32_t n_right,
+                                       const uint32_t* left_desc_words, const uint32_t* right_desc_words,
+                                       const vx_stereo_config* cfg, vx_stereo_match_result* matches,
+                                       uint32_t* match_count, vx_stream stream);
+
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);
 

@@ -199,3 +199,75 @@ def ref_depth_bilateral(depth: np.ndarray, radius: int, sigma_spatial: float,
     f.argtypes = [_P, _P, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, ctypes.c_float, ctypes.c_float]
     f(_P(d.ctypes.data), _P(out.ctypes.data), w, h, int(radius), float(sigma_spatial), float(sigma_depth))
     return out
+
+
+# ---- sparse ORB stereo matcher (vx-vision/shaders/StereoMatch.metal) ----
+
+REF_STEREO_SO = os.path.join(HERE, "_ref", "libstereo_ref.so")
+
+# StereoMatchResult as the host reads it (vx-vision/src/types.rs:64-70).
+MATCH_DTYPE = np.dtype([("left_idx", "<u4"), ("right_idx", "<u4"), ("disparity", "<f4"),
+                        ("point_3d", "<f4", (3,)), ("_pad", "<f4")])
+
+STEREO_DEFAULTS = dict(max_epipolar=2.0, min_disparity=1.0, max_disparity=120.0, max_hamming=50,
+                       ratio_thresh=0.8, fx=600.0, fy=600.0, cx=320.0, cy=240.0, baseline=0.12)
+
+
+class OracleStereoConfig(ctypes.Structure):
+    _fields_ = [("max_epipolar", ctypes.c_float), ("min_disparity", ctypes.c_float),
+                ("max_disparity", ctypes.c_float), ("max_hamming", ctypes.c_uint32),
+                ("ratio_thresh", ctypes.c_float), ("fx", ctypes.c_float), ("fy", ctypes.c_float),
+                ("cx", ctypes.c_float), ("cy", ctypes.c_float), ("baseline", ctypes.c_float)]
+
+
+def ref_stereo_available() -> bool:
+    return os.path.exists(REF_STEREO_SO)
+
+
+def _stereo_inputs(left_kpts, right_kpts, left_desc, right_desc):
+    lk = np.ascontiguousarray(np.asarray(left_kpts).view(np.float32).reshape(-1, 4))
+    rk = np.ascontiguousarray(np.asarray(right_kpts).view(np.float32).reshape(-1, 4))
+    ld = np.ascontiguousarray(left_desc, np.uint32).reshape(-1, 8)
+    rd = np.ascontiguousarray(right_desc, np.uint32).reshape(-1, 8)
+    if len(lk) != len(ld) or len(rk) != len(rd):
+        raise ValueError("keypoint and descriptor counts differ")
+    return lk, rk, ld, rd
+
+
+def _stereo_cfg(cfg):
+    c = dict(STEREO_DEFAULTS)
+    c.update(cfg or {})
+    return c
+
+
+def stereo_match(left_kpts, right_kpts, left_desc, right_desc, cfg=None, nthreads=0) -> np.ndarray:
+    """Restatement of StereoMatcher::run (stereomatch.rs:115-249): the matches in
+    ascending left index. kpts: (n, 4) float32 rows (x, y, response, level bits)
+    or CornerPoint records; desc: (n, 8) uint32 words."""
+    lk, rk, ld, rd = _stereo_inputs(left_kpts, right_kpts, left_desc, right_desc)
+    c = _stereo_cfg(cfg)
+    oc = OracleStereoConfig(**{k: c[k] for k, _ in OracleStereoConfig._fields_})
+    out = np.zeros(max(len(lk), 1), MATCH_DTYPE)
+    f = lib().oracle_stereo_match
+    f.argtypes = [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_int]
+    n = f(_P(lk.ctypes.data), len(lk), _P(rk.ctypes.data), len(rk), _P(ld.ctypes.data), _P(rd.ctypes.data),
+          ctypes.byref(oc), _P(out.ctypes.data), int(nthreads))
+    if n < 0:
+        raise ValueError("oracle_stereo_match rejected its arguments")
+    return out[:n].copy()
+
+
+def ref_stereo_match(left_kpts, right_kpts, left_desc, right_desc, cfg=None) -> np.ndarray:
+    """The reference shader itself (tier 1, built where the reference is mounted):
+    stereo_hamming over the full distance matrix, then stereo_extract per left."""
+    lk, rk, ld, rd = _stereo_inputs(left_kpts, right_kpts, left_desc, right_desc)
+    c = _stereo_cfg(cfg)
+    out = np.zeros(max(len(lk), 1), MATCH_DTYPE)
+    f = ctypes.CDLL(REF_STEREO_SO).ref_stereo_match
+    fl = ctypes.c_float
+    f.argtypes = [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, fl, fl, fl, ctypes.c_uint32, fl, fl, fl,
+                  fl, fl, fl, _P]
+    n = f(_P(lk.ctypes.data), len(lk), _P(rk.ctypes.data), len(rk), _P(ld.ctypes.data), _P(rd.ctypes.data),
+          c["max_epipolar"], c["min_disparity"], c["max_disparity"], int(c["max_hamming"]) & 0xFFFFFFFF,
+          c["ratio_thresh"], c["fx"], c["fy"], c["cx"], c["cy"], c["baseline"], _P(out.ctypes.data))
+    return out[:n].copy()

@@ -62,6 +62,26 @@ int oracle_depth_median(const float* in, float* out, int w, int h, int radius);
 int oracle_depth_bilateral(const float* in, float* out, int w, int h, int radius, float sigma_s,
                            float sigma_d);
 
+// Sparse ORB stereo matcher (vx-vision/shaders/StereoMatch.metal), stereo_oracle.cpp.
+// StereoParams without the counts (StereoMatch.metal:17-26).
+typedef struct oracle_stereo_config {
+    float max_epipolar, min_disparity, max_disparity;
+    uint32_t max_hamming;
+    float ratio_thresh, fx, fy, cx, cy, baseline;
+} oracle_stereo_config;
+// StereoMatchResult as the host reads it (vx-vision/src/types.rs:64-70).
+typedef struct oracle_stereo_match_record {
+    uint32_t left_idx, right_idx;
+    float disparity;
+    float point_3d[3];
+    float pad;
+} oracle_stereo_match_record;
+// kpts: n x (x, y, response, level); desc: n x 8 words; out: room for n_left
+// records. Returns the number of matches (ascending left index) or -1.
+int oracle_stereo_match(const float* left_kpts, uint32_t n_left, const float* right_kpts, uint32_t n_right,
+                        const uint32_t* left_desc, const uint32_t* right_desc, const oracle_stereo_config* cfg,
+                        oracle_stereo_match_record* out, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

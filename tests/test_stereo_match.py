@@ -1,0 +1,195 @@
+"""Sparse ORB stereo matching (vx-vision StereoMatcher: stereo_hamming + stereo_extract).
+
+CPU: the oracle restatement (oracle/stereo_oracle.cpp) equals the reference
+shader's own matches (tests/golden/stereo_match_cases.npz, made by
+tests/golden/make_stereo_golden.py from shaders/StereoMatch.metal compiled as
+C++), record for record, bit for bit; host-side argument checks.
+GPU: the CUDA matcher through the C ABI (host-buffer and device-buffer entry
+points) against the same fixtures and against the oracle at sizes up to
+16384 x 16384 keypoints: integer fields and floats bit-exact (the kernels use
+IEEE round-to-nearest arithmetic in the shader's operation order), except that
+NaN equals NaN whatever its bits (0 * inf from an infinite keypoint: x86 gives
+0xffc00000, CUDA 0x7fffffff; the reference does not fix a NaN encoding)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import vx_sgm
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "stereo_match_cases.npz")
+CFG_F = ["max_epipolar", "min_disparity", "max_disparity", "ratio_thresh", "fx", "fy", "cx", "cy", "baseline"]
+
+
+def _cases():
+    z = np.load(GOLDEN)
+    out = []
+    for name in z["names"]:
+        name = str(name)
+        cfg = {k: float(v) for k, v in zip(CFG_F, z[f"{name}/cfg_f"])}
+        cfg["max_hamming"] = int(z[f"{name}/max_hamming"][0])
+        out.append((name, z[f"{name}/lk"], z[f"{name}/rk"], z[f"{name}/ld"], z[f"{name}/rd"], cfg,
+                    z[f"{name}/matches"]))
+    return out
+
+
+def _words(m):
+    return np.ascontiguousarray(m).view(np.uint32).reshape(-1, 7)
+
+
+def _same_records(got, want):
+    """Bit-equal records, a NaN field matching any NaN."""
+    a, b = _words(got), _words(want)
+    if a.shape != b.shape:
+        return False
+    fa, fb = a[:, 2:6].view(np.float32), b[:, 2:6].view(np.float32)
+    both_nan = np.isnan(fa) & np.isnan(fb)
+    return bool(np.array_equal(a[:, [0, 1, 6]], b[:, [0, 1, 6]]) and np.all((a[:, 2:6] == b[:, 2:6]) | both_nan))
+
+
+def _lib_cfg(cfg):
+    return vx_sgm.StereoConfig(**cfg)
+
+
+def test_oracle_equals_reference_fixtures():
+    cases = _cases()
+    assert len(cases) >= 20
+    for name, lk, rk, ld, rd, cfg, want in cases:
+        got = oracle.stereo_match(lk, rk, ld, rd, cfg)
+        assert np.array_equal(_words(got), want), name
+
+
+def test_fixtures_cover_the_edge_cases():
+    """The cases the kernel's semantics hinge on are present and non-trivial."""
+    by = {c[0]: c for c in _cases()}
+    assert len(by["empty_left"][6]) == 0 and len(by["empty_right"][6]) == 0
+    ffff = by["max_hamming_ffff"]
+    assert len(ffff[6]) == len(ffff[1])  # every left keypoint is matched, candidates or not
+    edge = by["hamming_edge"][6]
+    assert sorted(edge[:, 0].tolist()) == [0, 1]  # distances 49 and 50 pass, 51 does not
+    ties = by["ties"]
+    for rec in ties[6]:
+        li, ri = int(rec[0]), int(rec[1])
+        dist = lambda j: sum(bin(int(a ^ b)).count("1") for a, b in zip(ties[3][li], ties[4][j]))  # noqa: E731
+        lx, ly = ties[1][li][:2]
+        cands = [j for j in range(len(ties[2]))
+                 if abs(np.float32(ly) - ties[2][j][1]) <= 2.0 and 1.0 <= np.float32(lx) - ties[2][j][0] <= 120.0]
+        best = min(dist(j) for j in cands)
+        assert ri == min(j for j in cands if dist(j) == best)  # first minimum in right index order
+    assert len(by["negative_epipolar"][6]) == 0 and len(by["empty_range"][6]) == 0
+
+
+def test_tier1_equals_oracle_on_fresh_cases():
+    if not oracle.ref_stereo_available():
+        pytest.skip("the reference shader is not built here (reference sources not mounted)")
+    for seed in range(3):
+        lk, rk, ld, rd = vx_sgm.synth_orb_stereo(400 + 37 * seed, 350 + 51 * seed, 100 + seed)
+        cfg = dict(max_hamming=40 + 20 * seed, max_epipolar=1.0 + seed)
+        a = oracle.stereo_match(lk, rk, ld["desc"], rd["desc"], cfg)
+        b = oracle.ref_stereo_match(lk, rk, ld["desc"], rd["desc"], cfg)
+        assert np.array_equal(_words(a), _words(b))
+
+
+def test_synthetic_keypoints_are_seeded():
+    a = vx_sgm.synth_orb_stereo(300, 280, 5)
+    b = vx_sgm.synth_orb_stereo(300, 280, 5)
+    for x, y in zip(a, b):
+        assert x.tobytes() == y.tobytes()
+    lk, rk, ld, rd = a
+    assert lk.dtype.itemsize == 16 and ld.dtype.itemsize == 36 and vx_sgm.STEREO_MATCH_RESULT.itemsize == 28
+
+
+def test_config_defaults_match_reference():
+    """StereoConfig::default (stereomatch.rs:54-69)."""
+    c = vx_sgm.StereoConfig()
+    assert (c.max_epipolar, c.min_disparity, c.max_disparity, c.max_hamming, c.ratio_thresh) == (
+        2.0, 1.0, 120.0, 50, pytest.approx(0.8))
+    assert (c.fx, c.fy, c.cx, c.cy, c.baseline) == (600.0, 600.0, 320.0, 240.0, pytest.approx(0.12))
+
+
+# ---------------------------------------------------------------------------- GPU
+
+
+@pytest.fixture(scope="module")
+def matcher(gpu_ctx):
+    m = vx_sgm.StereoMatcher(gpu_ctx)
+    yield m
+    m.close()
+
+
+@pytest.mark.gpu
+def test_gpu_equals_reference_fixtures(gpu_ctx, matcher):
+    for name, lk, rk, ld, rd, cfg, want in _cases():
+        got = matcher.run(gpu_ctx, lk, rk, ld, rd, _lib_cfg(cfg)).matches
+        assert _same_records(got, want), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_left,n_right,seed", [(1, 700, 1), (257, 255, 2), (2048, 2048, 3), (5000, 300, 4),
+                                                 (300, 9000, 5), (16384, 16384, 6)])
+def test_gpu_equals_oracle(gpu_ctx, matcher, n_left, n_right, seed):
+    """Single-chunk (few right keypoints) and multi-chunk launches (the keys of a
+    tile meet by atomicMin), partial tiles, one left keypoint, 16384 x 16384."""
+    lk, rk, ld, rd = vx_sgm.synth_orb_stereo(n_left, n_right, seed)
+    cfg = dict(max_hamming=60)
+    want = oracle.stereo_match(lk, rk, ld["desc"], rd["desc"], cfg)
+    got = matcher.run(gpu_ctx, lk, rk, ld, rd, _lib_cfg(cfg)).matches
+    assert len(got) == len(want) and len(want) > 0
+    assert _same_records(got, want)
+
+
+@pytest.mark.gpu
+def test_gpu_device_entry_point_and_scratch_reuse(gpu_ctx, matcher):
+    """The device-buffer entry point on torch memory, on the context's stream,
+    several calls in a row with growing and shrinking sizes and both launch
+    shapes: the scratch the kernels restore between calls stays valid."""
+    import torch
+    dev = torch.device("cuda", 0)
+    for i, (nl, nr) in enumerate([(3000, 4000), (100, 200), (6000, 6000), (3000, 4000), (10, 10)]):
+        lk, rk, ld, rd = vx_sgm.synth_orb_stereo(nl, nr, 40 + i)
+        cfg = vx_sgm.StereoConfig(max_hamming=55, max_epipolar=1.5)
+        want = oracle.stereo_match(lk, rk, ld["desc"], rd["desc"], dict(max_hamming=55, max_epipolar=1.5))
+        t_lk = torch.from_numpy(lk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_rk = torch.from_numpy(rk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_ld = torch.from_numpy(ld["desc"].view(np.int32).copy()).to(dev)
+        t_rd = torch.from_numpy(rd["desc"].view(np.int32).copy()).to(dev)
+        t_out = torch.full((nl, 7), -1, dtype=torch.int32, device=dev)
+        t_cnt = torch.full((1,), -1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()  # inputs and output fills (torch's stream) land before the call
+        stream = torch.cuda.ExternalStream(gpu_ctx.stream)
+        with torch.cuda.stream(stream):
+            matcher.run_device(gpu_ctx, t_lk.data_ptr(), nl, t_rk.data_ptr(), nr, t_ld.data_ptr(),
+                               t_rd.data_ptr(), cfg, t_out.data_ptr(), t_cnt.data_ptr(), stream=gpu_ctx.stream)
+        stream.synchronize()
+        n = int(t_cnt.item())
+        assert n == len(want)
+        got = t_out[:n].cpu().numpy().view(np.uint32)
+        assert _same_records(got, want), (nl, nr)
+
+
+@pytest.mark.gpu
+def test_gpu_is_deterministic(gpu_ctx, matcher):
+    lk, rk, ld, rd = vx_sgm.synth_orb_stereo(4096, 4096, 77, height=16)  # many candidates and ties
+    cfg = vx_sgm.StereoConfig(max_hamming=128)
+    a = matcher.run(gpu_ctx, lk, rk, ld, rd, cfg).matches
+    for _ in range(3):
+        assert a.tobytes() == matcher.run(gpu_ctx, lk, rk, ld, rd, cfg).matches.tobytes()
+    want = oracle.stereo_match(lk, rk, ld["desc"], rd["desc"], dict(max_hamming=128))
+    assert _same_records(a, want)
+
+
+@pytest.mark.gpu
+def test_gpu_argument_checks(gpu_ctx, matcher):
+    lk, rk, ld, rd = vx_sgm.synth_orb_stereo(10, 10, 1)
+    with pytest.raises(vx_sgm.VxError, match="left_kpts and left_descs length mismatch"):
+        matcher.run(gpu_ctx, lk, rk, ld[:9], rd)
+    with pytest.raises(vx_sgm.VxError, match="right_kpts and right_descs length mismatch"):
+        matcher.run(gpu_ctx, lk, rk[:9], ld, rd)
+    assert len(matcher.run(gpu_ctx, lk[:0], rk, ld[:0], rd).matches) == 0
+    import torch
+    buf = torch.zeros(1024, dtype=torch.int32, device="cuda:0")
+    p = buf.data_ptr()
+    with pytest.raises(vx_sgm.VxError, match="16-byte aligned"):
+        matcher.run_device(gpu_ctx, p + 4, 4, p + 256, 4, p + 512, p + 768, vx_sgm.StereoConfig(), p + 1024,
+                           p + 2000, stream=None)

@@ -64,4 +64,35 @@ cudaError_t launch_depth_median(const float* in, size_t in_pitch, float* out, si
 cudaError_t launch_depth_bilateral(const float* in, size_t in_pitch, float* out, size_t out_pitch, int W, int H,
                                    int radius, float sigma_s, float sigma_d, cudaStream_t stream);
 
+// Sparse ORB stereo matching (stereo_match.cu). Keypoints are CornerPoint
+// records read as float4 (x, y, response, level bits); descriptors are 8 words
+// per keypoint read as two uint4; both 16-byte aligned. n_right < 2^23.
+constexpr uint32_t kStereoMaxRight = (1u << 23) - 1u;
+constexpr uint32_t kStereoMaxLeft = 1u << 26;
+struct StereoMatchParams {
+    uint32_t n_left, n_right;
+    float max_epipolar, min_disparity, max_disparity;
+    uint32_t max_hamming;  // already cast to 16 bits
+    float fx, fy, cx, cy, baseline;
+    uint32_t splits, chunk;  // set by launch_stereo_match from the shape
+};
+// StereoMatchResult as the host reads it (vx-vision/src/types.rs:64-70).
+struct StereoMatchRecord {
+    uint32_t left_idx, right_idx;
+    float disparity;
+    float point_3d[3];
+    float pad;
+};
+struct StereoMatchShape {
+    uint32_t left_tiles = 0, emit_ctas = 0, splits = 1, chunk = 0;
+};
+StereoMatchShape stereo_match_shape(uint32_t n_left, uint32_t n_right, int sm_count);
+// Scratch: keys (n_left words, all 0xFFFFFFFF between calls), arrivals
+// (left_tiles words, all 0 between calls), tile_counts (left_tiles words).
+// Both invariants are restored by the launch itself.
+cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                const uint4* right_desc, uint32_t* keys, uint32_t* arrivals, uint32_t* tile_counts,
+                                StereoMatchRecord* out, uint32_t* count, StereoMatchParams p,
+                                const StereoMatchShape& shape, cudaStream_t stream);
+
 }  // namespace vxsgm

@@ -1,0 +1,231 @@
+// Sparse ORB stereo matching (vx-vision's StereoMatcher: kernels/stereomatch.rs,
+// shaders/StereoMatch.metal). For every left keypoint: the right keypoint of
+// smallest Hamming distance between 256-bit descriptors among those on the same
+// epipolar line (|yl - yr| <= max_epipolar) within the disparity range
+// (min_disparity <= xl - xr <= max_disparity), the first one in right index
+// order on ties; accepted when that distance is at most max_hamming (cast to
+// 16 bits, as the shader's ushort(params.max_hamming)); then triangulated.
+// A left keypoint without any candidate takes right index 0 at distance 0xFFFF
+// (StereoMatch.metal:79-96), which only a max_hamming of 0xFFFF accepts.
+//
+// The reference writes the n_left x n_right u16 distance matrix to memory and
+// scans each row in a second kernel. Here a row is reduced while it is produced:
+//   match_kernel  grid (left tiles of 256, right chunks). One thread per left
+//                 keypoint (descriptor in registers); the CTA stages its chunk of
+//                 right positions and descriptors in shared memory and every
+//                 thread scans it: the epipolar and disparity tests in float, the
+//                 distance (8 x LOP3 + POPC) only where both pass, and a running
+//                 minimum of key = distance << 23 | right index, whose minimum is
+//                 the first minimum in right index order. With several chunks per
+//                 tile the keys meet in global memory by atomicMin; the CTA that
+//                 arrives last at its tile (fence + arrival counter, no waiting)
+//                 decides the tile's matches and stores their count.
+//   emit_kernel   one CTA per 1024 left keypoints: the tile counts before it give
+//                 its output offset, a block scan of its accept flags the slots;
+//                 triangulation in the shader's operation order with IEEE
+//                 round-to-nearest (no fused multiply-add), then the record. It
+//                 resets the keys for the next call, the last CTA stores the count.
+// The matches come out in ascending left index (the reference appends through
+// an atomic counter, so its order is unspecified; the records are the same).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "launch.hpp"
+
+namespace vxsgm {
+
+namespace {
+
+constexpr int kTileLefts = 256;     // left keypoints (threads) per match CTA
+constexpr int kStage = 512;         // right keypoints staged in shared memory per pass
+constexpr int kEmitThreads = 1024;  // left keypoints per emit CTA
+constexpr int kRightBits = 23;
+constexpr uint32_t kRightMask = (1u << kRightBits) - 1u;
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t hamming256(const uint4& a0, const uint4& a1, const uint4& b0,
+                                               const uint4& b1) {
+    return __popc(a0.x ^ b0.x) + __popc(a0.y ^ b0.y) + __popc(a0.z ^ b0.z) + __popc(a0.w ^ b0.w) +
+           __popc(a1.x ^ b1.x) + __popc(a1.y ^ b1.y) + __popc(a1.z ^ b1.z) + __popc(a1.w ^ b1.w);
+}
+
+// Whether the match of a final key passes the distance threshold; a key that
+// saw no candidate stands for the shader's initial best = 0xFFFF
+// (StereoMatch.metal:79-96).
+__device__ __forceinline__ bool accepted(uint32_t key, uint32_t max_ham) {
+    const uint32_t dist = key == kNoKey ? 0xFFFFu : key >> kRightBits;
+    return dist <= max_ham;
+}
+
+__global__ void __launch_bounds__(kTileLefts) match_kernel(const float4* __restrict__ lk,
+                                                           const float4* __restrict__ rk,
+                                                           const uint4* __restrict__ ld,
+                                                           const uint4* __restrict__ rd, uint32_t* keys,
+                                                           uint32_t* arrivals, uint32_t* tile_counts,
+                                                           StereoMatchParams p) {
+    __shared__ float2 s_pos[kStage];
+    __shared__ uint4 s_desc[2 * kStage];
+    __shared__ int s_last;
+
+    const uint32_t tile = blockIdx.x;
+    const uint32_t li = tile * kTileLefts + threadIdx.x;
+    const bool have = li < p.n_left;
+    // A thread past the last left keypoint scans with y = NaN: no test passes.
+    float lx = 0.0f, ly = __int_as_float(0x7fc00000);
+    uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0;
+    if (have) {
+        const float4 k = lk[li];
+        lx = k.x;
+        ly = k.y;
+        a0 = ld[2 * (size_t)li];
+        a1 = ld[2 * (size_t)li + 1];
+    }
+
+    uint32_t best = kNoKey;
+    const uint32_t r_begin = blockIdx.y * p.chunk;
+    const uint32_t r_end = min(p.n_right, r_begin + p.chunk);
+    for (uint32_t base = r_begin; base < r_end; base += kStage) {
+        const uint32_t cnt = min((uint32_t)kStage, r_end - base);
+        __syncthreads();  // the previous stage has been read
+        for (uint32_t k = threadIdx.x; k < cnt; k += kTileLefts) {
+            const float4 q = rk[base + k];
+            s_pos[k] = make_float2(q.x, q.y);
+        }
+        for (uint32_t k = threadIdx.x; k < 2 * cnt; k += kTileLefts) s_desc[k] = rd[2 * (size_t)base + k];
+        __syncthreads();
+#pragma unroll 4
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const float2 q = s_pos[k];
+            const float dy = fabsf(__fsub_rn(ly, q.y));
+            const float d = __fsub_rn(lx, q.x);
+            if (dy <= p.max_epipolar && d >= p.min_disparity && d <= p.max_disparity) {
+                const uint32_t dist = hamming256(a0, a1, s_desc[2 * k], s_desc[2 * k + 1]);
+                best = min(best, (dist << kRightBits) | (base + k));
+            }
+        }
+    }
+
+    uint32_t key = best;
+    if (p.splits > 1) {
+        if (have && best != kNoKey) atomicMin(&keys[li], best);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(&arrivals[tile], 1u) == p.splits - 1;
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        if (have) key = __ldcg(&keys[li]);
+    } else if (have) {
+        keys[li] = key;
+    }
+    const int n = __syncthreads_count(have && accepted(key, p.max_hamming));
+    if (threadIdx.x == 0) {
+        tile_counts[tile] = (uint32_t)n;
+        if (p.splits > 1) arrivals[tile] = 0;  // ready for the next call
+    }
+}
+
+__global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float4* __restrict__ lk,
+                                                            const float4* __restrict__ rk, uint32_t* keys,
+                                                            const uint32_t* __restrict__ tile_counts,
+                                                            StereoMatchRecord* __restrict__ out,
+                                                            uint32_t* __restrict__ count, StereoMatchParams p) {
+    __shared__ uint32_t s_warp[kEmitThreads / 32];
+    __shared__ uint32_t s_prefix;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    // Matches of the tiles before this CTA's first tile.
+    const uint32_t first_tile = blockIdx.x * (kEmitThreads / kTileLefts);
+    uint32_t acc = 0;
+    for (uint32_t t = threadIdx.x; t < first_tile; t += kEmitThreads) acc += tile_counts[t];
+    acc = __reduce_add_sync(0xffffffffu, acc);
+    if (lane == 0) s_warp[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = s_warp[lane];
+        v = __reduce_add_sync(0xffffffffu, v);
+        if (lane == 0) s_prefix = v;
+    }
+    __syncthreads();
+    const uint32_t prefix = s_prefix;
+
+    const uint32_t li = blockIdx.x * kEmitThreads + threadIdx.x;
+    uint32_t key = kNoKey;
+    if (li < p.n_left) {
+        key = keys[li];
+        keys[li] = kNoKey;  // ready for the next call
+    }
+    const bool take = li < p.n_left && accepted(key, p.max_hamming);
+    const uint32_t ballot = __ballot_sync(0xffffffffu, take);
+    __syncthreads();  // s_warp reused
+    if (lane == 0) s_warp[warp] = __popc(ballot);
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = s_warp[lane];
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        s_warp[lane] = incl - v;
+        if (blockIdx.x == gridDim.x - 1 && lane == 31) *count = prefix + incl;
+    }
+    __syncthreads();
+    if (!take) return;
+    const uint32_t slot = prefix + s_warp[warp] + __popc(ballot & ((1u << lane) - 1u));
+    const uint32_t ri = key == kNoKey ? 0u : (key & kRightMask);
+    const float4 l = lk[li];
+    const float4 r = rk[ri];
+    // StereoMatch.metal:104-107, operation for operation.
+    const float disp = __fsub_rn(l.x, r.x);
+    const float Z = __fdiv_rn(__fmul_rn(p.fx, p.baseline), disp);
+    const float X = __fdiv_rn(__fmul_rn(Z, __fsub_rn(l.x, p.cx)), p.fx);
+    const float Y = __fdiv_rn(__fmul_rn(Z, __fsub_rn(l.y, p.cy)), p.fy);
+    StereoMatchRecord& o = out[slot];
+    o.left_idx = li;
+    o.right_idx = ri;
+    o.disparity = disp;
+    o.point_3d[0] = X;
+    o.point_3d[1] = Y;
+    o.point_3d[2] = Z;
+    o.pad = 0.0f;
+}
+
+}  // namespace
+
+StereoMatchShape stereo_match_shape(uint32_t n_left, uint32_t n_right, int sm_count) {
+    StereoMatchShape s;
+    s.left_tiles = (n_left + kTileLefts - 1) / kTileLefts;
+    s.emit_ctas = (n_left + kEmitThreads - 1) / kEmitThreads;
+    // About one wave of 256-thread CTAs (8 per SM), chunks of at least 256 rights.
+    const uint64_t want = (uint64_t)sm_count * 8;
+    uint64_t splits = (want + s.left_tiles - 1) / (s.left_tiles ? s.left_tiles : 1);
+    const uint64_t max_splits = n_right / 256 > 0 ? n_right / 256 : 1;
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    s.chunk = (uint32_t)((n_right + splits - 1) / splits);
+    s.splits = (n_right + s.chunk - 1) / s.chunk;
+    return s;
+}
+
+cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                const uint4* right_desc, uint32_t* keys, uint32_t* arrivals, uint32_t* tile_counts,
+                                StereoMatchRecord* out, uint32_t* count, StereoMatchParams p,
+                                const StereoMatchShape& shape, cudaStream_t stream) {
+    p.splits = shape.splits;
+    p.chunk = shape.chunk;
+    match_kernel<<<dim3(shape.left_tiles, shape.splits), kTileLefts, 0, stream>>>(
+        left_kpts, right_kpts, left_desc, right_desc, keys, arrivals, tile_counts, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    count_launch();
+    emit_kernel<<<shape.emit_ctas, kEmitThreads, 0, stream>>>(left_kpts, right_kpts, keys, tile_counts, out,
+                                                              count, p);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) count_launch();
+    return e;
+}
+
+}  // namespace vxsgm

@@ -483,6 +483,124 @@ class DepthFilter:
             pass
 
 
+# ---------------------------------------------------------------------------
+# Sparse ORB stereo matching (vx-vision/src/kernels/stereomatch.rs)
+
+# CornerPoint (types.rs:8-12), ORBOutput (types.rs:36-39), StereoMatchResult (types.rs:64-70).
+CORNER_POINT = np.dtype([("position", "<f4", (2,)), ("response", "<f4"), ("pyramid_level", "<u4")])
+ORB_OUTPUT = np.dtype([("desc", "<u4", (8,)), ("angle", "<f4")])
+STEREO_MATCH_RESULT = np.dtype([("left_idx", "<u4"), ("right_idx", "<u4"), ("disparity", "<f4"),
+                                ("point_3d", "<f4", (3,)), ("_pad", "<f4")])
+
+
+class _CStereoConfig(ctypes.Structure):
+    _fields_ = [("max_epipolar", ctypes.c_float), ("min_disparity", ctypes.c_float),
+                ("max_disparity", ctypes.c_float), ("max_hamming", ctypes.c_uint32),
+                ("ratio_thresh", ctypes.c_float), ("fx", ctypes.c_float), ("fy", ctypes.c_float),
+                ("cx", ctypes.c_float), ("cy", ctypes.c_float), ("baseline", ctypes.c_float)]
+
+
+_sm_create = _sig("vx_stereo_matcher_create", ctypes.c_int, _P, ctypes.POINTER(_P))
+_sm_destroy = _sig("vx_stereo_matcher_destroy", None, _P)
+_sm_run = _sig("vx_stereo_matcher_run", ctypes.c_int, _P, _P, _P, ctypes.c_size_t, _P, ctypes.c_size_t,
+               _P, ctypes.c_size_t, _P, ctypes.c_size_t, ctypes.POINTER(_CStereoConfig), _P,
+               ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t))
+_sm_run_device = _sig("vx_stereo_matcher_run_device", ctypes.c_int, _P, _P, _P, ctypes.c_uint32, _P,
+                      ctypes.c_uint32, _P, _P, ctypes.POINTER(_CStereoConfig), _P, _P, _P)
+
+
+@dataclass
+class StereoConfig:
+    """StereoConfig (stereomatch.rs:19-69), with the reference's defaults."""
+    max_epipolar: float = 2.0
+    min_disparity: float = 1.0
+    max_disparity: float = 120.0
+    max_hamming: int = 50
+    ratio_thresh: float = 0.8
+    fx: float = 600.0
+    fy: float = 600.0
+    cx: float = 320.0
+    cy: float = 240.0
+    baseline: float = 0.12
+
+    def to_c(self) -> _CStereoConfig:
+        return _CStereoConfig(self.max_epipolar, self.min_disparity, self.max_disparity,
+                              int(self.max_hamming) & 0xFFFFFFFF, self.ratio_thresh, self.fx, self.fy,
+                              self.cx, self.cy, self.baseline)
+
+
+@dataclass
+class StereoResult:
+    """StereoResult (stereomatch.rs:77-82): STEREO_MATCH_RESULT records."""
+    matches: np.ndarray
+
+
+def as_corner_points(kpts) -> np.ndarray:
+    """CornerPoint records from CORNER_POINT arrays or (n, 4) float32 rows
+    (x, y, response, level bits)."""
+    a = np.asarray(kpts)
+    if a.dtype == CORNER_POINT:
+        return np.ascontiguousarray(a)
+    return np.ascontiguousarray(a, np.float32).reshape(-1, 4).view(CORNER_POINT).reshape(-1)
+
+
+def as_orb_outputs(descs) -> np.ndarray:
+    """ORBOutput records from ORB_OUTPUT arrays or (n, 8) uint32 descriptor words."""
+    a = np.asarray(descs)
+    if a.dtype == ORB_OUTPUT:
+        return np.ascontiguousarray(a)
+    w = np.ascontiguousarray(a, np.uint32).reshape(-1, 8)
+    out = np.zeros(len(w), ORB_OUTPUT)
+    out["desc"] = w
+    return out
+
+
+class StereoMatcher:
+    """StereoMatcher (stereomatch.rs:71-249): sparse ORB matching on rectified pairs."""
+
+    def __init__(self, ctx: Context):
+        h = _P()
+        _check(_sm_create(ctx.handle, ctypes.byref(h)))
+        self._h, self._ctx = h, ctx
+
+    @classmethod
+    def new(cls, ctx: Context) -> "StereoMatcher":
+        return cls(ctx)
+
+    def run(self, ctx: Context, left_kpts, right_kpts, left_descs, right_descs,
+            config: StereoConfig = None) -> StereoResult:
+        """StereoMatcher::run (stereomatch.rs:115-249): host arrays in and out, synchronous."""
+        lk, rk = as_corner_points(left_kpts), as_corner_points(right_kpts)
+        ld, rd = as_orb_outputs(left_descs), as_orb_outputs(right_descs)
+        c = (config or StereoConfig()).to_c()
+        out = np.zeros(max(len(lk), 1), STEREO_MATCH_RESULT)
+        n = ctypes.c_size_t(0)
+        _check(_sm_run(self._h, ctx.handle, _P(lk.ctypes.data), len(lk), _P(rk.ctypes.data), len(rk),
+                       _P(ld.ctypes.data), len(ld), _P(rd.ctypes.data), len(rd), ctypes.byref(c),
+                       _P(out.ctypes.data), len(out), ctypes.byref(n)))
+        return StereoResult(out[:n.value].copy())
+
+    def run_device(self, ctx: Context, left_kpts: int, n_left: int, right_kpts: int, n_right: int,
+                   left_desc_words: int, right_desc_words: int, config: StereoConfig,
+                   matches: int, match_count: int, stream: int | None = None):
+        """Device pointers in and out (vx_stereo_matcher_run_device); asynchronous on `stream`."""
+        c = config.to_c()
+        _check(_sm_run_device(self._h, ctx.handle, _P(left_kpts), n_left, _P(right_kpts), n_right,
+                              _P(left_desc_words), _P(right_desc_words), ctypes.byref(c), _P(matches),
+                              _P(match_count), _P(stream) if stream else None))
+
+    def close(self):
+        if self._h:
+            _sm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class _CServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_size_t), ("max_batch", ctypes.c_uint32),
                 ("max_inflight_batches", ctypes.c_uint32), ("host_staging_bytes", ctypes.c_size_t)]
@@ -617,3 +735,73 @@ def synth_pair(scene: int, width: int, height: int, d_lo: float, d_hi: float, se
     if r != 0:
         raise ValueError("vx_synth_pair rejected its arguments")
     return L, R, G
+
+
+def synth_orb_stereo(n_left: int, n_right: int, seed: int, width: int = 752, height: int = 480,
+                     overlap: float = 0.8, d_lo: float = 0.5, d_hi: float = 130.0):
+    """Seeded synthetic ORB keypoints of a rectified pair (EuRoC-sized frames by
+    default): returns (left CORNER_POINT, right CORNER_POINT, left ORB_OUTPUT,
+    right ORB_OUTPUT). A share `overlap` of the left keypoints reappears on the
+    right at x - d (d uniform in [d_lo, d_hi), partly outside the usual search
+    range), y + N(0, 0.8) px, with 0-60 descriptor bits flipped; the remaining
+    right keypoints are distractors, some on the same rows as a left keypoint
+    with a descriptor 40-90 bits away. Positions are whole pixels at pyramid
+    level 0 and multiples of 1.2^level above, as FAST on a pyramid gives."""
+    rng = np.random.default_rng(seed)
+
+    def positions(n):
+        level = np.where(rng.random(n) < 0.6, 0, rng.integers(1, 4, n)).astype(np.uint32)
+        scale = (1.2 ** level).astype(np.float32)
+        x = (rng.integers(0, width, n) / scale).astype(np.int64) * scale
+        y = (rng.integers(0, height, n) / scale).astype(np.int64) * scale
+        return x.astype(np.float32), y.astype(np.float32), level
+
+    def flip(desc, nbits):
+        out = desc.copy()
+        for i, k in enumerate(nbits):
+            bits = rng.choice(256, int(k), replace=False)
+            for b in bits:
+                out[i, b >> 5] ^= np.uint32(1) << np.uint32(b & 31)
+        return out
+
+    lx, ly, llev = positions(n_left)
+    ldesc = rng.integers(0, 2 ** 32, (n_left, 8), dtype=np.uint64).astype(np.uint32)
+    n_pair = min(int(round(overlap * n_left)), n_right)
+    src = rng.permutation(n_left)[:n_pair]
+    rx = np.empty(n_right, np.float32)
+    ry = np.empty(n_right, np.float32)
+    rlev = np.zeros(n_right, np.uint32)
+    rdesc = rng.integers(0, 2 ** 32, (n_right, 8), dtype=np.uint64).astype(np.uint32)
+    rx[:n_pair] = lx[src] - rng.uniform(d_lo, d_hi, n_pair).astype(np.float32)
+    ry[:n_pair] = ly[src] + rng.normal(0.0, 0.8, n_pair).astype(np.float32)
+    rlev[:n_pair] = llev[src]
+    rdesc[:n_pair] = flip(ldesc[src], rng.integers(0, 61, n_pair))
+    n_rest = n_right - n_pair
+    if n_rest > 0:
+        dx, dy, dlev = positions(n_rest)
+        near = rng.random(n_rest) < 0.5
+        if n_left > 0 and near.any():
+            k = int(near.sum())
+            anchor = rng.integers(0, n_left, k)
+            dy[near] = ly[anchor] + rng.uniform(-2.5, 2.5, k).astype(np.float32)
+            dx[near] = lx[anchor] - rng.uniform(0.0, 125.0, k).astype(np.float32)
+            rdesc[n_pair:][near] = flip(ldesc[anchor], rng.integers(40, 91, k))
+        rx[n_pair:], ry[n_pair:], rlev[n_pair:] = dx, dy, dlev
+    order = rng.permutation(n_right)
+    rx, ry, rlev, rdesc = rx[order], ry[order], rlev[order], rdesc[order]
+
+    lk = np.zeros(n_left, CORNER_POINT)
+    lk["position"] = np.stack([lx, ly], 1) if n_left else np.zeros((0, 2), np.float32)
+    lk["response"] = rng.random(n_left).astype(np.float32)
+    lk["pyramid_level"] = llev
+    rk = np.zeros(n_right, CORNER_POINT)
+    rk["position"] = np.stack([rx, ry], 1) if n_right else np.zeros((0, 2), np.float32)
+    rk["response"] = rng.random(n_right).astype(np.float32)
+    rk["pyramid_level"] = rlev
+    ld = np.zeros(n_left, ORB_OUTPUT)
+    ld["desc"] = ldesc
+    ld["angle"] = rng.uniform(-np.pi, np.pi, n_left).astype(np.float32)
+    rd = np.zeros(n_right, ORB_OUTPUT)
+    rd["desc"] = rdesc
+    rd["angle"] = rng.uniform(-np.pi, np.pi, n_right).astype(np.float32)
+    return lk, rk, ld, rd
