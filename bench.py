@@ -337,6 +337,8 @@ def run_stereo_match(args, local_rank):
     threads = os.cpu_count() or 1
     dev = torch.device("cuda", local_rank)
     for (name, nl, nr, cfgd, desc) in STEREO_WORKLOADS:
+        if args.stereo_only and name != args.stereo_only:
+            continue
         lk, rk, ld, rd = vx_sgm.synth_orb_stereo(nl, nr, 9000 + nl)
         cfg = vx_sgm.StereoConfig(**cfgd)
         pairs = nl * nr
@@ -360,19 +362,30 @@ def run_stereo_match(args, local_rank):
         def call():
             matcher.run_device(ctx, t_lk.data_ptr(), nl, t_rk.data_ptr(), nr, t_ld.data_ptr(), t_rd.data_ptr(),
                                cfg, t_out.data_ptr(), t_cnt.data_ptr(), stream=ctx.stream)
-        for _ in range(args.warmup):
-            call()
-        reps = max(args.steps, 200)
-        launches0 = vx_sgm.kernel_launch_count()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            call()
-        e1.record(stream)
-        e1.synchronize()
-        dev_ms = e0.elapsed_time(e1) / reps
-        launches = (vx_sgm.kernel_launch_count() - launches0) / reps
-        assert int(t_cnt.item()) == n_match
+
+        def time_device(form):
+            if form:
+                os.environ["VX_STEREO_FORM"] = form
+            try:
+                for _ in range(args.warmup):
+                    call()
+                reps = max(args.steps, 200)
+                launches0 = vx_sgm.kernel_launch_count()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    call()
+                e1.record(stream)
+                e1.synchronize()
+                assert int(t_cnt.item()) == n_match
+                return e0.elapsed_time(e1) / reps, (vx_sgm.kernel_launch_count() - launches0) / reps
+            finally:
+                os.environ.pop("VX_STEREO_FORM", None)
+        # the form the library picks: banded from 2^24 pairs (0 <= max_epipolar < 2^20)
+        form = "banded" if pairs >= (1 << 24) and 0.0 <= cfg.max_epipolar < 2.0 ** 20 else "brute"
+        dev_ms, launches = time_device(None)
+        other = "brute" if form == "banded" else "banded"
+        other_ms, _ = time_device(other)
         # CPU: the oracle on every host thread (median of 3), the reference shader on one
         secs = []
         for _ in range(3):
@@ -383,14 +396,16 @@ def run_stereo_match(args, local_rank):
         cpu = pairs / float(np.median(secs)) / 1e9
         line = {"config": "stereo-match", "workload": name, "desc": desc, "n_left": nl, "n_right": nr,
                 "matches": n_match, "metric": "keypoint pairs/s", "unit": "G pairs/s",
+                "form": form,
                 "device": {"value": pairs / (dev_ms * 1e-3) / 1e9, "ms_per_call": dev_ms,
                            "gpu_launches_per_call": launches},
+                f"device_{other}": {"value": pairs / (other_ms * 1e-3) / 1e9, "ms_per_call": other_ms},
                 "e2e": {"value": pairs / float(np.mean(lat)) / 1e9, "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
                         "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)),
                         "h2d_bytes_per_call": 48 * (nl + nr), "d2h_bytes_per_call": 16 + 28 * nl},
                 "cpu_baseline": {"value": cpu, "unit": "G pairs/s", "cores": threads, "kind": "port",
                                  "sample": f"the whole workload, median of 3 ({float(np.median(secs)) * 1e3:.2f} ms)"},
-                "inputs": "device-resident and L2-sized (48 B per keypoint); the kernel is issue-bound"}
+                "inputs": "device-resident and L2-sized (48 B per keypoint); the kernels are issue- or launch-bound"}
         if oracle.ref_stereo_available() and pairs <= 2048 * 2048:
             t0 = time.perf_counter()
             oracle.ref_stereo_match(lk, rk, ld["desc"], rd["desc"], dict(oracle.STEREO_DEFAULTS, **cfgd))
@@ -451,6 +466,8 @@ def main():
     ap.add_argument("--stereo-match", action="store_true",
                     help="print one JSON line per sparse ORB stereo workload (device, end to end, "
                          "CPU) instead of the benchmark")
+    ap.add_argument("--stereo-only", default="", choices=[""] + [w[0] for w in STEREO_WORKLOADS],
+                    help="with --stereo-match: run this workload only (profiler runs)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()

@@ -118,8 +118,17 @@ def matcher(gpu_ctx):
     m.close()
 
 
+@pytest.fixture(params=["brute", "banded"])
+def stereo_form(request, monkeypatch):
+    """Runs a test through each matching form: every pair tested (brute), or the
+    right keypoints bucketed by row and only the epipolar band scanned (banded;
+    it applies where 0 <= max_epipolar < 2^20, elsewhere the brute form runs)."""
+    monkeypatch.setenv("VX_STEREO_FORM", request.param)
+    return request.param
+
+
 @pytest.mark.gpu
-def test_gpu_equals_reference_fixtures(gpu_ctx, matcher):
+def test_gpu_equals_reference_fixtures(gpu_ctx, matcher, stereo_form):
     for name, lk, rk, ld, rd, cfg, want in _cases():
         got = matcher.run(gpu_ctx, lk, rk, ld, rd, _lib_cfg(cfg)).matches
         assert _same_records(got, want), name
@@ -128,7 +137,7 @@ def test_gpu_equals_reference_fixtures(gpu_ctx, matcher):
 @pytest.mark.gpu
 @pytest.mark.parametrize("n_left,n_right,seed", [(1, 700, 1), (257, 255, 2), (2048, 2048, 3), (5000, 300, 4),
                                                  (300, 9000, 5), (16384, 16384, 6)])
-def test_gpu_equals_oracle(gpu_ctx, matcher, n_left, n_right, seed):
+def test_gpu_equals_oracle(gpu_ctx, matcher, stereo_form, n_left, n_right, seed):
     """Single-chunk (few right keypoints) and multi-chunk launches (the keys of a
     tile meet by atomicMin), partial tiles, one left keypoint, 16384 x 16384."""
     lk, rk, ld, rd = vx_sgm.synth_orb_stereo(n_left, n_right, seed)
@@ -140,7 +149,7 @@ def test_gpu_equals_oracle(gpu_ctx, matcher, n_left, n_right, seed):
 
 
 @pytest.mark.gpu
-def test_gpu_device_entry_point_and_scratch_reuse(gpu_ctx, matcher):
+def test_gpu_device_entry_point_and_scratch_reuse(gpu_ctx, matcher, stereo_form):
     """The device-buffer entry point on torch memory, on the context's stream,
     several calls in a row with growing and shrinking sizes and both launch
     shapes: the scratch the kernels restore between calls stays valid."""
@@ -169,7 +178,7 @@ def test_gpu_device_entry_point_and_scratch_reuse(gpu_ctx, matcher):
 
 
 @pytest.mark.gpu
-def test_gpu_is_deterministic(gpu_ctx, matcher):
+def test_gpu_is_deterministic(gpu_ctx, matcher, stereo_form):
     lk, rk, ld, rd = vx_sgm.synth_orb_stereo(4096, 4096, 77, height=16)  # many candidates and ties
     cfg = vx_sgm.StereoConfig(max_hamming=128)
     a = matcher.run(gpu_ctx, lk, rk, ld, rd, cfg).matches
@@ -193,3 +202,87 @@ def test_gpu_argument_checks(gpu_ctx, matcher):
     with pytest.raises(vx_sgm.VxError, match="16-byte aligned"):
         matcher.run_device(gpu_ctx, p + 4, 4, p + 256, 4, p + 512, p + 768, vx_sgm.StereoConfig(), p + 1024,
                            p + 2000, stream=None)
+
+
+ROW_BUCKETS = 8192
+
+
+def _band_covers(ly, ry, e):
+    """The banded kernel's choice for left y `ly` and right y `ry` (float32
+    arrays), emulated in float32: True where ry lies in the rows the left
+    keypoint scans or in the special bucket it always scans."""
+    f = np.float32
+    special = ~((ry >= f(0)) & (ry < f(ROW_BUCKETS)))
+    bucket = np.where(special, 0, np.floor(np.where(special, 0, ry))).astype(np.int64)
+    in_range = np.abs(ly) < f(4194304.0)
+    with np.errstate(invalid="ignore", over="ignore"):
+        lo = np.maximum(np.floor(np.where(in_range, ly - e, 0)).astype(np.int64) - 1, 0)
+        hi = np.minimum(np.floor(np.where(in_range, ly + e, 0)).astype(np.int64) + 1, ROW_BUCKETS - 1)
+    return special | (in_range & (bucket >= lo) & (bucket <= hi))
+
+
+def test_band_bounds_cover_the_epipolar_test():
+    """Every (left, right) pair that passes |yl - yr| <= e in float32 is scanned
+    by the banded form, for 0 <= e < 2^20: random and adversarial values
+    (bucket borders, one ulp off, large and tiny magnitudes, signed zeros)."""
+    rng = np.random.default_rng(11)
+    f = np.float32
+    n = 2_000_000
+    ly = np.concatenate([rng.uniform(-50, 8300, n), rng.uniform(-5e6, 5e6, n // 4),
+                         np.round(rng.uniform(0, 8192, n // 4))]).astype(f)
+    e = np.concatenate([rng.uniform(0, 8, n), rng.uniform(0, 2 ** 20, n // 4),
+                        rng.choice([0.0, -0.0, 0.5, 1.0, 2.0, 2.5], n // 4)]).astype(f)
+    m = len(ly)
+    # right y at the edge of acceptance: ly +- e nudged by a few ulps either way
+    side = rng.choice([-1.0, 1.0], m).astype(f)
+    base = (ly + side * e).astype(f)
+    steps = rng.integers(-3, 4, m)
+    ry = base.copy()
+    for k in range(1, 4):
+        up = steps >= k
+        dn = steps <= -k
+        ry[up] = np.nextafter(ry[up], f(np.inf))
+        ry[dn] = np.nextafter(ry[dn], f(-np.inf))
+    ry[: m // 10] = np.round(ry[: m // 10])  # whole rows (pyramid level 0)
+    with np.errstate(invalid="ignore"):
+        passes = np.abs(ly - ry) <= e
+    assert passes.sum() > m // 4
+    covered = _band_covers(ly, ry, e)
+    assert np.all(covered[passes]), np.flatnonzero(passes & ~covered)[:5]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("e", [0.0, -0.0, 0.5, 2.0, 7.25, 3000.0, 2.0 ** 20 - 64, 2.0 ** 20])
+def test_gpu_banded_edge_geometry(gpu_ctx, matcher, monkeypatch, e):
+    """Keypoints on bucket borders, one ulp either side, below row 0, above the
+    last bucket, beyond 2^22, subnormal and signed-zero y, with tolerances from
+    0 to 2^20 (2^20 runs the brute form): both forms equal the oracle."""
+    rng = np.random.default_rng(int(abs(e)) + 3)
+    f = np.float32
+    n = 3000
+    ly = np.concatenate([np.round(rng.uniform(0, 8192, n // 3)), rng.uniform(-40, 8240, n // 3),
+                         rng.choice([-0.0, 0.0, 1e-40, -1e-40, 8191.999, 8192.0, 4194304.0, 4194305.0,
+                                     -3.0, 5e6, 1e30], n - 2 * (n // 3))]).astype(f)
+    ry = np.empty(n, f)
+    side = rng.choice([-1.0, 1.0], n).astype(f)
+    ry[:] = ly + side * f(min(abs(e), 50.0)) * rng.uniform(0, 1.05, n).astype(f)
+    k = rng.integers(-2, 3, n)
+    ry[k > 0] = np.nextafter(ry[k > 0], f(np.inf))
+    ry[k < 0] = np.nextafter(ry[k < 0], f(-np.inf))
+    lx = rng.uniform(100, 700, n).astype(f)
+    rx = (lx - rng.uniform(0, 100, n)).astype(f)
+    lk = np.zeros((n, 4), f)
+    lk[:, 0], lk[:, 1] = lx, ly
+    rk = np.zeros((n, 4), f)
+    order = rng.permutation(n)
+    rk[:, 0], rk[:, 1] = rx[order], ry[order]
+    ld = rng.integers(0, 2 ** 32, (n, 8), dtype=np.uint64).astype(np.uint32)
+    rd = ld[order].copy()
+    rd[:, 0] ^= rng.integers(0, 2 ** 16, n).astype(np.uint32)
+    cfg = dict(max_epipolar=e, max_hamming=200)
+    want = oracle.stereo_match(lk, rk, ld, rd, cfg)
+    assert len(want) > n // 4
+    for form in ("brute", "banded"):
+        monkeypatch.setenv("VX_STEREO_FORM", form)
+        got = matcher.run(gpu_ctx, lk, rk, ld, rd, _lib_cfg(cfg)).matches
+        assert _same_records(got, want), form

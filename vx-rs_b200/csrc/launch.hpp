@@ -95,4 +95,26 @@ cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpt
                                 StereoMatchRecord* out, uint32_t* count, StereoMatchParams p,
                                 const StereoMatchShape& shape, cudaStream_t stream);
 
+// Banded form (large sets, 0 <= max_epipolar < 2^20): right keypoints
+// counting-sorted into 1-pixel row buckets 0..kRowBuckets-1 plus one bucket
+// for every other y. hist (kRowBuckets + 1) and arrival (1) are 0 between
+// calls (restored by the launch); row_start (kRowBuckets + 2) and cursor
+// (kRowBuckets + 1) are rewritten by each call; pos/desc/idx hold n_right
+// sorted copies (desc: two uint4 per keypoint).
+constexpr int kRowBuckets = 8192;
+constexpr float kStereoBandMaxEpipolar = 1048576.0f;  // 2^20
+struct StereoBandScratch {
+    uint32_t* hist = nullptr;
+    uint32_t* arrival = nullptr;
+    uint32_t* row_start = nullptr;
+    uint32_t* cursor = nullptr;
+    float2* pos = nullptr;
+    uint4* desc = nullptr;
+    uint32_t* idx = nullptr;
+};
+cudaError_t launch_stereo_match_banded(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                       const uint4* right_desc, const StereoBandScratch& band, uint32_t* keys,
+                                       uint32_t* tile_counts, StereoMatchRecord* out, uint32_t* count,
+                                       StereoMatchParams p, int sm_count, cudaStream_t stream);
+
 }  // namespace vxsgm

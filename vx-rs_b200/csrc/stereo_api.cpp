@@ -1,4 +1,5 @@
 // StereoMatcher entry points of the vx_sgm C ABI (vx-vision/src/kernels/stereomatch.rs).
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -21,6 +22,10 @@ struct vx_stereo_matcher {
     uint32_t* scratch = nullptr;  // keys[cap_left] | arrivals[cap_tiles] | tile_counts[cap_tiles]
     size_t cap_left = 0, cap_tiles = 0;
     bool scratch_dirty = false;  // a launch failed: the invariants of keys/arrivals are unknown
+    // Banded form: bucket tables and sorted copies of cap_right right keypoints.
+    char* band = nullptr;
+    size_t band_cap_right = 0;
+    bool band_dirty = false;
     char* dev_io = nullptr;
     size_t dev_io_bytes = 0;
     char* host_io = nullptr;
@@ -58,6 +63,59 @@ vx_status ensure_scratch(vx_stereo_matcher* m, uint32_t n_left, const StereoMatc
     return VX_OK;
 }
 
+// Bucket tables: hist[kRowBuckets+1] | arrival[1] | row_start[kRowBuckets+2] | cursor[kRowBuckets+1].
+constexpr size_t kBandTableWords = 3 * (size_t)kRowBuckets + 5;
+constexpr size_t kBandTableBytes = (kBandTableWords * 4 + 255) & ~size_t(255);
+
+StereoBandScratch band_views(char* base, size_t cap_right) {
+    StereoBandScratch b;
+    uint32_t* t = reinterpret_cast<uint32_t*>(base);
+    b.hist = t;
+    b.arrival = t + kRowBuckets + 1;
+    b.row_start = b.arrival + 1;
+    b.cursor = b.row_start + kRowBuckets + 2;
+    char* p = base + kBandTableBytes;
+    b.desc = reinterpret_cast<uint4*>(p);
+    p += 32 * cap_right;
+    b.pos = reinterpret_cast<float2*>(p);
+    p += 8 * cap_right;
+    b.idx = reinterpret_cast<uint32_t*>(p);
+    return b;
+}
+
+// Grows the banded form's scratch to n_right keypoints; new or dirty tables get
+// hist and arrival cleared on `stream`.
+vx_status ensure_band(vx_stereo_matcher* m, uint32_t n_right, cudaStream_t stream) {
+    if (m->band && n_right <= m->band_cap_right && !m->band_dirty) return VX_OK;
+    if (!m->band || n_right > m->band_cap_right) {
+        const size_t cap = std::max<size_t>(n_right, m->band_cap_right * 2);
+        if (m->band) cudaFreeAsync(m->band, stream);
+        m->band = nullptr;
+        m->band_cap_right = 0;
+        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->band), kBandTableBytes + 44 * cap,
+                                                m->ctx->pool, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "stereo matcher band scratch");
+        m->band_cap_right = cap;
+    }
+    cudaError_t e = cudaMemsetAsync(m->band, 0, (kRowBuckets + 2) * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stereo matcher band scratch reset");
+    m->band_dirty = false;
+    return VX_OK;
+}
+
+// The banded form pays two more launches and a scatter of the right keypoints
+// and saves the pairs outside the epipolar band: it is used for 2^24 pairs and
+// more (VX_STEREO_FORM=brute|banded forces one, where it applies).
+bool use_banded(const vx_stereo_config* cfg, uint32_t n_left, uint32_t n_right) {
+    const float e = cfg->max_epipolar;
+    if (!(e >= 0.0f && e < kStereoBandMaxEpipolar)) return false;
+    if (const char* f = std::getenv("VX_STEREO_FORM")) {
+        if (!std::strcmp(f, "brute")) return false;
+        if (!std::strcmp(f, "banded")) return true;
+    }
+    return (uint64_t)n_left * n_right >= (1ull << 24);
+}
+
 vx_status check_config(const vx_stereo_config* cfg) {
     if (!cfg) return fail(VX_ERR_INVALID_ARGUMENT, "stereo match: NULL config");
     return VX_OK;
@@ -93,6 +151,20 @@ vx_status run_locked(vx_stereo_matcher* m, const vx_corner_point* lk, uint32_t n
     uint32_t* keys = m->scratch;
     uint32_t* arrivals = m->scratch + m->cap_left;
     uint32_t* tile_counts = arrivals + m->cap_tiles;
+    if (use_banded(cfg, n_left, n_right)) {
+        st = ensure_band(m, n_right, stream);
+        if (st != VX_OK) return st;
+        cudaError_t e = launch_stereo_match_banded(
+            reinterpret_cast<const float4*>(lk), reinterpret_cast<const float4*>(rk),
+            reinterpret_cast<const uint4*>(ld), reinterpret_cast<const uint4*>(rd), band_views(m->band, m->band_cap_right),
+            keys, tile_counts, reinterpret_cast<StereoMatchRecord*>(out), count, make_params(cfg, n_left, n_right),
+            m->ctx->sm_count, stream);
+        if (e != cudaSuccess) {
+            m->scratch_dirty = m->band_dirty = true;
+            return cuda_fail(e, "stereo match launch");
+        }
+        return VX_OK;
+    }
     cudaError_t e = launch_stereo_match(reinterpret_cast<const float4*>(lk), reinterpret_cast<const float4*>(rk),
                                         reinterpret_cast<const uint4*>(ld), reinterpret_cast<const uint4*>(rd),
                                         keys, arrivals, tile_counts, reinterpret_cast<StereoMatchRecord*>(out),
@@ -129,6 +201,7 @@ void vx_stereo_matcher_destroy(vx_stereo_matcher* m) {
     DeviceGuard g(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
     if (m->scratch) cudaFree(m->scratch);
+    if (m->band) cudaFree(m->band);
     if (m->dev_io) cudaFree(m->dev_io);
     if (m->host_io) cudaFreeHost(m->host_io);
     delete m;

@@ -29,6 +29,7 @@
 // an atomic counter, so its order is unspecified; the records are the same).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "launch.hpp"
@@ -193,6 +194,160 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float4* __rest
     o.pad = 0.0f;
 }
 
+// ---- banded form: right keypoints bucketed by image row --------------------
+//
+// Only right keypoints within max_epipolar rows of a left keypoint can pass the
+// epipolar test, so for large sets the right keypoints are counting-sorted into
+// 1-pixel row buckets (rows 0..kRowBuckets-1; everything else, NaN and
+// infinities included, into one extra "special" bucket) and each left keypoint
+// scans the rows floor(fl(y - e)) - 1 .. floor(fl(y + e)) + 1 plus the special
+// bucket. That range holds every right keypoint the exact test can accept when
+// |y| < 2^22 and 0 <= e < 2^20: then |y - yr| and y +- e stay below 2^23, where
+// single-precision rounding moves a difference by at most 0.25, so
+// fl(|y - yr|) <= e implies yr in [fl(y - e) - 0.5, fl(y + e) + 0.5]. A left
+// keypoint with |y| >= 2^22 (or NaN, infinite) scans the special bucket only,
+// which holds every right keypoint it could pass with. The host uses this form
+// only for e in [0, 2^20). Keys carry the original right index, so the minimum
+// does not depend on the bucket order (which the scatter's atomics leave open).
+
+constexpr int kBandThreads = 256;  // = kTileLefts: one tile of left keypoints per CTA
+constexpr int kCountThreads = 1024;
+
+__device__ __forceinline__ uint32_t row_bucket(float y) {
+    return (y >= 0.0f && y < (float)kRowBuckets) ? (uint32_t)y : (uint32_t)kRowBuckets;
+}
+
+// Per-CTA shared histograms merged into `hist`; the last CTA to arrive turns
+// the histogram into bucket starts (row_start[0..kRowBuckets+1], the last =
+// n_right) and scatter cursors, and leaves hist and the arrival counter at 0.
+__global__ void __launch_bounds__(kCountThreads) bucket_count_kernel(const float4* __restrict__ rk,
+                                                                     uint32_t n_right, uint32_t* hist,
+                                                                     uint32_t* arrival, uint32_t* row_start,
+                                                                     uint32_t* cursor) {
+    __shared__ uint32_t s_hist[kRowBuckets + 1];
+    __shared__ uint32_t s_warp[kCountThreads / 32];
+    __shared__ int s_last;
+    for (int b = threadIdx.x; b <= kRowBuckets; b += kCountThreads) s_hist[b] = 0;
+    __syncthreads();
+    for (uint32_t k = blockIdx.x * kCountThreads + threadIdx.x; k < n_right; k += gridDim.x * kCountThreads)
+        atomicAdd(&s_hist[row_bucket(rk[k].y)], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b <= kRowBuckets; b += kCountThreads)
+        if (s_hist[b]) atomicAdd(&hist[b], s_hist[b]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(arrival, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+
+    // Exclusive scan of the kRowBuckets + 1 counts: each thread a run of kPer.
+    constexpr int kPer = (kRowBuckets + 1 + kCountThreads - 1) / kCountThreads;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b0 = threadIdx.x * kPer;
+    uint32_t v[kPer];
+    uint32_t run = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int b = b0 + i;
+        v[i] = b <= kRowBuckets ? __ldcg(&hist[b]) : 0u;
+        run += v[i];
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = s_warp[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        s_warp[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t start = s_warp[warp] + incl - run;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int b = b0 + i;
+        if (b <= kRowBuckets) {
+            row_start[b] = start;
+            cursor[b] = start;
+            hist[b] = 0;  // ready for the next call
+        }
+        start += v[i];
+    }
+    if (threadIdx.x == kCountThreads - 1) {
+        row_start[kRowBuckets + 1] = start;
+        *arrival = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) bucket_scatter_kernel(const float4* __restrict__ rk,
+                                                             const uint4* __restrict__ rd, uint32_t n_right,
+                                                             uint32_t* cursor, float2* __restrict__ s_pos,
+                                                             uint4* __restrict__ s_desc, uint32_t* __restrict__ s_idx) {
+    const uint32_t k = blockIdx.x * 256 + threadIdx.x;
+    if (k >= n_right) return;
+    const float4 q = rk[k];
+    const uint32_t at = atomicAdd(&cursor[row_bucket(q.y)], 1u);
+    s_pos[at] = make_float2(q.x, q.y);
+    s_desc[2 * (size_t)at] = rd[2 * (size_t)k];
+    s_desc[2 * (size_t)at + 1] = rd[2 * (size_t)k + 1];
+    s_idx[at] = k;
+}
+
+__device__ __forceinline__ uint32_t scan_range(uint32_t best, uint32_t r0, uint32_t r1, float lx, float ly,
+                                               const uint4& a0, const uint4& a1, const float2* __restrict__ s_pos,
+                                               const uint4* __restrict__ s_desc, const uint32_t* __restrict__ s_idx,
+                                               float max_epipolar, float min_disparity, float max_disparity) {
+#pragma unroll 4
+    for (uint32_t k = r0; k < r1; ++k) {
+        const float2 q = s_pos[k];
+        const float dy = fabsf(__fsub_rn(ly, q.y));
+        const float d = __fsub_rn(lx, q.x);
+        if (dy <= max_epipolar && d >= min_disparity && d <= max_disparity) {
+            const uint32_t dist = hamming256(a0, a1, s_desc[2 * (size_t)k], s_desc[2 * (size_t)k + 1]);
+            best = min(best, (dist << kRightBits) | s_idx[k]);
+        }
+    }
+    return best;
+}
+
+// One thread per left keypoint, one CTA per tile of 256 (the emit kernel's
+// tiles): the keypoint's band of rows, then the special bucket.
+__global__ void __launch_bounds__(kBandThreads) match_banded_kernel(
+    const float4* __restrict__ lk, const uint4* __restrict__ ld, const uint32_t* __restrict__ row_start,
+    const float2* __restrict__ s_pos, const uint4* __restrict__ s_desc, const uint32_t* __restrict__ s_idx,
+    uint32_t* keys, uint32_t* tile_counts, StereoMatchParams p) {
+    const uint32_t li = blockIdx.x * kBandThreads + threadIdx.x;
+    const bool have = li < p.n_left;
+    uint32_t best = kNoKey;
+    if (have) {
+        const float4 l = lk[li];
+        const uint4 a0 = ld[2 * (size_t)li], a1 = ld[2 * (size_t)li + 1];
+        const float e = p.max_epipolar;  // the host guarantees 0 <= e < 2^20
+        if (fabsf(l.y) < 4194304.0f) {   // 2^22
+            const int lo = max((int)floorf(__fsub_rn(l.y, e)) - 1, 0);
+            const int hi = min((int)floorf(__fadd_rn(l.y, e)) + 1, kRowBuckets - 1);
+            if (lo <= hi)
+                best = scan_range(best, row_start[lo], row_start[hi + 1], l.x, l.y, a0, a1, s_pos, s_desc, s_idx, e,
+                                  p.min_disparity, p.max_disparity);
+        }
+        best = scan_range(best, row_start[kRowBuckets], row_start[kRowBuckets + 1], l.x, l.y, a0, a1, s_pos,
+                          s_desc, s_idx, e, p.min_disparity, p.max_disparity);
+        keys[li] = best;
+    }
+    const int n = __syncthreads_count(have && accepted(best, p.max_hamming));
+    if (threadIdx.x == 0) tile_counts[blockIdx.x] = (uint32_t)n;
+}
+
 }  // namespace
 
 StereoMatchShape stereo_match_shape(uint32_t n_left, uint32_t n_right, int sm_count) {
@@ -223,6 +378,35 @@ cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpt
     count_launch();
     emit_kernel<<<shape.emit_ctas, kEmitThreads, 0, stream>>>(left_kpts, right_kpts, keys, tile_counts, out,
                                                               count, p);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) count_launch();
+    return e;
+}
+
+cudaError_t launch_stereo_match_banded(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                       const uint4* right_desc, const StereoBandScratch& band, uint32_t* keys,
+                                       uint32_t* tile_counts, StereoMatchRecord* out, uint32_t* count,
+                                       StereoMatchParams p, int sm_count, cudaStream_t stream) {
+    const uint32_t count_ctas = std::max(1u, std::min((uint32_t)sm_count,
+                                                      (p.n_right + kCountThreads - 1) / kCountThreads));
+    bucket_count_kernel<<<count_ctas, kCountThreads, 0, stream>>>(right_kpts, p.n_right, band.hist, band.arrival,
+                                                                  band.row_start, band.cursor);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    count_launch();
+    bucket_scatter_kernel<<<(p.n_right + 255) / 256, 256, 0, stream>>>(right_kpts, right_desc, p.n_right,
+                                                                       band.cursor, band.pos, band.desc, band.idx);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    count_launch();
+    const uint32_t tiles = (p.n_left + kTileLefts - 1) / kTileLefts;
+    match_banded_kernel<<<tiles, kBandThreads, 0, stream>>>(left_kpts, left_desc, band.row_start, band.pos,
+                                                            band.desc, band.idx, keys, tile_counts, p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    count_launch();
+    emit_kernel<<<(p.n_left + kEmitThreads - 1) / kEmitThreads, kEmitThreads, 0, stream>>>(
+        left_kpts, right_kpts, keys, tile_counts, out, count, p);
     e = cudaGetLastError();
     if (e == cudaSuccess) count_launch();
     return e;
