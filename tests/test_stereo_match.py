@@ -216,8 +216,15 @@ def _band_covers(ly, ry, e):
     bucket = np.where(special, 0, np.floor(np.where(special, 0, ry))).astype(np.int64)
     in_range = np.abs(ly) < f(4194304.0)
     with np.errstate(invalid="ignore", over="ignore"):
-        lo = np.maximum(np.floor(np.where(in_range, ly - e, 0)).astype(np.int64) - 1, 0)
-        hi = np.minimum(np.floor(np.where(in_range, ly + e, 0)).astype(np.int64) + 1, ROW_BUCKETS - 1)
+        fa = np.floor(np.where(in_range, ly - e, 0)).astype(f)
+        fb = np.floor(np.where(in_range, ly + e, 0)).astype(f)
+        lo = fa.astype(np.int64) - 1
+        hi = fb.astype(np.int64) + 1
+        below = np.nextafter(fa, f(-np.inf))
+        lo += (fa >= f(1)) & ~(np.abs(ly - below) <= e)
+        hi -= ~(np.abs(ly - (fb + f(1))) <= e)
+    lo = np.maximum(lo, 0)
+    hi = np.minimum(hi, ROW_BUCKETS - 1)
     return special | (in_range & (bucket >= lo) & (bucket <= hi))
 
 

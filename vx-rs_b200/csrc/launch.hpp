@@ -88,7 +88,8 @@ struct StereoMatchShape {
 };
 StereoMatchShape stereo_match_shape(uint32_t n_left, uint32_t n_right, int sm_count);
 // Scratch: keys (n_left words, all 0xFFFFFFFF between calls), arrivals
-// (left_tiles words, all 0 between calls), tile_counts (left_tiles words).
+// (left_tiles words, all 0 between calls), tile_counts (left_tiles words; the
+// banded form's tiles are 32 left keypoints: ceil(n_left / 32) words).
 // Both invariants are restored by the launch itself.
 cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
                                 const uint4* right_desc, uint32_t* keys, uint32_t* arrivals, uint32_t* tile_counts,

@@ -45,7 +45,8 @@ vx_status ensure_scratch(vx_stereo_matcher* m, uint32_t n_left, const StereoMatc
     size_t cap_left = m->cap_left, cap_tiles = m->cap_tiles;
     if (n_left > cap_left || shape.left_tiles > cap_tiles || !m->scratch) {
         cap_left = std::max<size_t>(n_left, cap_left * 2);
-        cap_tiles = std::max<size_t>(shape.left_tiles, (cap_left + 255) / 256);
+        // Tiles of 32 left keypoints (the banded form's) or of 256 (the other's).
+        cap_tiles = std::max<size_t>(shape.left_tiles, (cap_left + 31) / 32);
         if (m->scratch) cudaFreeAsync(m->scratch, stream);
         m->scratch = nullptr;
         m->cap_left = m->cap_tiles = 0;

@@ -131,13 +131,14 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float4* __rest
                                                             const float4* __restrict__ rk, uint32_t* keys,
                                                             const uint32_t* __restrict__ tile_counts,
                                                             StereoMatchRecord* __restrict__ out,
-                                                            uint32_t* __restrict__ count, StereoMatchParams p) {
+                                                            uint32_t* __restrict__ count, StereoMatchParams p,
+                                                            uint32_t tiles_per_cta) {
     __shared__ uint32_t s_warp[kEmitThreads / 32];
     __shared__ uint32_t s_prefix;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // Matches of the tiles before this CTA's first tile.
-    const uint32_t first_tile = blockIdx.x * (kEmitThreads / kTileLefts);
+    const uint32_t first_tile = blockIdx.x * tiles_per_cta;
     uint32_t acc = 0;
     for (uint32_t t = threadIdx.x; t < first_tile; t += kEmitThreads) acc += tile_counts[t];
     acc = __reduce_add_sync(0xffffffffu, acc);
@@ -200,8 +201,8 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float4* __rest
 // epipolar test, so for large sets the right keypoints are counting-sorted into
 // 1-pixel row buckets (rows 0..kRowBuckets-1; everything else, NaN and
 // infinities included, into one extra "special" bucket) and each left keypoint
-// scans the rows floor(fl(y - e)) - 1 .. floor(fl(y + e)) + 1 plus the special
-// bucket. That range holds every right keypoint the exact test can accept when
+// scans the rows floor(fl(y - e)) - 1 .. floor(fl(y + e)) + 1 (less the outer
+// two where the test provably fails there) plus the special bucket. That range holds every right keypoint the exact test can accept when
 // |y| < 2^22 and 0 <= e < 2^20: then |y - yr| and y +- e stay below 2^23, where
 // single-precision rounding moves a difference by at most 0.25, so
 // fl(|y - yr|) <= e implies yr in [fl(y - e) - 0.5, fl(y + e) + 0.5]. A left
@@ -210,49 +211,63 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float4* __rest
 // only for e in [0, 2^20). Keys carry the original right index, so the minimum
 // does not depend on the bucket order (which the scatter's atomics leave open).
 
-constexpr int kBandThreads = 256;  // = kTileLefts: one tile of left keypoints per CTA
-constexpr int kCountThreads = 1024;
+constexpr int kBandThreads = 256;               // threads per banded CTA
+constexpr int kBandLefts = kBandThreads / 32;    // left keypoints (one warp each) per banded CTA
+static_assert(kTileLefts % kBandLefts == 0, "a banded CTA's keypoints lie in one tile");
+constexpr int kCountThreads = 256;
 
 __device__ __forceinline__ uint32_t row_bucket(float y) {
     return (y >= 0.0f && y < (float)kRowBuckets) ? (uint32_t)y : (uint32_t)kRowBuckets;
 }
 
-// Per-CTA shared histograms merged into `hist`; the last CTA to arrive turns
-// the histogram into bucket starts (row_start[0..kRowBuckets+1], the last =
-// n_right) and scatter cursors, and leaves hist and the arrival counter at 0.
+// Counts the right keypoints per row bucket in `hist` (device atomics) and
+// zeroes the tile counts the banded match accumulates into. The last CTA to
+// arrive (the pattern of a cooperative grid barrier: CTA barrier, then one
+// thread fences and takes a ticket; nothing waits) turns the counts into
+// bucket starts (row_start[0..kRowBuckets+1], the last = n_right) and scatter
+// cursors, and leaves hist and the arrival counter at 0. Its scan stages the
+// counts in shared memory so that global reads and writes stay coalesced; each
+// thread sums a run of kPer (odd) consecutive words, which no two lanes of a
+// warp read from the same bank.
 __global__ void __launch_bounds__(kCountThreads) bucket_count_kernel(const float4* __restrict__ rk,
                                                                      uint32_t n_right, uint32_t* hist,
                                                                      uint32_t* arrival, uint32_t* row_start,
-                                                                     uint32_t* cursor) {
-    __shared__ uint32_t s_hist[kRowBuckets + 1];
+                                                                     uint32_t* cursor, uint32_t* tile_counts,
+                                                                     uint32_t n_tiles) {
+    constexpr int kPer = (kRowBuckets + 1 + kCountThreads - 1) / kCountThreads;
+    static_assert(kPer % 2 == 1, "odd run length keeps the runs on distinct banks");
+    static_assert(kPer * kCountThreads > kRowBuckets + 1, "room for the total past the counts");
+    __shared__ uint32_t s_cnt[kPer * kCountThreads];
     __shared__ uint32_t s_warp[kCountThreads / 32];
     __shared__ int s_last;
-    for (int b = threadIdx.x; b <= kRowBuckets; b += kCountThreads) s_hist[b] = 0;
+    const uint32_t k = blockIdx.x * kCountThreads + threadIdx.x;
+    if (k < n_right) atomicAdd(&hist[row_bucket(rk[k].y)], 1u);
+    for (uint32_t t = k; t < n_tiles; t += gridDim.x * kCountThreads) tile_counts[t] = 0;
     __syncthreads();
-    for (uint32_t k = blockIdx.x * kCountThreads + threadIdx.x; k < n_right; k += gridDim.x * kCountThreads)
-        atomicAdd(&s_hist[row_bucket(rk[k].y)], 1u);
-    __syncthreads();
-    for (int b = threadIdx.x; b <= kRowBuckets; b += kCountThreads)
-        if (s_hist[b]) atomicAdd(&hist[b], s_hist[b]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(arrival, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(arrival, 1u) == gridDim.x - 1;
+        if (s_last) __threadfence();
+    }
     __syncthreads();
     if (!s_last) return;
-    __threadfence();
 
-    // Exclusive scan of the kRowBuckets + 1 counts: each thread a run of kPer.
-    constexpr int kPer = (kRowBuckets + 1 + kCountThreads - 1) / kCountThreads;
+    {
+        uint32_t v[kPer];  // all loads in flight before the first store
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int b = threadIdx.x + i * kCountThreads;
+            v[i] = b <= kRowBuckets ? __ldcg(&hist[b]) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) s_cnt[threadIdx.x + i * kCountThreads] = v[i];
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int b0 = threadIdx.x * kPer;
-    uint32_t v[kPer];
+    uint32_t* run_at = s_cnt + threadIdx.x * kPer;
     uint32_t run = 0;
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        const int b = b0 + i;
-        v[i] = b <= kRowBuckets ? __ldcg(&hist[b]) : 0u;
-        run += v[i];
-    }
+    for (int i = 0; i < kPer; ++i) run += run_at[i];
     uint32_t incl = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -262,31 +277,33 @@ __global__ void __launch_bounds__(kCountThreads) bucket_count_kernel(const float
     if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        const uint32_t w = s_warp[lane];
+        const uint32_t w = lane < kCountThreads / 32 ? s_warp[lane] : 0u;
         uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += t;
         }
-        s_warp[lane] = wi - w;
+        if (lane < kCountThreads / 32) s_warp[lane] = wi - w;
     }
     __syncthreads();
     uint32_t start = s_warp[warp] + incl - run;
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int b = b0 + i;
+        const uint32_t c = run_at[i];
+        run_at[i] = start;
+        start += c;
+    }
+    __syncthreads();
+    // Entry kRowBuckets + 1 (a zero past the counts) now holds the total.
+    for (int b = threadIdx.x; b <= kRowBuckets + 1; b += kCountThreads) {
+        row_start[b] = s_cnt[b];
         if (b <= kRowBuckets) {
-            row_start[b] = start;
-            cursor[b] = start;
+            cursor[b] = s_cnt[b];
             hist[b] = 0;  // ready for the next call
         }
-        start += v[i];
     }
-    if (threadIdx.x == kCountThreads - 1) {
-        row_start[kRowBuckets + 1] = start;
-        *arrival = 0;
-    }
+    if (threadIdx.x == 0) *arrival = 0;
 }
 
 __global__ void __launch_bounds__(256) bucket_scatter_kernel(const float4* __restrict__ rk,
@@ -303,30 +320,35 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const float4* __res
     s_idx[at] = k;
 }
 
-__device__ __forceinline__ uint32_t scan_range(uint32_t best, uint32_t r0, uint32_t r1, float lx, float ly,
-                                               const uint4& a0, const uint4& a1, const float2* __restrict__ s_pos,
-                                               const uint4* __restrict__ s_desc, const uint32_t* __restrict__ s_idx,
-                                               float max_epipolar, float min_disparity, float max_disparity) {
-#pragma unroll 4
-    for (uint32_t k = r0; k < r1; ++k) {
+// The lanes of a warp take every 32nd right keypoint of [r0, r1).
+__device__ __forceinline__ uint32_t scan_range(uint32_t best, uint32_t r0, uint32_t r1, uint32_t lane, float lx,
+                                               float ly, const uint4& a0, const uint4& a1,
+                                               const float2* __restrict__ s_pos, const uint4* __restrict__ s_desc,
+                                               const uint32_t* __restrict__ s_idx, float max_epipolar,
+                                               float min_disparity, float max_disparity) {
+    for (uint32_t k = r0 + lane; k < r1; k += 32) {
         const float2 q = s_pos[k];
         const float dy = fabsf(__fsub_rn(ly, q.y));
         const float d = __fsub_rn(lx, q.x);
         if (dy <= max_epipolar && d >= min_disparity && d <= max_disparity) {
-            const uint32_t dist = hamming256(a0, a1, s_desc[2 * (size_t)k], s_desc[2 * (size_t)k + 1]);
+            const uint4* b = s_desc + 2 * k;
+            const uint32_t dist = hamming256(a0, a1, b[0], b[1]);
             best = min(best, (dist << kRightBits) | s_idx[k]);
         }
     }
     return best;
 }
 
-// One thread per left keypoint, one CTA per tile of 256 (the emit kernel's
-// tiles): the keypoint's band of rows, then the special bucket.
+// One warp per left keypoint, kBandLefts keypoints per CTA: the warp scans the
+// keypoint's band of rows, then the special bucket, with coalesced reads of the
+// sorted copies, and takes the minimum over its lanes. The CTA adds its
+// matches to the count of its 256-keypoint tile (zeroed by the count kernel).
 __global__ void __launch_bounds__(kBandThreads) match_banded_kernel(
     const float4* __restrict__ lk, const uint4* __restrict__ ld, const uint32_t* __restrict__ row_start,
     const float2* __restrict__ s_pos, const uint4* __restrict__ s_desc, const uint32_t* __restrict__ s_idx,
     uint32_t* keys, uint32_t* tile_counts, StereoMatchParams p) {
-    const uint32_t li = blockIdx.x * kBandThreads + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t li = blockIdx.x * kBandLefts + (threadIdx.x >> 5);
     const bool have = li < p.n_left;
     uint32_t best = kNoKey;
     if (have) {
@@ -334,18 +356,29 @@ __global__ void __launch_bounds__(kBandThreads) match_banded_kernel(
         const uint4 a0 = ld[2 * (size_t)li], a1 = ld[2 * (size_t)li + 1];
         const float e = p.max_epipolar;  // the host guarantees 0 <= e < 2^20
         if (fabsf(l.y) < 4194304.0f) {   // 2^22
-            const int lo = max((int)floorf(__fsub_rn(l.y, e)) - 1, 0);
-            const int hi = min((int)floorf(__fadd_rn(l.y, e)) + 1, kRowBuckets - 1);
+            // Rows floor(fl(y - e)) - 1 .. floor(fl(y + e)) + 1 hold every right
+            // keypoint that can pass; the outer two are dropped when the test
+            // already fails at their inner edge (the largest float below
+            // floor(fl(y - e)), resp. floor(fl(y + e)) + 1): fl(|y - yr|) only
+            // grows as yr moves outward, so no keypoint of that row can pass.
+            const float fa = floorf(__fsub_rn(l.y, e)), fb = floorf(__fadd_rn(l.y, e));
+            int lo = (int)fa - 1, hi = (int)fb + 1;
+            if (fa >= 1.0f && !(fabsf(__fsub_rn(l.y, __int_as_float(__float_as_int(fa) - 1))) <= e)) ++lo;
+            if (!(fabsf(__fsub_rn(l.y, fb + 1.0f)) <= e)) --hi;
+            lo = max(lo, 0);
+            hi = min(hi, kRowBuckets - 1);
             if (lo <= hi)
-                best = scan_range(best, row_start[lo], row_start[hi + 1], l.x, l.y, a0, a1, s_pos, s_desc, s_idx, e,
-                                  p.min_disparity, p.max_disparity);
+                best = scan_range(best, row_start[lo], row_start[hi + 1], lane, l.x, l.y, a0, a1, s_pos, s_desc,
+                                  s_idx, e, p.min_disparity, p.max_disparity);
         }
-        best = scan_range(best, row_start[kRowBuckets], row_start[kRowBuckets + 1], l.x, l.y, a0, a1, s_pos,
+        best = scan_range(best, row_start[kRowBuckets], row_start[kRowBuckets + 1], lane, l.x, l.y, a0, a1, s_pos,
                           s_desc, s_idx, e, p.min_disparity, p.max_disparity);
-        keys[li] = best;
+        best = __reduce_min_sync(0xffffffffu, best);  // `have` is uniform across the warp
     }
-    const int n = __syncthreads_count(have && accepted(best, p.max_hamming));
-    if (threadIdx.x == 0) tile_counts[blockIdx.x] = (uint32_t)n;
+    const bool lead = have && lane == 0;
+    if (lead) keys[li] = best;
+    const int n = __syncthreads_count(lead && accepted(best, p.max_hamming));
+    if (threadIdx.x == 0 && n) atomicAdd(&tile_counts[(blockIdx.x * kBandLefts) / kTileLefts], (uint32_t)n);
 }
 
 }  // namespace
@@ -377,7 +410,7 @@ cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpt
     if (e != cudaSuccess) return e;
     count_launch();
     emit_kernel<<<shape.emit_ctas, kEmitThreads, 0, stream>>>(left_kpts, right_kpts, keys, tile_counts, out,
-                                                              count, p);
+                                                              count, p, kEmitThreads / kTileLefts);
     e = cudaGetLastError();
     if (e == cudaSuccess) count_launch();
     return e;
@@ -387,10 +420,11 @@ cudaError_t launch_stereo_match_banded(const float4* left_kpts, const float4* ri
                                        const uint4* right_desc, const StereoBandScratch& band, uint32_t* keys,
                                        uint32_t* tile_counts, StereoMatchRecord* out, uint32_t* count,
                                        StereoMatchParams p, int sm_count, cudaStream_t stream) {
-    const uint32_t count_ctas = std::max(1u, std::min((uint32_t)sm_count,
-                                                      (p.n_right + kCountThreads - 1) / kCountThreads));
+    (void)sm_count;
+    const uint32_t count_ctas = (p.n_right + kCountThreads - 1) / kCountThreads;
+    const uint32_t tiles = (p.n_left + kTileLefts - 1) / kTileLefts;
     bucket_count_kernel<<<count_ctas, kCountThreads, 0, stream>>>(right_kpts, p.n_right, band.hist, band.arrival,
-                                                                  band.row_start, band.cursor);
+                                                                  band.row_start, band.cursor, tile_counts, tiles);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     count_launch();
@@ -399,14 +433,13 @@ cudaError_t launch_stereo_match_banded(const float4* left_kpts, const float4* ri
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     count_launch();
-    const uint32_t tiles = (p.n_left + kTileLefts - 1) / kTileLefts;
-    match_banded_kernel<<<tiles, kBandThreads, 0, stream>>>(left_kpts, left_desc, band.row_start, band.pos,
+    match_banded_kernel<<<(p.n_left + kBandLefts - 1) / kBandLefts, kBandThreads, 0, stream>>>(left_kpts, left_desc, band.row_start, band.pos,
                                                             band.desc, band.idx, keys, tile_counts, p);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     count_launch();
     emit_kernel<<<(p.n_left + kEmitThreads - 1) / kEmitThreads, kEmitThreads, 0, stream>>>(
-        left_kpts, right_kpts, keys, tile_counts, out, count, p);
+        left_kpts, right_kpts, keys, tile_counts, out, count, p, kEmitThreads / kTileLefts);
     e = cudaGetLastError();
     if (e == cudaSuccess) count_launch();
     return e;
