@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 
 #include "launch.hpp"
 
@@ -47,7 +48,52 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ in, size_t 
     }
 }
 
-// Median for a compile-time radius R (window in registers, unrolled ranks).
+// Batcher's odd-even merge sorting network restricted to N inputs (a
+// comparator that would touch index >= N meets an implicit +inf and is a
+// no-op, so it is left out), as a compile-time list of index pairs.
+template <int N>
+struct SortNet {
+    int a[512] = {}, b[512] = {};
+    int n = 0;
+    constexpr SortNet() {
+        for (int p = 1; p < N; p <<= 1)
+            for (int k = p; k >= 1; k >>= 1)
+                for (int j = k % p; j + k < N; j += 2 * k)
+                    for (int i = 0; i < k; ++i)
+                        if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+                            a[n] = i + j;
+                            b[n] = i + j + k;
+                            ++n;
+                        }
+    }
+};
+template <int N>
+constexpr SortNet<N> kSortNet{};
+
+template <int A, int B, int N>
+__device__ __forceinline__ void compare_exchange(uint32_t (&v)[N]) {
+    const uint32_t x = v[A], y = v[B];
+    v[A] = min(x, y);
+    v[B] = max(x, y);
+}
+
+template <int N, int... I>
+__device__ __forceinline__ void apply_net(uint32_t (&v)[N], std::integer_sequence<int, I...>) {
+    (compare_exchange<kSortNet<N>.a[I], kSortNet<N>.b[I]>(v), ...);
+}
+
+// Sorts v ascending; every index is a template argument, so v stays in registers.
+template <int N>
+__device__ __forceinline__ void sort_network(uint32_t (&v)[N]) {
+    apply_net<N>(v, std::make_integer_sequence<int, kSortNet<N>.n>{});
+}
+
+// Median for a compile-time radius R (window in registers). The values taken
+// (> 0, +inf included) and the +inf standing in for invalid ones are positive
+// floats, whose order is that of their bit patterns: the window is sorted as
+// uint32 and the element of index count/2 is read (equal values have equal
+// bits, so this is the shader's pick). Only indices <= N/2 are read, so the
+// compiler drops the comparators that feed only the upper half.
 template <int R>
 __global__ void __launch_bounds__(kTileW * kTileH)
 median_kernel(const float* __restrict__ in, size_t in_pitch, float* __restrict__ out, size_t out_pitch, int W,
@@ -59,25 +105,22 @@ median_kernel(const float* __restrict__ in, size_t in_pitch, float* __restrict__
     __syncthreads();
     const int x = blockIdx.x * kTileW + threadIdx.x, y = blockIdx.y * kTileH + threadIdx.y;
     if (x >= W || y >= H) return;
-    float v[N];
+    constexpr uint32_t kInf = 0x7F800000u;
+    uint32_t v[N];
     int count = 0;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
         const float d = s[(threadIdx.y + i / (2 * R + 1)) * TW + threadIdx.x + i % (2 * R + 1)];
         const bool ok = d > 0.0f;
-        v[i] = ok ? d : INFINITY;
+        v[i] = ok ? __float_as_uint(d) : kInf;
         count += ok ? 1 : 0;
     }
+    sort_network<N>(v);
     const int k = count / 2;
-    float r = 0.0f;
+    uint32_t pick = v[0];
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-        int rank = 0;
-#pragma unroll
-        for (int j = 0; j < N; ++j) rank += (v[j] < v[i] || (j < i && v[j] == v[i])) ? 1 : 0;
-        if (rank == k) r = v[i];
-    }
-    if (count == 0) r = 0.0f;
+    for (int i = 1; i <= N / 2; ++i) pick = k == i ? v[i] : pick;
+    const float r = count == 0 ? 0.0f : __uint_as_float(pick);
     *reinterpret_cast<float*>(reinterpret_cast<char*>(out) + (size_t)y * out_pitch + (size_t)x * sizeof(float)) = r;
 }
 
