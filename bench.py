@@ -171,17 +171,22 @@ AGG_DRAM_BYTES_PER_PATH_PD = 31.75e9 / (8 * 3737760000)
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
 
-def served(vx_sgm, ctx, sgm, rates, num_requests):
+def served(vx_sgm, ctx, sgm, rates, num_requests, max_batch=32, slots=2):
     """Served SGM: open-loop Poisson arrivals, mixed sizes and D, 40 GB budget."""
     import loadgen
     reqs = loadgen.make_requests(48)
-    srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=32,
-                        max_inflight_batches=2)
+    srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=max_batch,
+                        max_inflight_batches=slots)
     loadgen.run_poisson(srv, reqs, 100.0, 16)  # warm the pool and the planner
     out = []
     for r in rates:
+        before = srv.stats()
         res = loadgen.run_poisson(srv, reqs, r, num_requests)
-        res["server"] = srv.stats()
+        after = srv.stats()
+        res["server"] = after
+        batches = after["batches"] - before["batches"]
+        res["mean_batch"] = (after["completed"] - before["completed"]) / batches if batches else None
+        res["max_batch"], res["slots"] = max_batch, slots
         out.append(res)
     srv.close()
     return out
@@ -192,7 +197,7 @@ def run_serve_sweep(args, local_rank):
     ctx = vx_sgm.Context(local_rank)
     sgm = vx_sgm.SGMStereo(ctx)
     rates = [float(x) for x in args.serve_sweep.split(",") if x]
-    for res in served(vx_sgm, ctx, sgm, rates, args.serve_requests):
+    for res in served(vx_sgm, ctx, sgm, rates, args.serve_requests, args.serve_max_batch, args.serve_slots):
         print(json.dumps({"metric": "served SGM", "unit": UNIT, "budget_bytes": SERVE_BUDGET,
                           "workload": "Poisson arrivals, sizes {640x480,1242x375,1280x720,1920x1080} "
                                       "x D{64,128,192}, 8 paths", **res}), flush=True)
@@ -455,6 +460,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served measurement (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-max-batch", type=int, default=32, help="server: requests per batch at most")
+    ap.add_argument("--serve-slots", type=int, default=2, help="server: batches in flight at most")
     ap.add_argument("--serve-sweep", default="",
                     help="comma-separated arrival rates: run the served sweep and print one JSON "
                          "line per rate instead of the benchmark")

@@ -261,6 +261,7 @@ typedef struct vx_server_stats {
     uint64_t max_launch_us;               /* longest host time to issue one batch */
     uint64_t max_pinned_alloc_us;         /* longest pinned allocation past the arena */
     uint64_t staging_overflows;           /* requests staged past the pinned arena */
+    uint64_t shadow_reruns;               /* requests recomputed after their escape pool ran out */
 } vx_server_stats;
 
 vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config* cfg,

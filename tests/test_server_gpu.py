@@ -38,6 +38,32 @@ def test_served_results_equal_solo(gpu_ctx, sgm):
         assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
 
 
+@pytest.mark.parametrize("pool", [None, "1"])
+def test_escape_pool_and_reruns(gpu_ctx, sgm, monkeypatch, pool):
+    """Served requests keep their escaped path vectors in a pool of 1/16 of their
+    vectors. With the default pool nothing overflows and every result equals the
+    solo (full-shadow) result; with a pool of one vector every pair with two or
+    more escapes overflows, is recomputed with a full shadow, and still equals it."""
+    if pool:
+        monkeypatch.setenv("VX_SGM_SHADOW_POOL", pool)
+    reqs = [_request(i) for i in range(10)]
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=3 * biggest, max_batch=6,
+                        max_inflight_batches=2)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    results = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    monkeypatch.delenv("VX_SGM_SHADOW_POOL", raising=False)
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    if pool:
+        assert st["shadow_reruns"] > 0
+    else:
+        assert st["shadow_reruns"] == 0
+    for (L, R, c), (d, di, _) in zip(reqs, results):
+        assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
+
+
 def test_serving_allocates_nothing_after_start(gpu_ctx, sgm):
     """The device arena and the pinned staging arena are taken at creation; serving a
     stream of mixed requests grows neither the context's pool nor the pinned memory."""

@@ -392,19 +392,40 @@ __device__ __forceinline__ void write_u16_vectors(uint32_t tstate, int G, bool w
 
 // After one pixel step: the rows of the active run go to the path's slab.
 // Byte slabs: a vector with a value of 255 or more (escape) gets the marker in
-// byte 0 of its row, and its exact u16 values are read back from TMEM to the
-// shadow slab. Wide slabs: the tile rows are the u16 vectors. pix0 = pixel of
+// byte 0 of its row and its shadow slot in bytes 4..7, and its exact u16
+// values are read back from TMEM to that slot (nothing is written when the
+// pair's shadow pool has run out). Wide slabs: the tile rows are the u16 vectors. pix0 = pixel of
 // tile row 0; pix_lo / pix_hi = this lane's two scanlines' pixels (used only for
 // an active scanline); pstride = pixel stride between tile rows (1 or W).
-__device__ __forceinline__ void finish_pixel(const PairDev& pr, int path, bool wide, int Dv, uint32_t tstate,
-                                             int G, uint32_t mx, bool act_lo, bool act_hi,
+// CP (compact): the batch has pairs whose escaped vectors go to a shadow pool;
+// their rows carry the slot, which the WTA kernel reads. Without CP every
+// escaped vector goes to its pixel's place in the full shadow (the slot the
+// WTA kernel computes for a pair without a pool), and the pixel loop has none
+// of the pool's bookkeeping.
+template <bool CP>
+__device__ __forceinline__ void finish_pixel(const PairDev& pr, const EscapeTarget& et, int path, bool wide, int Dv,
+                                             uint32_t tstate, int G, uint32_t mx, bool act_lo, bool act_hi,
                                              const unsigned char* tile, int row_bytes, unsigned char* row_lo,
                                              unsigned char* row_hi, size_t pix0, size_t pstride, size_t pix_lo,
                                              size_t pix_hi, int lane) {
     const bool esc_lo = !wide && act_lo && (mx & 0xFFFFu) >= 0xFFu;
     const bool esc_hi = !wide && act_hi && (mx >> 16) >= 0xFFu;
-    if (esc_lo) row_lo[0] = 0xFFu;
-    if (esc_hi) row_hi[0] = 0xFFu;
+    uint32_t slot_lo = kNoSlot, slot_hi = kNoSlot;
+    if constexpr (CP) {
+        if (esc_lo) {
+            slot_lo = take_slot(et, pix_lo);
+            row_lo[0] = 0xFFu;
+            *reinterpret_cast<uint32_t*>(row_lo + 4) = slot_lo;  // rows are 8-byte aligned
+        }
+        if (esc_hi) {
+            slot_hi = take_slot(et, pix_hi);
+            row_hi[0] = 0xFFu;
+            *reinterpret_cast<uint32_t*>(row_hi + 4) = slot_hi;
+        }
+    } else {
+        if (esc_lo) row_lo[0] = 0xFFu;
+        if (esc_hi) row_hi[0] = 0xFFu;
+    }
     const unsigned al = __ballot_sync(kFull, act_lo), ah = __ballot_sync(kFull, act_hi);
     const unsigned e = __ballot_sync(kFull, esc_lo || esc_hi);
     __syncwarp();
@@ -423,15 +444,21 @@ __device__ __forceinline__ void finish_pixel(const PairDev& pr, int path, bool w
         }
     }
     if (e) {
-        uint16_t* base = pr.shadow + pr.shadow_stride * (size_t)path;
-        write_u16_vectors(tstate, G, esc_lo, esc_hi, base + pix_lo * pr.nd_pad, base + pix_hi * pr.nd_pad);
+        if constexpr (CP) {
+            const bool w_lo = esc_lo && slot_lo != kNoSlot, w_hi = esc_hi && slot_hi != kNoSlot;
+            write_u16_vectors(tstate, G, w_lo, w_hi, et.shadow + (w_lo ? (size_t)slot_lo * et.Dp : 0),
+                              et.shadow + (w_hi ? (size_t)slot_hi * et.Dp : 0));
+        } else {
+            uint16_t* base = pr.shadow + pr.shadow_stride * (size_t)path;
+            write_u16_vectors(tstate, G, esc_lo, esc_hi, base + pix_lo * pr.nd_pad, base + pix_hi * pr.nd_pad);
+        }
     }
     __syncwarp();
 }
 
 // Unit = 64 scanlines of a vertical or diagonal path. WT: the batch has
 // wide-slab pairs (the u16 body is compiled in).
-template <typename CT, bool WT>
+template <typename CT, bool WT, bool CP>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
                                                   uint32_t tstate, CT* __restrict__ stage,
                                                   int seg_words, unsigned char* __restrict__ tile,
@@ -442,6 +469,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     const int Dp = k.Dp, Dv = pr.nd_vec;
     const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx, dy = job.dy;
+    const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
 
     const int k0 = job.k_min + first;         // scanline index of tile row 0
     // This lane's two scanlines (tile rows lane and lane + 32): a scanline's
@@ -524,13 +552,13 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
             mx = wide ? sgm_pixel<true, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
                       : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
         const size_t pix0 = (size_t)y * W + xb;
-        finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
+        finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                      row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
     }
 }
 
 // Unit = 64 rows of a horizontal path (banded census).
-template <typename CT, bool WT>
+template <typename CT, bool WT, bool CP>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job, int first,
                                                     uint32_t tstate, unsigned char* __restrict__ tile,
                                                     int row_bytes) {
@@ -540,6 +568,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const int Dp = k.Dp, Dv = pr.nd_vec;
     const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx;
+    const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
     const bool act_lo = first + lane < job.num_scanlines;
     const bool act_hi = first + 32 + lane < job.num_scanlines;
     // Banded census: word (x, y) at ((y / 32) * W + x) * 32 + y % 32, so the 32
@@ -581,7 +610,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
                       : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
         // Rows first..first+63, one vector per row at column x.
         const size_t pix0 = (size_t)first * W + x;
-        finish_pixel(pr, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
+        finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                      row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
     }
     (void)H;
@@ -589,7 +618,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
 
 }  // namespace
 
-template <typename CT, bool WT>
+template <typename CT, bool WT, bool CP>
 __global__ void __launch_bounds__(kAggMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
@@ -628,9 +657,9 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT, WT>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
+            run_horizontal_unit<CT, WT, CP>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
         else
-            run_vertical_unit<CT, WT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
+            run_vertical_unit<CT, WT, CP>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
         __syncwarp();
     }
 
@@ -643,11 +672,17 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     }
 }
 
-// The kernel for a batch's census word width and tile format.
-const void* aggregate_kernel_fn(bool census64, bool wide_tiles) {
-    if (census64) return wide_tiles ? (const void*)aggregate_kernel<uint64_t, true>
-                                    : (const void*)aggregate_kernel<uint64_t, false>;
-    return wide_tiles ? (const void*)aggregate_kernel<uint32_t, true> : (const void*)aggregate_kernel<uint32_t, false>;
+// The kernel for a batch's census word width, tile format and shadow kind.
+template <bool CP>
+const void* aggregate_kernel_cp(bool census64, bool wide_tiles) {
+    if (census64) return wide_tiles ? (const void*)aggregate_kernel<uint64_t, true, CP>
+                                    : (const void*)aggregate_kernel<uint64_t, false, CP>;
+    return wide_tiles ? (const void*)aggregate_kernel<uint32_t, true, CP>
+                      : (const void*)aggregate_kernel<uint32_t, false, CP>;
+}
+
+const void* aggregate_kernel_fn(bool census64, bool wide_tiles, bool compact) {
+    return compact ? aggregate_kernel_cp<true>(census64, wide_tiles) : aggregate_kernel_cp<false>(census64, wide_tiles);
 }
 
 // Launch shape of the aggregation kernel for a batch whose largest padded D is
@@ -670,9 +705,13 @@ int max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, aggregate_kernel_fn(census64, wide_tiles)) == cudaSuccess && fa.numRegs > 0)
-        regs = fa.numRegs;
+    // Either shadow kind may run with the shape chosen here: the larger register count counts.
+    for (bool compact : {false, true}) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, aggregate_kernel_fn(census64, wide_tiles, compact)) == cudaSuccess &&
+            fa.numRegs > 0)
+            regs = compact ? std::max(regs, fa.numRegs) : fa.numRegs;
+    }
     cudaGetLastError();
     const int by_regs = regs_sm / (regs * 128);
     const int by_smem =
@@ -711,8 +750,10 @@ cudaError_t prepare() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaError_t e = cudaSuccess;
-    for (const void* fn : {aggregate_kernel_fn(false, false), aggregate_kernel_fn(true, false),
-                           aggregate_kernel_fn(false, true), aggregate_kernel_fn(true, true)}) {
+    for (const void* fn : {aggregate_kernel_fn(false, false, false), aggregate_kernel_fn(true, false, false),
+                           aggregate_kernel_fn(false, true, false), aggregate_kernel_fn(true, true, false),
+                           aggregate_kernel_fn(false, false, true), aggregate_kernel_fn(true, false, true),
+                           aggregate_kernel_fn(false, true, true), aggregate_kernel_fn(true, true, true)}) {
         cudaFuncAttributes fa{};
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)   // dynamic + static shared memory must fit the opt-in limit
@@ -736,7 +777,7 @@ static int grid_ctas_for(int dp_max, bool census64) {
 
 cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, bool compact) {
     if (num_units <= 0) return cudaSuccess;
     if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, census64, wide_tiles, num_units);
     const AggShape sh = shape_for(dp_max, census64, wide_tiles, warpgroups);
@@ -750,8 +791,8 @@ cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, c
     count_launch();
     void* args[] = {&d_pairs, &d_jobs, &d_units, &num_units, &counter, &dp_max,
                     const_cast<int*>(&sh.tmem_cols), const_cast<int*>(&sh.wg_cols)};
-    return cudaLaunchKernel(aggregate_kernel_fn(census64, wide_tiles), dim3(grid_ctas), dim3(threads), args,
-                            sh.smem, stream);
+    return cudaLaunchKernel(aggregate_kernel_fn(census64, wide_tiles, compact), dim3(grid_ctas), dim3(threads),
+                            args, sh.smem, stream);
 }
 
 }  // namespace pairs
@@ -769,11 +810,12 @@ int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool
 
 cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, int warpgroups,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                             int num_units, unsigned* counter, cudaStream_t stream) {
+                             int num_units, unsigned* counter, cudaStream_t stream, bool compact) {
     if (unit_scanlines == kUnitScanlines)
         return pairs::launch(dp_max, census64, wide_tiles, warpgroups, d_pairs, d_jobs, d_units, num_units,
-                             counter, stream);
-    return single::launch(dp_max, census64, warpgroups, d_pairs, d_jobs, d_units, num_units, counter, stream);
+                             counter, stream, compact);
+    return single::launch(dp_max, census64, warpgroups, d_pairs, d_jobs, d_units, num_units, counter, stream,
+                          compact);
 }
 
 }  // namespace vxsgm

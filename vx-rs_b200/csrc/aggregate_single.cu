@@ -178,17 +178,38 @@ __device__ __forceinline__ void flush_tile_wide(const uint4* __restrict__ tile, 
 // Writes the warp's output tile to the byte slab: lanes [la, lb] hold the
 // results of one pixel step; row p's vector goes to dst0 + p * stride bytes,
 // its 16-byte chunk h holding d = 16h..16h+15 (tile words 2h and 2h+1, the low
-// byte of every u16). A row whose bit is set in em (escaped) gets 0xFF in
-// byte 0 and its exact u16 words at sh0 + p * sstride (in u16) of the shadow.
+// byte of every u16). A row whose bit is set in em (escaped, pixel pix0 + p *
+// pstride) first gets a shadow slot s and its exact u16 words go to
+// shadow + s * Dp; then its byte row is written with 0xFF in byte 0 and s in
+// bytes 4..7 (the slot is put into the tile words whose low bytes form them).
 // Chunks are distributed over the lanes in address order, so that consecutive
 // lanes write consecutive 16 bytes of a vector (streaming stores: slabs are
 // read once by the WTA kernel and must not push the census planes, which every
 // path re-reads, out of L2).
-__device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int row_words, int G,
-                                           int la, int lb, unsigned em, uint8_t* __restrict__ dst0,
-                                           size_t stride, uint16_t* __restrict__ sh0,
-                                           size_t sstride, int lane) {
+// Without CP (no shadow pool in the batch) the escaped vectors' u16 words go to
+// sh0 + p * sstride, their pixels' places in the full shadow, after the chunks.
+template <bool CP>
+__device__ __forceinline__ void flush_tile(uint4* __restrict__ tile, int row_words, int G, int la, int lb,
+                                           unsigned em, uint8_t* __restrict__ dst0, size_t stride,
+                                           uint16_t* __restrict__ sh0, size_t sstride, const EscapeTarget& et,
+                                           size_t pix0, size_t pstride, int lane) {
     __syncwarp();
+    // Escaped vectors (rare): a slot each, their u16 words, the slot into the tile.
+    if constexpr (CP) for (unsigned m = em; m; m &= m - 1) {
+        const int pe = __ffs(m) - 1;               // bit p of em = row p (la <= p <= lb)
+        uint32_t slot = 0;
+        if (lane == 0) slot = take_slot(et, pix0 + (size_t)pe * pstride);
+        slot = __shfl_sync(kFull, slot, 0);
+        if (slot != kNoSlot)
+            for (int g = lane; g < G; g += 32)
+                __stcs(reinterpret_cast<uint4*>(et.shadow + (size_t)slot * et.Dp + 8 * g), tile[pe * row_words + g]);
+        __syncwarp();
+        if (lane == 0) {
+            tile[pe * row_words].z = (slot & 0xFFu) | ((slot >> 8) & 0xFFu) << 16;
+            tile[pe * row_words].w = ((slot >> 16) & 0xFFu) | (slot >> 24) << 16;
+        }
+        __syncwarp();
+    }
     // Chunk c = (p - la) * V + h of the run, walked with a running (p, h) so
     // that no division is needed per chunk: lane starts at c = lane, steps 32.
     const int V = (G + 1) >> 1;
@@ -213,12 +234,14 @@ __device__ __forceinline__ void flush_tile(const uint4* __restrict__ tile, int r
             ++p;
         }
     }
-    // Escaped vectors (rare): the warp writes their u16 words, one row at a time.
-    while (em) {
-        const int pe = __ffs(em) - 1;              // bit p of em = row p (la <= p <= lb)
-        em &= em - 1;
-        for (int g = lane; g < G; g += 32)
-            __stcs(reinterpret_cast<uint4*>(sh0 + (size_t)pe * sstride + 8 * g), tile[pe * row_words + g]);
+    if constexpr (!CP) {
+        // Escaped vectors (rare): the warp writes their u16 words, one row at a time.
+        while (em) {
+            const int pe = __ffs(em) - 1;          // bit p of em = row p (la <= p <= lb)
+            em &= em - 1;
+            for (int g = lane; g < G; g += 32)
+                __stcs(reinterpret_cast<uint4*>(sh0 + (size_t)pe * sstride + 8 * g), tile[pe * row_words + g]);
+        }
     }
     __syncwarp();
 }
@@ -357,7 +380,7 @@ __device__ __forceinline__ void clear_state(uint32_t tstate, int G) {
 }
 
 // Unit = 32 scanlines of a vertical or diagonal path.
-template <typename CT>
+template <typename CT, bool CP>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
                                                   uint32_t tstate, CT* __restrict__ stage,
                                                   int seg_words, uint4* __restrict__ tile,
@@ -386,6 +409,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
     uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
     uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
+    const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
     const int Dv = pr.nd_vec;
 
     // Stage the right-census segment [xb-(Dp-1), xb+31] of the step's row in
@@ -445,15 +469,15 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
             if (pr.wide_slabs)
                 flush_tile_wide(tile, row_words, k.G, la, lb, shd + pix0 * Dp, (size_t)Dp, lane);
             else
-                flush_tile(tile, row_words, k.G, la, lb, em, out + pix0 * Dv, (size_t)Dv,
-                           shd + pix0 * Dp, (size_t)Dp, lane);
+                flush_tile<CP>(tile, row_words, k.G, la, lb, em, out + pix0 * Dv, (size_t)Dv, shd + pix0 * Dp,
+                               (size_t)Dp, et, pix0, 1, lane);
         }
         __syncwarp();
     }
 }
 
 // Unit = 32 rows of a horizontal path (column-major census).
-template <typename CT>
+template <typename CT, bool CP>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job,
                                                     int first, uint32_t tstate,
                                                     uint4* __restrict__ tile, int row_words) {
@@ -474,6 +498,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const CT* __restrict__ CR = static_cast<const CT*>(pr.census_rt) + band * 32 + lane;
     uint8_t* __restrict__ out = pr.slabs + pr.slab_stride * (size_t)job.path;
     uint16_t* __restrict__ shd = pr.shadow + pr.shadow_stride * (size_t)job.path;
+    const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
     const int Dv = pr.nd_vec;
     (void)H;
 
@@ -497,8 +522,8 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
         if (pr.wide_slabs)
             flush_tile_wide(tile, row_words, k.G, 0, nrows - 1, shd + pix0 * Dp, (size_t)W * Dp, lane);
         else
-            flush_tile(tile, row_words, k.G, 0, nrows - 1, em, out + pix0 * Dv, (size_t)W * Dv,
-                       shd + pix0 * Dp, (size_t)W * Dp, lane);
+            flush_tile<CP>(tile, row_words, k.G, 0, nrows - 1, em, out + pix0 * Dv, (size_t)W * Dv, shd + pix0 * Dp,
+                           (size_t)W * Dp, et, pix0, (size_t)W, lane);
     }
 }
 
@@ -509,7 +534,7 @@ __host__ __device__ constexpr size_t single_warp_smem(int dp_max, size_t ct) {
     return 2 * (size_t)(dp_max + 40) * ct + (size_t)32 * (dp_max / 8 + 1) * 16;
 }
 
-template <typename CT>
+template <typename CT, bool CP>
 __global__ void __launch_bounds__(kMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
@@ -548,9 +573,9 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT>(pr, job, unit.first_scanline, tstate, tile, row_words);
+            run_horizontal_unit<CT, CP>(pr, job, unit.first_scanline, tstate, tile, row_words);
         else
-            run_vertical_unit<CT>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile,
+            run_vertical_unit<CT, CP>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile,
                                   row_words);
         __syncwarp();
     }
@@ -587,12 +612,16 @@ int max_warpgroups(int dp_max, bool census64) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, census64 ? (const void*)aggregate_kernel<uint64_t>
-                                            : (const void*)aggregate_kernel<uint32_t>) ==
-            cudaSuccess &&
-        fa.numRegs > 0)
-        regs = fa.numRegs;
+    // Either shadow kind may run with the shape chosen here: the larger register count counts.
+    for (bool compact : {false, true}) {
+        cudaFuncAttributes fa{};
+        const void* fn = census64 ? (compact ? (const void*)aggregate_kernel<uint64_t, true>
+                                             : (const void*)aggregate_kernel<uint64_t, false>)
+                                  : (compact ? (const void*)aggregate_kernel<uint32_t, true>
+                                             : (const void*)aggregate_kernel<uint32_t, false>);
+        if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess && fa.numRegs > 0)
+            regs = compact ? std::max(regs, fa.numRegs) : fa.numRegs;
+    }
     cudaGetLastError();
     const int by_regs = regs_sm / (regs * 128);
     const int by_smem = (int)((smem_sm - 1024) / (4 * single_warp_smem(dp_max, census64 ? 8 : 4)));
@@ -630,7 +659,8 @@ cudaError_t prepare() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaError_t e = cudaSuccess;
-    for (const void* fn : {(const void*)aggregate_kernel<uint32_t>, (const void*)aggregate_kernel<uint64_t>}) {
+    for (const void* fn : {(const void*)aggregate_kernel<uint32_t, false>, (const void*)aggregate_kernel<uint64_t, false>,
+                           (const void*)aggregate_kernel<uint32_t, true>, (const void*)aggregate_kernel<uint64_t, true>}) {
         cudaFuncAttributes fa{};
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)   // dynamic + static shared memory must fit the opt-in limit
@@ -654,7 +684,7 @@ static int grid_ctas_for(int dp_max, bool census64) {
 
 cudaError_t launch(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs,
                              const JobDev* d_jobs, const UnitDev* d_units, int num_units,
-                             unsigned* counter, cudaStream_t stream) {
+                             unsigned* counter, cudaStream_t stream, bool compact) {
     if (num_units <= 0) return cudaSuccess;
     if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, census64, num_units);
     const AggShape sh = shape_for(dp_max, census64, warpgroups);
@@ -666,12 +696,10 @@ cudaError_t launch(int dp_max, bool census64, int warpgroups, const PairDev* d_p
         std::fprintf(stderr, "vx_sgm: aggregation (single) %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
                      grid_ctas, sh.warpgroups, sh.tmem_cols, sh.smem);
     count_launch();
-    if (census64)
-        aggregate_kernel<uint64_t><<<grid_ctas, threads, sh.smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
-    else
-        aggregate_kernel<uint32_t><<<grid_ctas, threads, sh.smem, stream>>>(
-            d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols, sh.wg_cols);
+    auto fn = census64 ? (compact ? aggregate_kernel<uint64_t, true> : aggregate_kernel<uint64_t, false>)
+                       : (compact ? aggregate_kernel<uint32_t, true> : aggregate_kernel<uint32_t, false>);
+    fn<<<grid_ctas, threads, sh.smem, stream>>>(d_pairs, d_jobs, d_units, num_units, counter, dp_max, sh.tmem_cols,
+                                                sh.wg_cols);
     return cudaGetLastError();
 }
 

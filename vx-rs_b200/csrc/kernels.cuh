@@ -18,8 +18,12 @@ struct PairDev {
     // Per-path costs, pixel-major and d-minor, in one of two formats:
     //  * byte slabs (wide_slabs = 0): num_paths slabs of H*W vectors of Dv bytes.
     //    A vector whose values are all <= 254 is stored as bytes; any other has
-    //    byte 0 set to 0xFF (the escape marker) and its exact u16 values in the
-    //    shadow slab at the same pixel.
+    //    byte 0 set to 0xFF (the escape marker), bytes 4..7 set to its slot s
+    //    (u32) and its exact u16 values at shadow + s * Dp. With shadow_cap = 0
+    //    the shadow holds every vector, s = path * H*W + pixel; otherwise it is
+    //    a pool of shadow_cap vectors handed out in escape order by
+    //    esc_state[0], and esc_state[1] is set when the pool ran out (the
+    //    pair's result is then void and must be recomputed with a full shadow).
     //  * wide slabs (wide_slabs = 1, for configurations whose costs mostly
     //    exceed a byte): every vector in the shadow slabs; no byte slabs.
     uint8_t* slabs;
@@ -27,6 +31,8 @@ struct PairDev {
     uint16_t* shadow;      // num_paths slabs of H*W*Dp u16
     size_t shadow_stride;  // elements per shadow slab = H*W*Dp
     int wide_slabs;
+    uint32_t shadow_cap;   // 0: full shadow; else pool size in vectors
+    uint32_t* esc_state;   // [0] vectors taken from the pool, [1] overflow flag
     float* out_f32;        // subpixel (or integer) disparity, pitch in bytes
     size_t out_f32_pitch;
     int16_t* out_i16;      // optional integer disparity, pitch in bytes
@@ -47,6 +53,35 @@ struct PairDev {
     int census_tile_begin; // first census tile of this pair (census launch)
     int row_begin;         // first WTA row of this pair (WTA launch)
 };
+
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+
+#ifdef __CUDACC__
+// Where the escaped vectors of one path of one pair go, taken from the pair's
+// descriptor once per work unit so that the pixel loop keeps it in registers.
+struct EscapeTarget {
+    uint16_t* shadow;
+    uint32_t* esc_state;
+    uint32_t cap;        // 0: full shadow
+    uint32_t slot_base;  // full shadow: path * H*W
+    int Dp;
+};
+
+__device__ __forceinline__ EscapeTarget escape_target(const PairDev& pr, int path) {
+    return EscapeTarget{pr.shadow, pr.esc_state, pr.shadow_cap,
+                        (uint32_t)((size_t)path * pr.width * pr.height), pr.nd_pad};
+}
+
+// The shadow slot of an escaped vector at pixel `pix` (one lane), or kNoSlot
+// when the pool has run out (the overflow flag is then set).
+__device__ __forceinline__ uint32_t take_slot(const EscapeTarget& et, size_t pix) {
+    if (et.cap == 0) return et.slot_base + (uint32_t)pix;
+    const uint32_t s = atomicAdd(&et.esc_state[0], 1u);
+    if (s < et.cap) return s;
+    atomicExch(&et.esc_state[1], 1u);
+    return kNoSlot;
+}
+#endif
 
 // One aggregation job: one path direction of one pair.
 struct JobDev {

@@ -25,26 +25,28 @@ cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles
 // Two forms, picked by the plan's unit size: units of kUnitScanlines (64)
 // scanlines run the scanline-pair kernel (aggregate.cu), units of 32 the
 // single-scanline kernel (aggregate_single.cu). wide_tiles: the batch has
-// wide-slab pairs.
+// wide-slab pairs. compact: the batch has pairs with a shadow pool (their
+// kernels write the escape slot into the byte rows).
 cudaError_t prepare_aggregate_kernels();  // shared-memory limits of both; once per device
 int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool wide_tiles);
 cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, int warpgroups,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                             int num_units, unsigned* counter, cudaStream_t stream);
+                             int num_units, unsigned* counter, cudaStream_t stream, bool compact = false);
 namespace pairs {
 cudaError_t prepare();
 int max_warpgroups(int dp_max, bool census64, bool wide_tiles);
 int default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units);
 cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
-                   cudaStream_t stream);
+                   cudaStream_t stream, bool compact = false);
 }  // namespace pairs
 namespace single {
 cudaError_t prepare();
 int max_warpgroups(int dp_max, bool census64);
 int default_warpgroups(int dp_max, bool census64, int num_units);
 cudaError_t launch(int dp_max, bool census64, int warpgroups, const PairDev* d_pairs, const JobDev* d_jobs,
-                   const UnitDev* d_units, int num_units, unsigned* counter, cudaStream_t stream);
+                   const UnitDev* d_units, int num_units, unsigned* counter, cudaStream_t stream,
+                   bool compact = false);
 }  // namespace single
 
 // WTA + subpixel + optional LR check: one CTA per (pair, row). The kernel keeps

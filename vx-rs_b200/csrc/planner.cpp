@@ -38,16 +38,27 @@ bool wide_slabs(const vx_sgm_config& c) {
     return 64 + (int)(uint16_t)c.p2 > 254;
 }
 
+uint32_t shadow_pool_vectors(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
+    if (const char* f = std::getenv("VX_SGM_SHADOW_POOL")) {
+        const long v = std::strtol(f, nullptr, 10);
+        if (v > 0) return (uint32_t)v;
+    }
+    const size_t vectors = (size_t)width * height * cfg.num_paths;
+    return (uint32_t)std::max<size_t>(1024, (vectors + 15) / 16);
+}
+
 size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg,
-                            size_t census_word_bytes) {
+                            size_t census_word_bytes, bool compact_shadow) {
     const size_t npx = (size_t)width * height, ct = census_word_bytes, P = cfg.num_paths;
     const size_t dp = (cfg.num_disparities + 7) / 8 * 8;
     const size_t dv = (cfg.num_disparities + 15) / 16 * 16;
     const size_t banded = (size_t)((height + 31) / 32) * 32 * width * ct;
     const size_t guard = kCensusGuardWords * ct;
-    const size_t bytes = wide_slabs(cfg) ? 0 : align_up(npx * dv * P);
+    const bool wide = wide_slabs(cfg);
+    const size_t bytes = wide ? 0 : align_up(npx * dv * P);
+    const size_t shadow_vectors = (compact_shadow && !wide) ? shadow_pool_vectors(width, height, cfg) : npx * P;
     return 2 * align_up(npx * ct + 2 * guard) + 2 * align_up(banded) + bytes +
-           align_up(npx * dp * P * sizeof(uint16_t));
+           align_up(shadow_vectors * dp * sizeof(uint16_t));
 }
 
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
@@ -185,8 +196,14 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
         data += align_up(pd.slab_stride * P);
         pd.shadow_stride = npx * (size_t)Dp;
         pd.shadow = reinterpret_cast<uint16_t*>(data);
-        data += align_up(pd.shadow_stride * P * sizeof(uint16_t));
-        if (data - data0 != pair_workspace_bytes((uint32_t)W, (uint32_t)H, c, ct))
+        if ((size_t)P * npx >= kNoSlot)
+            return fail(VX_ERR_INVALID_ARGUMENT, "pair %d: %zu path vectors exceed the 32-bit shadow slots", i,
+                        (size_t)P * npx);
+        const bool compact = s.compact_shadow && !pd.wide_slabs;
+        pd.shadow_cap = compact ? shadow_pool_vectors((uint32_t)W, (uint32_t)H, c) : 0u;
+        if (compact) pl.compact = true;
+        data += align_up((compact ? (size_t)pd.shadow_cap : npx * P) * Dp * sizeof(uint16_t));
+        if (data - data0 != pair_workspace_bytes((uint32_t)W, (uint32_t)H, c, ct, compact))
             return fail(VX_ERR_GPU, "planner: pair layout and its size formula disagree");
 
         pl.dp_max = std::max(pl.dp_max, Dp);
@@ -263,8 +280,12 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     off = align_up(off + pl.jobs.size() * sizeof(JobDev));
     pl.off_units = off;
     off = align_up(off + pl.units.size() * sizeof(UnitDev));
+    // Counters: the aggregation work queue, then per pair the escape pool's
+    // taken count and overflow flag (all cleared by every launch).
     pl.off_counters = off;
-    off = align_up(off + sizeof(unsigned));
+    for (int i = 0; i < n; ++i)
+        pl.pairs[i].esc_state = reinterpret_cast<uint32_t*>(off + sizeof(unsigned) * (1 + 2 * (size_t)i));
+    off = align_up(off + sizeof(unsigned) * (1 + 2 * (size_t)n));
     pl.off_data = off;
     pl.ws_bytes = off + data;
     return VX_OK;
@@ -279,6 +300,7 @@ void bind_plan(Plan& pl, char* base) {
         pd.census_rt = data + reinterpret_cast<size_t>(pd.census_rt);
         pd.slabs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.slabs));
         pd.shadow = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.shadow));
+        pd.esc_state = reinterpret_cast<uint32_t*>(base + reinterpret_cast<size_t>(pd.esc_state));
     }
 }
 
@@ -308,8 +330,8 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     };
     const int n = (int)pl.pairs.size();
     if (n == 0) return VX_OK;
-    cudaError_t e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned), stream);
-    if (e != cudaSuccess) return cuda_fail(e, "clearing the work counter");
+    cudaError_t e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)n), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the work and escape counters");
     const PairDev* d_pairs = reinterpret_cast<const PairDev*>(base + pl.off_pairs);
     const JobDev* d_jobs = reinterpret_cast<const JobDev*>(base + pl.off_jobs);
     const UnitDev* d_units = reinterpret_cast<const UnitDev*>(base + pl.off_units);
@@ -320,7 +342,7 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) record(ev[1]);
     e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
-                         (int)pl.units.size(), counters, stream);
+                         (int)pl.units.size(), counters, stream, pl.compact);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) record(ev[2]);
     e = launch_wta(d_pairs, n, pl.total_rows, pl.max_width, stream);

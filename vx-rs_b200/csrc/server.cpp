@@ -20,7 +20,13 @@
 //    batch, as soon as one of max_inflight stream slots is free, and
 //  * launches the batch on that slot's stream: H2D of the images, the batched
 //    SGM (census, one persistent aggregation launch, WTA), D2H of the
-//    disparities, completion event.
+//    disparities and of the pairs' escape-pool flags, completion event.
+// A request's workspace holds its escaped path vectors (values above a byte,
+// rare) in a pool of 1/16 of its vectors instead of a full u16 shadow, which
+// cuts the device bytes a request reserves by about 3x and so lets three times
+// as many requests share a batch. A pair whose pool ran out is recomputed at
+// the head of the queue with a full shadow (or fails with VX_ERR_BUDGET if that
+// does not fit the budget), so results never depend on the pool.
 // Batches on different slots overlap on the GPU, so requests that arrive while
 // others run join the next batch instead of waiting for the GPU to drain. Each
 // request's result does not depend on which other requests share its batch.
@@ -115,6 +121,7 @@ struct Request {
     size_t host_off = kNoBlock;  // block of the staging arena, or kNoBlock (own pinned buffer)
     size_t host_bytes = 0;
     size_t dev_bytes = 0;        // upper bound of the request's share of a batch block
+    bool full_shadow = false;    // recomputed after its escape pool ran out
     Clock::time_point t_submit, t_done;
     ReqState state = kPending;
     vx_status status = VX_OK;
@@ -131,6 +138,7 @@ struct Slot {
     std::vector<Request*> reqs;
     bool busy = false;
     size_t block_off = kNoBlock, block_bytes = 0;  // the batch's block of the device arena
+    uint32_t* esc_host = nullptr;  // pinned: per request (escape count, pool overflow flag)
 };
 
 // Device bytes of a request's images and outputs inside a batch block.
@@ -168,8 +176,8 @@ struct vx_sgm_server {
     // Upper bound of the device bytes a request adds to a batch block: its
     // buffers, its workspace with 8-byte census words (a batch takes those for
     // all pairs when one pair needs them) and its share of the plan tables.
-    static size_t request_bytes(uint32_t w, uint32_t h, const vx_sgm_config& cfg, bool i16) {
-        return buffer_bytes(w, h, i16) + pair_workspace_bytes(w, h, cfg, 8) +
+    static size_t request_bytes(uint32_t w, uint32_t h, const vx_sgm_config& cfg, bool i16, bool compact) {
+        return buffer_bytes(w, h, i16) + pair_workspace_bytes(w, h, cfg, 8, compact) +
                pair_table_bytes_bound(w, h, cfg);
     }
 
@@ -225,7 +233,27 @@ void vx_sgm_server::retire(Slot& s) {
     if (s.block_off != kNoBlock) dev_alloc.release(s.block_off, s.block_bytes);
     s.block_off = kNoBlock;
     std::lock_guard<std::mutex> lk(mu);
+    // Pairs whose escape pool ran out go back to the head of the queue, in
+    // their order, with a full shadow.
+    for (size_t i = s.reqs.size(); i-- > 0;) {
+        Request* r = s.reqs[i];
+        if (r->state != kRunning || r->full_shadow || s.esc_host[2 * i + 1] == 0) continue;
+        r->full_shadow = true;
+        r->dev_bytes = request_bytes(r->w, r->h, r->cfg, r->want_i16, false);
+        ++stats.shadow_reruns;
+        if (r->dev_bytes > budget) {
+            r->state = kFailed;
+            r->status = VX_ERR_BUDGET;
+            r->t_done = now;
+            ++stats.failed;
+        } else {
+            r->state = kPending;
+            pending.push_front(r);
+        }
+    }
+    stats.queued = pending.size();
     for (Request* r : s.reqs) {
+        if (r->state == kPending) continue;  // queued again above
         r->t_done = now;
         if (r->state == kRunning) {
             r->state = kDone;
@@ -258,6 +286,7 @@ void vx_sgm_server::launch(Slot& s, std::vector<Request*>& batch) {
         im[2] = {ctx, nullptr, (size_t)r->w * 4, r->w, r->h, VX_FORMAT_F32, false};
         im[3] = {ctx, nullptr, (size_t)r->w * 2, r->w, r->h, VX_FORMAT_I16, false};
         specs.push_back({&im[0], &im[1], &im[2], r->want_i16 ? &im[3] : nullptr, r->cfg});
+        specs.back().compact_shadow = !r->full_shadow;
         buf_off[i] = buf_total;
         buf_total += buffer_bytes(r->w, r->h, r->want_i16);
     }
@@ -299,6 +328,11 @@ void vx_sgm_server::launch(Slot& s, std::vector<Request*>& batch) {
         rebind_pointers(plan, specs);
         bind_plan(plan, ws);
         st = run_plan(plan, ws, s.stream, ctx->next_timing_slot(), sgm->warpgroups_for(plan));
+        if (st == VX_OK) {
+            cudaError_t e = cudaMemcpyAsync(s.esc_host, ws + plan.off_counters + sizeof(unsigned),
+                                            2 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream);
+            if (e != cudaSuccess) st = cuda_fail(e, "server: escape flags download");
+        }
     }
     for (size_t i = 0; i < n && st == VX_OK; ++i) {
         Request* r = batch[i];
@@ -409,6 +443,7 @@ void destroy_server(vx_sgm_server* s) {
             cudaStreamDestroy(sl.stream);
         }
         if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.esc_host) cudaFreeHost(sl.esc_host);
     }
     for (auto& kv : s->requests) s->host_put(kv.second.get());
     if (s->dev_arena) {
@@ -440,6 +475,8 @@ vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config*
     for (auto& sl : s->slots) {
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(reinterpret_cast<void**>(&sl.esc_host), 2 * sizeof(uint32_t) * cfg->max_batch);
         if (e != cudaSuccess) {
             vx_status st = cuda_fail(e, "server_create");
             destroy_server(s);
@@ -506,7 +543,7 @@ vx_status vx_sgm_server_submit(vx_sgm_server* s, const uint8_t* left, const uint
     r->h = height;
     r->cfg = *cfg;
     r->want_i16 = want_i16 != 0;
-    r->dev_bytes = vx_sgm_server::request_bytes(width, height, *cfg, r->want_i16);
+    r->dev_bytes = vx_sgm_server::request_bytes(width, height, *cfg, r->want_i16, true);
     if (r->dev_bytes > s->budget) {
         std::lock_guard<std::mutex> lk(s->mu);
         ++s->stats.rejected;

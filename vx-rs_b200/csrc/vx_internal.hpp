@@ -80,7 +80,16 @@ struct PairSpec {
     vx_image* out_depth = nullptr;  // optional: fx * baseline / disparity
     float depth_scale = 0.0f;
     float depth_invalid = 0.0f;
+    // Byte-slab pairs only: escaped vectors go to a pool of
+    // shadow_pool_vectors() instead of a full shadow (a third of the
+    // workspace); the caller must check the pair's overflow flag after the run
+    // and recompute it with a full shadow if it is set (the server does).
+    bool compact_shadow = false;
 };
+
+// Vectors in a compact shadow pool: 1/16 of the pair's path-pixel vectors (at
+// least 1024); VX_SGM_SHADOW_POOL=<n> sets it (tests force overflows with it).
+uint32_t shadow_pool_vectors(uint32_t width, uint32_t height, const vx_sgm_config& cfg);
 
 vx_status validate_pair(const PairSpec& p);
 int census_bits(const vx_sgm_config& cfg);
@@ -93,6 +102,7 @@ struct Plan {
     std::vector<UnitDev> units;     // all (pair, path, scanline-group) units, longest first
     bool census64 = false;
     bool wide_tiles = false;        // some pair has wide (u16) slabs
+    bool compact = false;           // some pair has a shadow pool (shadow_cap > 0)
     int unit_scanlines = 32;        // 64: scanline-pair kernel, 32: single-scanline kernel
     long long units32 = 0;          // units the plan has at 32 scanlines (tuning key)
     int dp_max = 8;                 // largest padded disparity count
@@ -109,8 +119,9 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
 // Workspace bytes of one pair's census planes and path slabs with census words
 // of census_word_bytes (a batch uses 8-byte words for all its pairs as soon as
 // one needs them), and an upper bound of its share of the plan tables.
+// compact_shadow: the escape shadow is a pool (byte-slab pairs only).
 size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg,
-                            size_t census_word_bytes);
+                            size_t census_word_bytes, bool compact_shadow = false);
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg);
 // Points plan.pairs at the images and outputs of specs (same sizes and order
 // as the specs the plan was built from).

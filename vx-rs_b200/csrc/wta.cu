@@ -49,6 +49,7 @@ struct RowView {
     const uint16_t* shadow;
     size_t slab_stride, shadow_stride;
     int Dp, Dv;
+    uint32_t shadow_cap;  // 0: full shadow; else the pool size (slots beyond it were never written)
 };
 
 // The same sums for 8 u16 values (natural (d, d+1) pairs) into lo/hi words
@@ -68,8 +69,9 @@ __device__ __forceinline__ void add_u16_split(uint32_t (&a)[4], const uint4 v) {
 // 2^11 and whole 32-bit words can be added: the byte pairs (0, 2) and (1, 3) of
 // a 4-byte word are widened by a mask and a byte permute and summed with plain
 // 3-input adds, no carry reaching the next half. Escaped vectors (marker in the
-// byte 0 of the pixel's lane c = 0) are taken out again and replaced by their
-// exact u16 values from the shadow slab with per-half wrapping adds (rare).
+// byte 0 of the pixel's lane c = 0, shadow slot in its bytes 4..7) are taken
+// out again and replaced by their exact u16 values from the shadow with
+// per-half wrapping adds (rare).
 template <int NP, bool WIDE>
 __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, bool act, int lead,
                                           uint32_t (&acc)[4]) {
@@ -120,11 +122,22 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
                 a[3] -= __byte_perm(v[p].y, 0u, 0x4341);
             }
         }
+        // The slot: with a full shadow the vector's own place (path, pixel);
+        // with a pool the one written into the row's bytes 4..7.
+        const uint8_t* row0 = rv.slabs + pix * rv.Dv;  // the pixel's rows start here in every slab
 #pragma unroll
-        for (int p = 0; p < NP; ++p)
-            if (in_dp && ((em >> p) & 1u))
-                add_u16_split(a, __ldcs(reinterpret_cast<const uint4*>(rv.shadow + rv.shadow_stride * p +
-                                                                       pix * rv.Dp + 8 * c)));
+        for (int p = 0; p < NP; ++p) {
+            if (in_dp && ((em >> p) & 1u)) {
+                const uint16_t* src = rv.shadow + rv.shadow_stride * p + pix * rv.Dp;
+                bool ok = true;
+                if (rv.shadow_cap != 0) {
+                    const uint32_t slot = *reinterpret_cast<const uint32_t*>(row0 + rv.slab_stride * p + 4);
+                    ok = slot < rv.shadow_cap;
+                    src = rv.shadow + (size_t)slot * rv.Dp;
+                }
+                if (ok) add_u16_split(a, __ldcs(reinterpret_cast<const uint4*>(src + 8 * c)));
+            }
+        }
     }
     acc[0] = __byte_perm(a[0], a[1], 0x5410);
     acc[1] = __byte_perm(a[0], a[1], 0x7632);
@@ -166,7 +179,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const int sub = lane / seg, c = lane % seg;
     const int ppw = 32 / seg;
     const int kind = (P == 2 ? 0 : P == 4 ? 1 : 2) + (pr.wide_slabs ? 3 : 0);
-    const RowView rv{pr.slabs, pr.shadow, pr.slab_stride, pr.shadow_stride, pr.nd_pad, pr.nd_vec};
+    const RowView rv{pr.slabs, pr.shadow, pr.slab_stride, pr.shadow_stride, pr.nd_pad, pr.nd_vec, pr.shadow_cap};
     const bool subpixel = pr.subpixel != 0;
 
     for (int xb = warp * ppw; xb < W; xb += nwarps * ppw) {

@@ -614,7 +614,7 @@ class ServerStats(ctypes.Structure):
                 ("completed_pixel_disparities", ctypes.c_uint64),
                 ("pool_reserved_bytes", ctypes.c_uint64), ("pinned_bytes", ctypes.c_uint64),
                 ("max_launch_us", ctypes.c_uint64), ("max_pinned_alloc_us", ctypes.c_uint64),
-                ("staging_overflows", ctypes.c_uint64)]
+                ("staging_overflows", ctypes.c_uint64), ("shadow_reruns", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
