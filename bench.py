@@ -421,6 +421,47 @@ def run_stereo_match(args, local_rank):
     matcher.close()
 
 
+def run_single_pair(args, local_rank):
+    """The plain path for one pair size: synchronous compute_disparity calls on one
+    seeded slanted-plane pair (W x H, D disparities, P paths), device-resident images;
+    per-call latency (CUDA events) and per-stage device times."""
+    import torch
+
+    import vx_sgm
+    parts = [int(v) for v in args.pair.lower().split("x")]
+    w, h, d = parts[:3]
+    paths = parts[3] if len(parts) > 3 else 8
+    torch.cuda.set_device(local_rank)
+    ctx = vx_sgm.Context(local_rank)
+    sgm = vx_sgm.SGMStereo(ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    cfg = vx_sgm.SGMStereoConfig(num_disparities=d, p1=10.0, p2=120.0, census_radius_x=2, census_radius_y=2,
+                                 num_paths=paths, subpixel=True, lr_check=True, lr_tolerance=1,
+                                 invalid_value=-1.0)
+    L, R, _ = vx_sgm.synth_pair(vx_sgm.SCENE_SLANTED, w, h, 0, max(d - 8, 1), 3)
+    tl, tr = ctx.texture_gray8(L, w, h), ctx.texture_gray8(R, w, h)
+    of, oi = ctx.texture_output_r32float(w, h), ctx.texture_output_i16(w, h)
+    for _ in range(args.warmup):
+        sgm.compute_disparity(ctx, tl, tr, of, cfg, output_i16=oi)
+    ctx.enable_stage_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    for _ in range(args.steps):
+        e0.record(stream)
+        sgm.compute_disparity(ctx, tl, tr, of, cfg, output_i16=oi)
+        e1.record(stream)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    census_ms, agg_ms, wta_ms = ctx.stage_times()
+    ctx.enable_stage_timing(False)
+    pd = w * h * d
+    print(json.dumps({"config": "single pair", "pair": f"{w}x{h} D={d}, {paths} paths", "calls": args.steps,
+                      "value": pd / (float(np.mean(lat)) * 1e-3) / 1e9, "unit": UNIT,
+                      "latency_ms_p50": float(np.percentile(lat, 50)),
+                      "latency_ms_p99": float(np.percentile(lat, 99)),
+                      "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms}}), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -475,6 +516,9 @@ def main():
                          "CPU) instead of the benchmark")
     ap.add_argument("--stereo-only", default="", choices=[""] + [w[0] for w in STEREO_WORKLOADS],
                     help="with --stereo-match: run this workload only (profiler runs)")
+    ap.add_argument("--pair", default="", metavar="WxHxD[xP]",
+                    help="time synchronous calls on one pair of this size (the plain path) instead of "
+                         "the benchmark")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident batched steps only (profiler runs)")
     args = ap.parse_args()
@@ -507,6 +551,9 @@ def main():
         return
     if args.stereo_match:
         run_stereo_match(args, local_rank)
+        return
+    if args.pair:
+        run_single_pair(args, local_rank)
         return
     items = workload(rank, args.workload)
     if args.pairs:
