@@ -31,10 +31,36 @@ __device__ __forceinline__ int find_pair_by_tile(const PairDev* pairs, int n, in
     return lo;
 }
 
+// Descriptor of the window centred at (cx, cy) of the staged tile (row stride
+// sw); RX, RY < 0: the radii rx, ry at run time.
+template <int RX, int RY>
+__device__ __forceinline__ uint64_t window_bits(const uint8_t* __restrict__ tile_px, int sw, int cx, int cy, int rx,
+                                                int ry) {
+    if (RX >= 0) {
+        rx = RX;
+        ry = RY;
+    }
+    const int c = tile_px[cy * sw + cx];
+    uint64_t bits = 0;
+    int b = 0;
+#pragma unroll
+    for (int dy = -ry; dy <= ry; ++dy) {
+        const uint8_t* row = tile_px + (cy + dy) * sw + cx;
+#pragma unroll
+        for (int dx = -rx; dx <= rx; ++dx) {
+            if (dx == 0 && dy == 0) continue;
+            bits |= (uint64_t)(row[dx] < c) << b;
+            ++b;
+        }
+    }
+    return bits;
+}
+
 template <typename CT>
 __global__ void __launch_bounds__(kCensusTileW * kCensusTileH)
 census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint8_t tile_px[];
+    __shared__ CT tile_bits[kCensusTileH][kCensusTileW];
     const int pi = find_pair_by_tile(pairs, num_pairs, blockIdx.x);
     const PairDev& pr = pairs[pi];
     const int W = pr.width, H = pr.height, rx = pr.rx, ry = pr.ry;
@@ -58,25 +84,26 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     __syncthreads();
 
     const int x = bx + threadIdx.x, y = by + threadIdx.y;
-    if (x >= W || y >= H) return;
     // Clamped reads at the image border equal reads of the staged apron, which
     // was filled with clamped coordinates; interior threads read their window.
+    // The common windows (5x5, 9x7) are unrolled; the radii are uniform per CTA.
     const int cx = threadIdx.x + rx, cy = threadIdx.y + ry;
-    const int c = tile_px[cy * sw + cx];
-    uint64_t bits = 0;
-    int b = 0;
-    for (int dy = -ry; dy <= ry; ++dy) {
-        const uint8_t* row = tile_px + (cy + dy) * sw + cx;
-        for (int dx = -rx; dx <= rx; ++dx) {
-            if (dx == 0 && dy == 0) continue;
-            bits |= (uint64_t)(row[dx] < c) << b;
-            ++b;
-        }
-    }
+    uint64_t bits;
+    if (rx == 2 && ry == 2) bits = window_bits<2, 2>(tile_px, sw, cx, cy, rx, ry);
+    else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, sw, cx, cy, rx, ry);
+    else bits = window_bits<-1, -1>(tile_px, sw, cx, cy, rx, ry);
     CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
     CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
-    rm[(size_t)y * W + x] = (CT)bits;
-    cm[((size_t)(y >> 5) * W + x) * 32 + (y & 31)] = (CT)bits;
+    if (x < W && y < H) rm[(size_t)y * W + x] = (CT)bits;
+    // Banded copy: the tile's 8 rows of one column are 8 consecutive words
+    // there, so the descriptors go through shared memory and thread t writes
+    // column t / 8, row t % 8: eight threads fill one contiguous run.
+    tile_bits[threadIdx.y][threadIdx.x] = (CT)bits;
+    __syncthreads();
+    const int tid2 = threadIdx.y * kCensusTileW + threadIdx.x;
+    const int ox = bx + tid2 / kCensusTileH, oy = by + tid2 % kCensusTileH;
+    if (ox < W && oy < H)
+        cm[((size_t)(oy >> 5) * W + ox) * 32 + (oy & 31)] = tile_bits[tid2 % kCensusTileH][tid2 / kCensusTileH];
 }
 
 }  // namespace
