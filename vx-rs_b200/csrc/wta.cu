@@ -195,31 +195,33 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
             case 4: sum_paths<4, true>(rv, pix, c, act, sub * seg, acc); break;
             default: sum_paths<8, true>(rv, pix, c, act, sub * seg, acc); break;
         }
-        uint32_t s[8];
+        // key = S(d) << 8 | d (one byte permute: d in byte 0, S in bytes 1-2;
+        // d = 8c + j < 256), whose minimum is the first minimum.
+        const uint32_t d0 = 8u * (uint32_t)c;
+        uint32_t key[8];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            s[2 * k] = acc[k] & 0xFFFFu;
-            s[2 * k + 1] = acc[k] >> 16;
+            key[2 * k] = __byte_perm(acc[k], d0 + 2 * k, 0x5104);
+            key[2 * k + 1] = __byte_perm(acc[k], d0 + 2 * k + 1, 0x5324);
         }
+        const int nb = (act ? D : 0) - (int)d0;     // this lane's keys j < nb take part
         uint32_t best = 0xFFFFFFFFu;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int d = 8 * c + j;
-            if (act && d < D) best = min(best, (s[j] << 8) | (uint32_t)d);
-        }
+        for (int j = 0; j < 8; ++j)
+            if (j < nb) best = min(best, key[j]);
         for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
         const int bd = (int)(best & 0xFFu);
         // S(bd-1) and S(bd+1) from the lanes that hold them (only used when
         // 0 < bd < D-1, so both exist).
         const int dm = max(bd - 1, 0), dq = min(bd + 1, D - 1);
-        const uint32_t c0 = __shfl_sync(kFull, pick8(s, dm & 7), sub * seg + (dm >> 3));
-        const uint32_t c2 = __shfl_sync(kFull, pick8(s, dq & 7), sub * seg + (dq >> 3));
+        const uint32_t c0 = __shfl_sync(kFull, pick8(key, dm & 7), sub * seg + (dm >> 3)) >> 8;
+        const uint32_t c2 = __shfl_sync(kFull, pick8(key, dq & 7), sub * seg + (dq >> 3)) >> 8;
         if (lr && act) {
+            const int xr = x - 8 * c;               // right-view column of this lane's d = 8c
+            const int nr = min(D - 8 * c, xr + 1);  // j < nr: d < D and x - d >= 0
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int d = 8 * c + j;
-                if (d < D && x - d >= 0) atomicMin(&right_key[x - d], (s[j] << 8) | (uint32_t)d);
-            }
+            for (int j = 0; j < 8; ++j)
+                if (j < nr) atomicMin(&right_key[xr - j], key[j]);
         }
         if (c == 0 && x < W) {
             float v = (float)bd;
