@@ -64,6 +64,31 @@ def test_escape_pool_and_reruns(gpu_ctx, sgm, monkeypatch, pool):
         assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
 
 
+def test_escape_pool_with_wide_slab_requests(gpu_ctx, sgm, monkeypatch):
+    """Batches that mix wide-slab requests (P2 = 300: every vector in u16, no pool)
+    with pooled byte-slab requests run the pool-aware kernels with wide tiles; with
+    a one-vector pool the byte-slab requests overflow, are recomputed, and every
+    result equals its solo result."""
+    monkeypatch.setenv("VX_SGM_SHADOW_POOL", "1")
+    reqs = []
+    for i in range(8):
+        L, R, c = _request(i)
+        if i % 2:
+            c = vx_sgm.SGMStereoConfig(num_disparities=c.num_disparities, census_radius_x=2, census_radius_y=2,
+                                       num_paths=8, p1=15.0, p2=300.0, lr_check=True)
+        reqs.append((L, R, c))
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=4 * biggest, max_batch=8, max_inflight_batches=1)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    results = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    monkeypatch.delenv("VX_SGM_SHADOW_POOL", raising=False)
+    assert st["completed"] == len(reqs) and st["failed"] == 0 and st["shadow_reruns"] > 0
+    for (L, R, c), (d, di, _) in zip(reqs, results):
+        assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
+
+
 def test_serving_allocates_nothing_after_start(gpu_ctx, sgm):
     """The device arena and the pinned staging arena are taken at creation; serving a
     stream of mixed requests grows neither the context's pool nor the pinned memory."""
