@@ -11,7 +11,10 @@
 // centre <= 0 gives 0; otherwise the mean of the valid neighbours weighted by
 // exp(-(dx^2+dy^2) / (2 ss^2)) * exp(-(n-c)^2 / (2 sd^2)), or the centre when
 // the weights sum to at most 1e-8; single-precision arithmetic in the shader's
-// order, without fused multiply-adds (so only expf may differ from a host's).
+// order, without fused multiply-adds. The spatial weights use expf; the range
+// weight, one per neighbour, the __expf intrinsic (a few ulp from expf, and
+// Metal's fast-math exp is not exact either), so results agree with a host
+// build to about 1e-6 relative.
 //
 // Mapping: one thread per output pixel of a 32x8 tile; the tile and its apron
 // (clamped coordinates) are staged in shared memory once per CTA. Median: the
@@ -133,27 +136,34 @@ median_kernel_large(const float* __restrict__ in, size_t in_pitch, float* __rest
     __syncthreads();
     const int x = blockIdx.x * kTileW + threadIdx.x, y = blockIdx.y * kTileH + threadIdx.y;
     if (x >= W || y >= H) return;
-    const int TW = kTileW + 2 * R, n = 2 * R + 1, N = n * n;
-    auto val = [&](int i) {
-        const float d = s[(threadIdx.y + i / n) * TW + threadIdx.x + i % n];
+    const int TW = kTileW + 2 * R, n = 2 * R + 1;
+    const float* win = s + threadIdx.y * TW + threadIdx.x;  // the window's top-left value
+    // Values in raster order: element i = (i / n, i % n), walked row by row.
+    auto val = [&](int dy, int dx) {
+        const float d = win[dy * TW + dx];
         return d > 0.0f ? d : INFINITY;
     };
     int count = 0;
-    for (int i = 0; i < N; ++i) count += s[(threadIdx.y + i / n) * TW + threadIdx.x + i % n] > 0.0f ? 1 : 0;
+    for (int dy = 0; dy < n; ++dy)
+        for (int dx = 0; dx < n; ++dx) count += win[dy * TW + dx] > 0.0f ? 1 : 0;
     const int k = count / 2;
     float r = 0.0f;
-    for (int i = 0; i < N && count > 0; ++i) {
-        const float vi = val(i);
-        int rank = 0;
-        for (int j = 0; j < N; ++j) {
-            const float vj = val(j);
-            rank += (vj < vi || (j < i && vj == vi)) ? 1 : 0;
+    bool found = count == 0;
+    for (int iy = 0; iy < n && !found; ++iy)
+        for (int ix = 0; ix < n && !found; ++ix) {
+            const float vi = val(iy, ix);
+            const int i = iy * n + ix;
+            int rank = 0;
+            for (int jy = 0; jy < n; ++jy)
+                for (int jx = 0; jx < n; ++jx) {
+                    const float vj = val(jy, jx);
+                    rank += (vj < vi || (jy * n + jx < i && vj == vi)) ? 1 : 0;
+                }
+            if (rank == k) {
+                r = vi;
+                found = true;
+            }
         }
-        if (rank == k) {
-            r = vi;
-            break;
-        }
-    }
     *reinterpret_cast<float*>(reinterpret_cast<char*>(out) + (size_t)y * out_pitch + (size_t)x * sizeof(float)) = r;
 }
 
@@ -177,14 +187,19 @@ bilateral_kernel(const float* __restrict__ in, size_t in_pitch, float* __restric
     float res = 0.0f;
     if (!(c <= 0.0f)) {
         float sum = 0.0f, wsum = 0.0f;
-        for (int i = 0; i < n * n; ++i) {
-            const float nb = s[(threadIdx.y + i / n) * TW + threadIdx.x + i % n];
-            if (nb <= 0.0f) continue;
-            const float diff = __fsub_rn(nb, c);
-            const float wd = expf(__fmul_rn(__fmul_rn(-diff, diff), inv_2sd));
-            const float wt = __fmul_rn(ws[i], wd);
-            sum = __fadd_rn(sum, __fmul_rn(nb, wt));
-            wsum = __fadd_rn(wsum, wt);
+        // Raster order (the shader's): rows dy, then columns dx.
+        for (int dy = 0; dy < n; ++dy) {
+            const float* row = s + (threadIdx.y + dy) * TW + threadIdx.x;
+            const float* wrow = ws + dy * n;
+            for (int dx = 0; dx < n; ++dx) {
+                const float nb = row[dx];
+                if (nb <= 0.0f) continue;
+                const float diff = __fsub_rn(nb, c);
+                const float wd = __expf(__fmul_rn(__fmul_rn(-diff, diff), inv_2sd));
+                const float wt = __fmul_rn(wrow[dx], wd);
+                sum = __fadd_rn(sum, __fmul_rn(nb, wt));
+                wsum = __fadd_rn(wsum, wt);
+            }
         }
         res = wsum > 1e-8f ? __fdiv_rn(sum, wsum) : c;
     }
