@@ -5,8 +5,9 @@ shader's own outputs (tests/golden/depth_filter_cases.npz, made by
 tests/golden/make_depth_golden.py from shaders/DepthFilter.metal compiled as
 C++); the reference's own test assertions hold on the oracle.
 GPU: the CUDA filters through the C ABI against the same fixtures — the median
-bit-exact, the bilateral within 1e-5 relative (its exp is CUDA's expf, the
-fixtures' the host's) — and against the oracle on SGM disparity maps."""
+bit-exact, the bilateral within 1e-5 relative (its range weights come from CUDA's
+__expf intrinsic, the fixtures' from the host's expf) — and against the oracle on SGM
+disparity maps."""
 import json
 import os
 
