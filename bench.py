@@ -418,6 +418,44 @@ def run_stereo_match(args, local_rank):
             line["cpu_reference"] = {"value": pairs / rs / 1e9, "unit": "G pairs/s", "cores": 1,
                                      "kind": "reference", "sample": f"the whole workload once ({rs * 1e3:.1f} ms)"}
         print(json.dumps(line), flush=True)
+
+    # Frames: 64 frames of the example's size in one launch, against 64 calls.
+    if not args.stereo_only or args.stereo_only == "frames-64x512":
+        nf, n = 64, 512
+        cfg = vx_sgm.StereoConfig(**STEREO_WORKLOADS[0][3])
+        frames = [vx_sgm.synth_orb_stereo(n, n, 5000 + i) for i in range(nf)]
+        lo = np.arange(nf + 1, dtype=np.uint32) * n
+        ro = lo.copy()
+        cat = lambda i: np.concatenate([f[i] for f in frames])  # noqa: E731
+        lk, rk, ld, rd = cat(0), cat(1), cat(2), cat(3)
+        t_lk = torch.from_numpy(lk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_rk = torch.from_numpy(rk.view(np.float32).reshape(-1, 4).copy()).to(dev)
+        t_ld = torch.from_numpy(ld["desc"].view(np.int32).copy()).to(dev)
+        t_rd = torch.from_numpy(rd["desc"].view(np.int32).copy()).to(dev)
+        t_out = torch.empty((nf * n, 7), dtype=torch.int32, device=dev)
+        t_cnt = torch.empty((nf,), dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+
+        def frames_call():
+            matcher.run_frames_device(ctx, lo, ro, t_lk.data_ptr(), t_rk.data_ptr(), t_ld.data_ptr(),
+                                      t_rd.data_ptr(), cfg, t_out.data_ptr(), t_cnt.data_ptr(), stream=ctx.stream)
+        for _ in range(args.warmup):
+            frames_call()
+        reps = max(args.steps, 100)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            frames_call()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        pairs = nf * n * n
+        print(json.dumps({"config": "stereo-match", "workload": "frames-64x512",
+                          "desc": f"{nf} frames of {n} x {n} ORB keypoints in one launch, EuRoC intrinsics",
+                          "metric": "keypoint pairs/s", "unit": "G pairs/s",
+                          "device": {"value": pairs / (ms * 1e-3) / 1e9, "ms_per_call": ms,
+                                     "us_per_frame": 1e3 * ms / nf, "gpu_launches_per_call": 1},
+                          "matches": int(t_cnt.sum().item())}), flush=True)
     matcher.close()
 
 
@@ -514,7 +552,8 @@ def main():
     ap.add_argument("--stereo-match", action="store_true",
                     help="print one JSON line per sparse ORB stereo workload (device, end to end, "
                          "CPU) instead of the benchmark")
-    ap.add_argument("--stereo-only", default="", choices=[""] + [w[0] for w in STEREO_WORKLOADS],
+    ap.add_argument("--stereo-only", default="",
+                    choices=[""] + [w[0] for w in STEREO_WORKLOADS] + ["frames-64x512"],
                     help="with --stereo-match: run this workload only (profiler runs)")
     ap.add_argument("--pair", default="", metavar="WxHxD[xP]",
                     help="time synchronous calls on one pair of this size (the plain path) instead of "

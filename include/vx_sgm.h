@@ -390,6 +390,22 @@ vx_status vx_stereo_matcher_run_device(vx_stereo_matcher* matcher, vx_ctx* ctx, 
                                        const vx_stereo_config* cfg, vx_stereo_match_result* matches,
                                        uint32_t* match_count, vx_stream stream);
 
+/* Many frames in one launch (an addition for callers that match every frame of
+ * a sequence; per frame the result of run()): the keypoints and descriptors of
+ * all frames concatenated on the device, frame f's left keypoints at
+ * [left_offsets[f], left_offsets[f+1]) and right ones likewise (host arrays of
+ * n_frames + 1, starting at 0, non-decreasing; at most 2^23 - 1 right keypoints
+ * a frame). Frame f's matches go to matches + left_offsets[f] in ascending left
+ * index with frame-relative indices; match_counts[f] (device) gets their
+ * number. One CTA per frame: for frames of up to a few thousand keypoints.
+ * NULL stream = the context's stream, synchronous. */
+vx_status vx_stereo_matcher_run_frames_device(vx_stereo_matcher* matcher, vx_ctx* ctx, uint32_t n_frames,
+                                              const uint32_t* left_offsets, const uint32_t* right_offsets,
+                                              const vx_corner_point* left_kpts, const vx_corner_point* right_kpts,
+                                              const uint32_t* left_desc_words, const uint32_t* right_desc_words,
+                                              const vx_stereo_config* cfg, vx_stereo_match_result* matches,
+                                              uint32_t* match_counts, vx_stream stream);
+
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);
 

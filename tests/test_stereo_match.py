@@ -293,3 +293,53 @@ def test_gpu_banded_edge_geometry(gpu_ctx, matcher, monkeypatch, e):
         monkeypatch.setenv("VX_STEREO_FORM", form)
         got = matcher.run(gpu_ctx, lk, rk, ld, rd, _lib_cfg(cfg)).matches
         assert _same_records(got, want), form
+
+
+def _frames(sizes, seed):
+    frames = [vx_sgm.synth_orb_stereo(nl, nr, seed + i) for i, (nl, nr) in enumerate(sizes)]
+    lo = np.concatenate([[0], np.cumsum([len(f[0]) for f in frames])]).astype(np.uint32)
+    ro = np.concatenate([[0], np.cumsum([len(f[1]) for f in frames])]).astype(np.uint32)
+    cat = lambda i, dt: np.concatenate([f[i] for f in frames]) if len(frames) else np.zeros(0, dt)  # noqa: E731
+    return frames, lo, ro, cat(0, vx_sgm.CORNER_POINT), cat(1, vx_sgm.CORNER_POINT), cat(2, vx_sgm.ORB_OUTPUT), \
+        cat(3, vx_sgm.ORB_OUTPUT)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("max_hamming", [60, 0xFFFF])
+def test_gpu_frames_equal_per_frame_runs(gpu_ctx, matcher, max_hamming):
+    """Many frames in one launch: every frame's matches equal the oracle's for that
+    frame alone (frames without left or right keypoints, one keypoint, several
+    tiles of left keypoints, several shared-memory stages of right ones)."""
+    import torch
+    sizes = [(512, 512), (0, 40), (40, 0), (1, 1), (300, 700), (2000, 1100), (700, 2600), (257, 255)] * 3
+    frames, lo, ro, lk, rk, ld, rd = _frames(sizes, 300)
+    dev = torch.device("cuda", 0)
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a).view(dt).copy()).to(dev)  # noqa: E731
+    t_lk, t_rk = t(lk, np.float32), t(rk, np.float32)
+    t_ld, t_rd = t(ld["desc"], np.int32), t(rd["desc"], np.int32)
+    t_out = torch.full((int(lo[-1]), 7), -1, dtype=torch.int32, device=dev)
+    t_cnt = torch.full((len(sizes),), -1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    cfg = dict(max_hamming=max_hamming)
+    for _ in range(2):  # twice: nothing carries over between calls
+        matcher.run_frames_device(gpu_ctx, lo, ro, t_lk.data_ptr(), t_rk.data_ptr(), t_ld.data_ptr(),
+                                  t_rd.data_ptr(), _lib_cfg(dict(oracle.STEREO_DEFAULTS, **cfg)), t_out.data_ptr(),
+                                  t_cnt.data_ptr(), stream=None)
+        out = t_out.cpu().numpy().view(np.uint32)
+        cnt = t_cnt.cpu().numpy()
+        for f, (flk, frk, fld, frd) in enumerate(frames):
+            want = oracle.stereo_match(flk, frk, fld["desc"], frd["desc"], cfg)
+            assert cnt[f] == len(want), f
+            assert _same_records(out[lo[f]:lo[f] + cnt[f]], want), f
+
+
+@pytest.mark.gpu
+def test_gpu_frames_argument_checks(gpu_ctx, matcher):
+    """Offsets are checked on the host before anything runs."""
+    import torch
+    cnt = torch.zeros(4, dtype=torch.int32, device="cuda:0")
+    cfg = vx_sgm.StereoConfig()
+    with pytest.raises(vx_sgm.VxError, match="start at 0"):
+        matcher.run_frames_device(gpu_ctx, [1, 2], [0, 2], 0, 0, 0, 0, cfg, 0, cnt.data_ptr())
+    with pytest.raises(vx_sgm.VxError, match="decrease"):
+        matcher.run_frames_device(gpu_ctx, [0, 5, 3], [0, 1, 2], 0, 0, 0, 0, cfg, 0, cnt.data_ptr())

@@ -98,6 +98,15 @@ cudaError_t launch_stereo_match(const float4* left_kpts, const float4* right_kpt
                                 StereoMatchRecord* out, uint32_t* count, StereoMatchParams p,
                                 const StereoMatchShape& shape, cudaStream_t stream);
 
+// Frames: one launch over n_frames keypoint sets of the concatenated arrays
+// (frame f: left [left_offsets[f], left_offsets[f+1]), right likewise); each
+// frame's matches go to out + left_offsets[f] in ascending left index, with
+// frame-relative indices, and counts[f] receives their number. No scratch.
+cudaError_t launch_stereo_match_frames(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                       const uint4* right_desc, const uint32_t* left_offsets,
+                                       const uint32_t* right_offsets, uint32_t n_frames, StereoMatchRecord* out,
+                                       uint32_t* counts, StereoMatchParams p, cudaStream_t stream);
+
 // Banded form (large sets, 0 <= max_epipolar < 2^20): right keypoints
 // counting-sorted into 1-pixel row buckets 0..kRowBuckets-1 plus one bucket
 // for every other y. hist (kRowBuckets + 1) and arrival (1) are 0 between

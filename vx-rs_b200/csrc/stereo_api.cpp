@@ -28,6 +28,8 @@ struct vx_stereo_matcher {
     bool band_dirty = false;
     char* dev_io = nullptr;
     size_t dev_io_bytes = 0;
+    uint32_t* frame_offsets = nullptr;  // left | right offsets of the last frames call
+    size_t frame_offsets_cap = 0;       // words
     char* host_io = nullptr;
     size_t host_io_bytes = 0;
 };
@@ -203,6 +205,7 @@ void vx_stereo_matcher_destroy(vx_stereo_matcher* m) {
     cudaStreamSynchronize(m->ctx->stream);
     if (m->scratch) cudaFree(m->scratch);
     if (m->band) cudaFree(m->band);
+    if (m->frame_offsets) cudaFree(m->frame_offsets);
     if (m->dev_io) cudaFree(m->dev_io);
     if (m->host_io) cudaFreeHost(m->host_io);
     delete m;
@@ -237,6 +240,65 @@ vx_status vx_stereo_matcher_run_device(vx_stereo_matcher* m, vx_ctx* ctx, const 
         if (e != cudaSuccess) return cuda_fail(e, "stereo match");
     }
     return VX_OK;
+}
+
+vx_status vx_stereo_matcher_run_frames_device(vx_stereo_matcher* m, vx_ctx* ctx, uint32_t n_frames,
+                                              const uint32_t* left_offsets, const uint32_t* right_offsets,
+                                              const vx_corner_point* left_kpts, const vx_corner_point* right_kpts,
+                                              const uint32_t* left_desc_words, const uint32_t* right_desc_words,
+                                              const vx_stereo_config* cfg, vx_stereo_match_result* matches,
+                                              uint32_t* match_counts, vx_stream stream) {
+    if (!m || !ctx || !left_offsets || !right_offsets || !match_counts)
+        return fail(VX_ERR_INVALID_ARGUMENT, "stereo frames: NULL argument");
+    vx_status st = check_config(cfg);
+    if (st != VX_OK) return st;
+    if (n_frames == 0) return VX_OK;
+    if (left_offsets[0] != 0 || right_offsets[0] != 0)
+        return fail(VX_ERR_INVALID_ARGUMENT, "stereo frames: offsets must start at 0");
+    for (uint32_t f = 0; f < n_frames; ++f) {
+        if (left_offsets[f + 1] < left_offsets[f] || right_offsets[f + 1] < right_offsets[f])
+            return fail(VX_ERR_INVALID_ARGUMENT, "stereo frames: offsets of frame %u decrease", f);
+        if (right_offsets[f + 1] - right_offsets[f] > kStereoMaxRight)
+            return fail(VX_ERR_INVALID_ARGUMENT, "stereo frames: frame %u has more than %u right keypoints", f,
+                        kStereoMaxRight);
+    }
+    const uint32_t nl = left_offsets[n_frames], nr = right_offsets[n_frames];
+    if ((nl && (!left_kpts || !left_desc_words || !matches)) || (nr && (!right_kpts || !right_desc_words)))
+        return fail(VX_ERR_INVALID_ARGUMENT, "stereo frames: NULL device pointer");
+    if (!aligned16(left_kpts) || !aligned16(right_kpts) || !aligned16(left_desc_words) ||
+        !aligned16(right_desc_words) || !aligned4(matches) || !aligned4(match_counts))
+        return fail(VX_ERR_INVALID_ARGUMENT,
+                    "stereo frames: keypoints and descriptors must be 16-byte aligned, results 4-byte aligned");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    std::lock_guard<std::mutex> lock(m->mu);
+    const size_t words = 2 * ((size_t)n_frames + 1);
+    if (m->frame_offsets_cap < words) {
+        const size_t cap = std::max(words, 2 * m->frame_offsets_cap);
+        if (m->frame_offsets) cudaFreeAsync(m->frame_offsets, s);
+        m->frame_offsets = nullptr;
+        m->frame_offsets_cap = 0;
+        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->frame_offsets), cap * sizeof(uint32_t),
+                                                ctx->pool, s);
+        if (e != cudaSuccess) return cuda_fail(e, "stereo frames offsets");
+        m->frame_offsets_cap = cap;
+    }
+    // Pageable sources: the copies are staged before they return.
+    cudaError_t e = cudaMemcpyAsync(m->frame_offsets, left_offsets, (n_frames + 1) * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->frame_offsets + n_frames + 1, right_offsets, (n_frames + 1) * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_stereo_match_frames(reinterpret_cast<const float4*>(left_kpts),
+                                       reinterpret_cast<const float4*>(right_kpts),
+                                       reinterpret_cast<const uint4*>(left_desc_words),
+                                       reinterpret_cast<const uint4*>(right_desc_words), m->frame_offsets,
+                                       m->frame_offsets + n_frames + 1, n_frames,
+                                       reinterpret_cast<StereoMatchRecord*>(matches), match_counts,
+                                       make_params(cfg, 0, 0), s);
+    if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? VX_OK : cuda_fail(e, "stereo frames");
 }
 
 vx_status vx_stereo_matcher_run(vx_stereo_matcher* m, vx_ctx* ctx, const vx_corner_point* left_kpts,

@@ -381,7 +381,111 @@ __global__ void __launch_bounds__(kBandThreads) match_banded_kernel(
     if (threadIdx.x == 0 && n) atomicAdd(&tile_counts[(blockIdx.x * kBandLefts) / kTileLefts], (uint32_t)n);
 }
 
+// ---- frames: many small keypoint sets in one launch -------------------------
+//
+// One CTA per frame (frame f: left keypoints [lo[f], lo[f+1]), right keypoints
+// [ro[f], ro[f+1]) of the concatenated arrays). The CTA takes its left
+// keypoints 256 at a time; for each such tile it stages the frame's right
+// keypoints in shared memory as the match kernel does, keeps the running
+// minimum key per thread, then emits the tile's matches in left index order
+// (block scan) after those of the frame's earlier tiles. Records go to
+// out[lo[f] + slot] with frame-relative indices; counts[f] gets the frame's
+// number of matches. No scratch, no second kernel: for frames of up to a few
+// thousand keypoints, where a launch per frame would cost more than its work.
+__global__ void __launch_bounds__(kTileLefts) match_frames_kernel(
+    const float4* __restrict__ lk, const float4* __restrict__ rk, const uint4* __restrict__ ld,
+    const uint4* __restrict__ rd, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ ro,
+    StereoMatchRecord* __restrict__ out, uint32_t* __restrict__ counts, StereoMatchParams p) {
+    __shared__ float2 s_pos[kStage];
+    __shared__ uint4 s_desc[2 * kStage];
+    __shared__ uint32_t s_warp[kTileLefts / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t f = blockIdx.x;
+    const uint32_t l_begin = lo[f], nl = lo[f + 1] - l_begin;
+    const uint32_t r_begin = ro[f], nr = ro[f + 1] - r_begin;
+    uint32_t emitted = 0;
+    for (uint32_t t0 = 0; t0 < nl; t0 += kTileLefts) {
+        const uint32_t li = t0 + threadIdx.x;  // frame-relative
+        const bool have = li < nl && nr > 0;
+        float lx = 0.0f, ly = __int_as_float(0x7fc00000);
+        uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0;
+        if (have) {
+            const float4 k = lk[l_begin + li];
+            lx = k.x;
+            ly = k.y;
+            a0 = ld[2 * (size_t)(l_begin + li)];
+            a1 = ld[2 * (size_t)(l_begin + li) + 1];
+        }
+        uint32_t best = kNoKey;
+        for (uint32_t base = 0; base < nr; base += kStage) {
+            const uint32_t cnt = min((uint32_t)kStage, nr - base);
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < cnt; k += kTileLefts) {
+                const float4 q = rk[r_begin + base + k];
+                s_pos[k] = make_float2(q.x, q.y);
+            }
+            for (uint32_t k = threadIdx.x; k < 2 * cnt; k += kTileLefts)
+                s_desc[k] = rd[2 * (size_t)(r_begin + base) + k];
+            __syncthreads();
+#pragma unroll 4
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const float2 q = s_pos[k];
+                const float dy = fabsf(__fsub_rn(ly, q.y));
+                const float d = __fsub_rn(lx, q.x);
+                if (dy <= p.max_epipolar && d >= p.min_disparity && d <= p.max_disparity) {
+                    const uint32_t dist = hamming256(a0, a1, s_desc[2 * k], s_desc[2 * k + 1]);
+                    best = min(best, (dist << kRightBits) | (base + k));
+                }
+            }
+        }
+        // A frame without right keypoints has no matches (stereomatch.rs:138-142).
+        const bool take = have && accepted(best, p.max_hamming);
+        const uint32_t ballot = __ballot_sync(0xffffffffu, take);
+        __syncthreads();  // s_warp reused across tiles
+        if (lane == 0) s_warp[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (int w = 0; w < kTileLefts / 32; ++w) {
+            const uint32_t c = s_warp[w];
+            before += w < warp ? c : 0u;
+            total += c;
+        }
+        if (take) {
+            const uint32_t slot = emitted + before + __popc(ballot & ((1u << lane) - 1u));
+            const uint32_t ri = best == kNoKey ? 0u : (best & kRightMask);
+            const float4 l = lk[l_begin + li];
+            const float4 r = rk[r_begin + ri];
+            const float disp = __fsub_rn(l.x, r.x);
+            const float Z = __fdiv_rn(__fmul_rn(p.fx, p.baseline), disp);
+            const float X = __fdiv_rn(__fmul_rn(Z, __fsub_rn(l.x, p.cx)), p.fx);
+            const float Y = __fdiv_rn(__fmul_rn(Z, __fsub_rn(l.y, p.cy)), p.fy);
+            StereoMatchRecord& o = out[l_begin + slot];
+            o.left_idx = li;
+            o.right_idx = ri;
+            o.disparity = disp;
+            o.point_3d[0] = X;
+            o.point_3d[1] = Y;
+            o.point_3d[2] = Z;
+            o.pad = 0.0f;
+        }
+        emitted += total;
+    }
+    if (threadIdx.x == 0) counts[f] = emitted;
+}
+
 }  // namespace
+
+cudaError_t launch_stereo_match_frames(const float4* left_kpts, const float4* right_kpts, const uint4* left_desc,
+                                       const uint4* right_desc, const uint32_t* left_offsets,
+                                       const uint32_t* right_offsets, uint32_t n_frames, StereoMatchRecord* out,
+                                       uint32_t* counts, StereoMatchParams p, cudaStream_t stream) {
+    if (n_frames == 0) return cudaSuccess;
+    match_frames_kernel<<<n_frames, kTileLefts, 0, stream>>>(left_kpts, right_kpts, left_desc, right_desc,
+                                                             left_offsets, right_offsets, out, counts, p);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) count_launch();
+    return e;
+}
 
 StereoMatchShape stereo_match_shape(uint32_t n_left, uint32_t n_right, int sm_count) {
     StereoMatchShape s;

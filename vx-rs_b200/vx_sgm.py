@@ -507,6 +507,8 @@ _sm_run = _sig("vx_stereo_matcher_run", ctypes.c_int, _P, _P, _P, ctypes.c_size_
                ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t))
 _sm_run_device = _sig("vx_stereo_matcher_run_device", ctypes.c_int, _P, _P, _P, ctypes.c_uint32, _P,
                       ctypes.c_uint32, _P, _P, ctypes.POINTER(_CStereoConfig), _P, _P, _P)
+_sm_run_frames = _sig("vx_stereo_matcher_run_frames_device", ctypes.c_int, _P, _P, ctypes.c_uint32, _P, _P,
+                      _P, _P, _P, _P, ctypes.POINTER(_CStereoConfig), _P, _P, _P)
 
 
 @dataclass
@@ -588,6 +590,20 @@ class StereoMatcher:
         _check(_sm_run_device(self._h, ctx.handle, _P(left_kpts), n_left, _P(right_kpts), n_right,
                               _P(left_desc_words), _P(right_desc_words), ctypes.byref(c), _P(matches),
                               _P(match_count), _P(stream) if stream else None))
+
+    def run_frames_device(self, ctx: Context, left_offsets, right_offsets, left_kpts: int, right_kpts: int,
+                          left_desc_words: int, right_desc_words: int, config: StereoConfig, matches: int,
+                          match_counts: int, stream: int | None = None):
+        """Many frames in one launch (vx_stereo_matcher_run_frames_device): offsets
+        are host arrays of n_frames + 1 (numpy or lists), the rest device pointers."""
+        lo = np.ascontiguousarray(left_offsets, np.uint32)
+        ro = np.ascontiguousarray(right_offsets, np.uint32)
+        if lo.shape != ro.shape or lo.size < 1:
+            raise ValueError("left and right offsets need n_frames + 1 entries each")
+        c = config.to_c()
+        _check(_sm_run_frames(self._h, ctx.handle, lo.size - 1, _P(lo.ctypes.data), _P(ro.ctypes.data),
+                              _P(left_kpts), _P(right_kpts), _P(left_desc_words), _P(right_desc_words),
+                              ctypes.byref(c), _P(matches), _P(match_counts), _P(stream) if stream else None))
 
     def close(self):
         if self._h:
