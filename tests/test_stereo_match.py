@@ -343,3 +343,32 @@ def test_gpu_frames_argument_checks(gpu_ctx, matcher):
         matcher.run_frames_device(gpu_ctx, [1, 2], [0, 2], 0, 0, 0, 0, cfg, 0, cnt.data_ptr())
     with pytest.raises(vx_sgm.VxError, match="decrease"):
         matcher.run_frames_device(gpu_ctx, [0, 5, 3], [0, 1, 2], 0, 0, 0, 0, cfg, 0, cnt.data_ptr())
+
+
+@pytest.mark.gpu
+def test_gpu_matcher_shared_between_host_threads(gpu_ctx, matcher):
+    """StereoMatcher is Send + Sync in the reference (stereomatch.rs:338-339): calls
+    from several host threads on one matcher (the library serialises them on its
+    scratch) each return their own frame's matches."""
+    import threading
+    frames = [vx_sgm.synth_orb_stereo(600 + 50 * i, 700, 900 + i) for i in range(6)]
+    want = [oracle.stereo_match(lk, rk, ld["desc"], rd["desc"]) for lk, rk, ld, rd in frames]
+    got = [None] * len(frames)
+    errors = []
+
+    def work(i):
+        try:
+            for _ in range(5):
+                lk, rk, ld, rd = frames[i]
+                got[i] = matcher.run(gpu_ctx, lk, rk, ld, rd, vx_sgm.StereoConfig()).matches
+        except Exception as e:  # noqa: BLE001 (reported below)
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(len(frames))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for g, w in zip(got, want):
+        assert _same_records(g, w)
