@@ -208,7 +208,8 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path);
  * bucket share its workspace, so they must be ordered on one stream. */
 vx_status vx_sgm_set_graph_cache(vx_sgm* sgm, uint32_t max_buckets);
 
-/* Device bytes of intermediate state one pair needs (census + path slabs). */
+/* Device bytes of intermediate state one pair needs (census, path slabs and the
+ * matching-cost volume of the scanline-pair kernel). */
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg);
 
 /* Debug dump for parity tests (no reference counterpart): runs one pair and

@@ -47,23 +47,25 @@ def test_workspace_bytes_formula():
     cfg = vx_sgm.SGMStereoConfig(num_disparities=64, census_radius_x=2, census_radius_y=2, num_paths=4)
     b = vx_sgm.workspace_bytes(640, 480, cfg)
     # guarded row-major census planes + 32-row banded copies (480 = 15 bands)
-    # + byte slabs (Dv = 64) + u16 shadow slabs (Dp = 64)
+    # + byte slabs (Dv = 64) + u16 shadow slabs (Dp = 64) + the cost volume (Dv bytes a pixel)
     al = lambda v: (v + 255) // 256 * 256
     assert b == (2 * al(640 * 480 * 4 + 2 * 352 * 4) + 2 * 640 * 480 * 4 + 640 * 480 * 64 * 4
-                 + 640 * 480 * 64 * 4 * 2)
+                 + 640 * 480 * 64 * 4 * 2 + 640 * 480 * 64)
     # 9x7 census -> u64 words; D = 60 -> Dp = 64 (u16 shadow), Dv = 64 (bytes)
     cfg64 = vx_sgm.SGMStereoConfig(num_disparities=60, num_paths=8)
     assert vx_sgm.workspace_bytes(100, 10, cfg64) == (2 * al(1000 * 8 + 2 * 352 * 8) + 2 * al(32 * 100 * 8)
-                                                      + 1000 * 64 * 8 + 1000 * 64 * 8 * 2)
+                                                      + 1000 * 64 * 8 + 1000 * 64 * 8 * 2 + 1000 * 64)
     # D = 72: Dp = 72 for the shadow, Dv = 80 for the byte vectors
     cfg72 = vx_sgm.SGMStereoConfig(num_disparities=72, census_radius_x=2, census_radius_y=2, num_paths=2)
     assert vx_sgm.workspace_bytes(100, 10, cfg72) == (2 * al(1000 * 4 + 2 * 352 * 4) + 2 * al(32 * 100 * 4)
-                                                      + al(1000 * 80 * 2) + al(1000 * 72 * 2 * 2))
+                                                      + al(1000 * 80 * 2) + al(1000 * 72 * 2 * 2)
+                                                      + al(1000 * 80))
     # P2 > 190: most costs exceed a byte, so the vectors go to u16 slabs alone
     cfg_wide = vx_sgm.SGMStereoConfig(num_disparities=72, census_radius_x=2, census_radius_y=2,
                                       num_paths=2, p2=191.0)
     assert vx_sgm.workspace_bytes(100, 10, cfg_wide) == (2 * al(1000 * 4 + 2 * 352 * 4)
-                                                         + 2 * al(32 * 100 * 4) + al(1000 * 72 * 2 * 2))
+                                                         + 2 * al(32 * 100 * 4) + al(1000 * 72 * 2 * 2)
+                                                         + al(1000 * 80))
 
 
 def test_workspace_follows_the_slab_format(monkeypatch):

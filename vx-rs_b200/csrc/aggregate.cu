@@ -328,6 +328,108 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
     return ps.mx;
 }
 
+// Packed costs of disparities 4i..4i+3 (one word of each scanline's cost row):
+// cw = C_lo | C_hi << 16 by one byte permute each; the costs are at most 64, so
+// the sign-replicating selector bytes give the zero high bytes.
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
+__device__ __forceinline__ void cost_words(uint32_t (&cw)[8], const uint2 lo, const uint2 hi) {
+    cw[0] = prmt(lo.x, hi.x, 0xC480u);
+    cw[1] = prmt(lo.x, hi.x, 0xD591u);
+    cw[2] = prmt(lo.x, hi.x, 0xE6A2u);
+    cw[3] = prmt(lo.x, hi.x, 0xF7B3u);
+    cw[4] = prmt(lo.y, hi.y, 0xC480u);
+    cw[5] = prmt(lo.y, hi.y, 0xD591u);
+    cw[6] = prmt(lo.y, hi.y, 0xE6A2u);
+    cw[7] = prmt(lo.y, hi.y, 0xF7B3u);
+}
+
+// sgm_pixel with the costs read from the pair's cost volume: cv_lo / cv_hi = the
+// two scanlines' cost rows at this pixel (Dv bytes each, 64 already in place
+// where x - d < 0), 8 bytes per group, requested one group ahead.
+template <bool WIDE>
+__device__ __forceinline__ uint32_t sgm_pixel_cv(const uint32_t tstate, uint32_t& m, const uint32_t start,
+                                                 const uint8_t* __restrict__ cv_lo,
+                                                 const uint8_t* __restrict__ cv_hi, const ScanConst& k,
+                                                 unsigned char* __restrict__ row_lo,
+                                                 unsigned char* __restrict__ row_hi) {
+    PixelState ps;
+    const uint32_t m0 = m & ~start;
+    ps.o3x2 = __vadd2(m0, k.p2x2) & ~start;
+    ps.kc2 = __vadd2(~m0, k.p1p1x2);
+    ps.f = 0xFFFFFFFFu;            // o1 at d = 0
+    ps.mn = 0xFFFFFFFFu;
+    ps.mx = 0u;
+    auto load = [&](uint2& lo, uint2& hi, int g) {
+        lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo + 8 * g));
+        hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi + 8 * g));
+    };
+    auto store = [&](const Words8& o, int g) {
+        if (WIDE) {             // u16 rows: 8 values (16 bytes) per group
+            *reinterpret_cast<uint4*>(row_lo + 16 * g) = make_uint4(
+                __byte_perm(o.w[0], o.w[1], 0x5410), __byte_perm(o.w[2], o.w[3], 0x5410),
+                __byte_perm(o.w[4], o.w[5], 0x5410), __byte_perm(o.w[6], o.w[7], 0x5410));
+            *reinterpret_cast<uint4*>(row_hi + 16 * g) = make_uint4(
+                __byte_perm(o.w[0], o.w[1], 0x7632), __byte_perm(o.w[2], o.w[3], 0x7632),
+                __byte_perm(o.w[4], o.w[5], 0x7632), __byte_perm(o.w[6], o.w[7], 0x7632));
+        } else {                // byte rows: 8 bytes per group
+            uint2 lo, hi;
+            group_bytes(o, lo, hi);
+            *reinterpret_cast<uint2*>(row_lo + 8 * g) = lo;
+            *reinterpret_cast<uint2*>(row_hi + 8 * g) = hi;
+        }
+        tmem_st8(tstate + 8 * g, o);
+    };
+    uint2 pa_l, pa_h, pb_l, pb_h;
+    uint32_t ca[8], cb[8];
+    Words8 oa, ob;
+    uint32_t w7;
+    load(pa_l, pa_h, 0);
+    Words8 sa = tmem_ld8(tstate), sb;
+    cost_words(ca, pa_l, pa_h);
+    tmem_wait_ld(sa);
+    int g = 0;
+#pragma unroll 1
+    for (; g + 2 < k.G; g += 2) {
+        sb = tmem_ld8(tstate + 8 * (g + 1));
+        load(pb_l, pb_h, g + 1);
+        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
+        tmem_wait_ld(sb);
+        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
+        store(oa, g);
+        cost_words(cb, pb_l, pb_h);
+        sa = tmem_ld8(tstate + 8 * (g + 2));
+        load(pa_l, pa_h, g + 2);
+        sgm_group_head<false>(sb, cb, k, ps, ob, w7);
+        tmem_wait_ld(sa);
+        sgm_group_tail<false>(sb, sa.w[0], w7, k, ps, ob);
+        store(ob, g + 1);
+        cost_words(ca, pa_l, pa_h);
+    }
+    if (g + 1 < k.G) {
+        sb = tmem_ld8(tstate + 8 * (g + 1));
+        load(pb_l, pb_h, g + 1);
+        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
+        tmem_wait_ld(sb);
+        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
+        store(oa, g);
+        cost_words(cb, pb_l, pb_h);
+        sgm_group_head<true>(sb, cb, k, ps, ob, w7);
+        sgm_group_tail<true>(sb, 0u, w7, k, ps, ob);
+        store(ob, g + 1);
+    } else {
+        sgm_group_head<true>(sa, ca, k, ps, oa, w7);
+        sgm_group_tail<true>(sa, 0u, w7, k, ps, oa);
+        store(oa, g);
+    }
+    tmem_wait_st();            // the next pixel reads this state back
+    m = ps.mn;
+    return ps.mx;
+}
+
 __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
     ScanConst k;
     const uint32_t P1 = (uint32_t)pr.p1, P2 = (uint32_t)pr.p2;
@@ -489,75 +591,32 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     const int t_hi = __reduce_max_sync(kFull, max(te_lo, te_hi));
     if (t_lo >= t_hi) return;
 
-    const CT* __restrict__ CL = static_cast<const CT*>(pr.census_l);
-    const CT* __restrict__ CR = static_cast<const CT*>(pr.census_r);
-    // Stage the right-census segment [xb-(Dp-1), xb+63] of the step's row in
-    // 16-byte chunks from the aligned word at or below its start. The planes are
-    // surrounded by guard words (kCensusGuardWords), so the chunks may run past
-    // the row ends: words outside the image are never used for a cost (halves
-    // with x >= W are idle and x-d < 0 takes the border body).
-    // The alignment is taken on the plane's linear word index (row starts y*W
-    // are not 16-byte aligned in general); the plane base is.
-    constexpr int kPerChunk = 16 / sizeof(CT);
-    auto seg_start = [&](int t) {
-        return (ptrdiff_t)(y0 + dy * t) * W + (k0 + dx * t - (Dp - 1));
-    };
-    auto stage_step = [&](int t, int buf) {
-        const ptrdiff_t ls = seg_start(t);
-        const ptrdiff_t la = ls & ~(ptrdiff_t)(kPerChunk - 1);
-        const CT* src = CR + la;
-        CT* dstb = stage + buf * seg_words;
-        const int chunks = (Dp + 63 + (int)(ls - la) + kPerChunk - 1) / kPerChunk;
-        for (int j = lane; j < chunks; j += 32) cp_async16(dstb + j * kPerChunk, src + j * kPerChunk);
-        cp_async_commit();
-    };
-    auto seg_offset = [&](int t) {
-        const ptrdiff_t ls = seg_start(t);
-        return (int)(ls - (ls & ~(ptrdiff_t)(kPerChunk - 1)));
-    };
-    auto left = [&](int t, int i, int tb, int te) -> CT {
-        return (t >= tb && t < te) ? CL[(size_t)(y0 + dy * t) * W + (k0 + i) + dx * t] : CT(0);
-    };
-
+    // Costs from the pair's cost volume: the two scanlines' rows at the step's
+    // pixels (a half outside its scanline reads pixel 0's row, in bounds and
+    // unused: it restarts from L = C where its scanline begins).
+    const uint8_t* __restrict__ CV = pr.costs;
     unsigned char* row_lo = tile + lane * row_bytes;
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
-    stage_step(t_lo, t_lo & 1);
-    CT lcn_lo = left(t_lo, lane, tb_lo, te_lo), lcn_hi = left(t_lo, lane + 32, tb_hi, te_hi);
     for (int t = t_lo; t < t_hi; ++t) {
-        if (t + 1 < t_hi) stage_step(t + 1, (t + 1) & 1);
-        else cp_async_commit();                 // keep one group per step
-        const CT lc_lo = lcn_lo, lc_hi = lcn_hi;
         const bool act_lo = t >= tb_lo && t < te_lo, act_hi = t >= tb_hi && t < te_hi;
         const uint32_t start = (t == tb_lo ? 0x0000FFFFu : 0u) | (t == tb_hi ? 0xFFFF0000u : 0u);
         const int xb = k0 + dx * t;             // x of tile row 0
         const int y = y0 + dy * t;
-        if (t + 1 < t_hi) {
-            lcn_lo = left(t + 1, lane, tb_lo, te_lo);
-            lcn_hi = left(t + 1, lane + 32, tb_hi, te_hi);
-        }
-        cp_async_wait_1();
-        __syncwarp();
-        const CT* seg = stage + (t & 1) * seg_words + seg_offset(t) + lane + (Dp - 1);  // seg[-d] = R(x_lo-d)
-        auto getR = [seg](int d, CT& lo, CT& hi) {
-            lo = seg[-d];
-            hi = seg[32 - d];
-        };
-        const int x_lo = xb + lane, x_hi = xb + lane + 32;
-        uint32_t mx;
-        if (xb >= Dp - 1)
-            mx = wide ? sgm_pixel<false, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
-                      : sgm_pixel<false, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
-        else
-            mx = wide ? sgm_pixel<true, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi)
-                      : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x_lo, x_hi, k, row_lo, row_hi);
-        const size_t pix0 = (size_t)y * W + xb;
+        const size_t pix0 = (size_t)((ptrdiff_t)y * W + xb);
+        const uint8_t* cv_lo = CV + (act_lo ? (pix0 + lane) * Dv : 0);
+        const uint8_t* cv_hi = CV + (act_hi ? (pix0 + lane + 32) * Dv : 0);
+        const uint32_t mx = wide ? sgm_pixel_cv<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
+                                 : sgm_pixel_cv<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
-                     row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
+                         row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
     }
+    (void)stage;
+    (void)seg_words;
+    (void)Dp;
 }
 
-// Unit = 64 rows of a horizontal path (banded census).
+// Unit = 64 rows of a horizontal path.
 template <typename CT, bool WT, bool CP>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job, int first,
                                                     uint32_t tstate, unsigned char* __restrict__ tile,
@@ -571,48 +630,26 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
     const bool act_lo = first + lane < job.num_scanlines;
     const bool act_hi = first + 32 + lane < job.num_scanlines;
-    // Banded census: word (x, y) at ((y / 32) * W + x) * 32 + y % 32, so the 32
-    // rows of a band (first is a multiple of 64) read 128 contiguous bytes per
-    // column and column x-d sits at a constant offset of -32*d words. Bands are
-    // allocated whole; the second band of a unit that has none (H <= first+32)
-    // is read from the first one and its rows stay idle.
-    const size_t band_lo = (size_t)(first >> 5) * W;
-    const size_t band_hi = first + 32 < H ? band_lo + W : band_lo;
-    const CT* __restrict__ CLl = static_cast<const CT*>(pr.census_lt) + band_lo * 32 + lane;
-    const CT* __restrict__ CLh = static_cast<const CT*>(pr.census_lt) + band_hi * 32 + lane;
-    const CT* __restrict__ CRl = static_cast<const CT*>(pr.census_rt) + band_lo * 32 + lane;
-    const CT* __restrict__ CRh = static_cast<const CT*>(pr.census_rt) + band_hi * 32 + lane;
+    // Costs from the pair's cost volume: rows first + lane and first + 32 + lane
+    // at column x (a row past the image reads pixel 0's row, unused).
+    const uint8_t* __restrict__ CV = pr.costs;
     unsigned char* row_lo = tile + lane * row_bytes;
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
     const int x0 = dx > 0 ? 0 : W - 1;
-    CT lcn_lo = CLl[(size_t)x0 * 32], lcn_hi = CLh[(size_t)x0 * 32];
     for (int t = 0; t < W; ++t) {
         const int x = x0 + dx * t;
-        const CT lc_lo = lcn_lo, lc_hi = lcn_hi;
-        if (t + 1 < W) {
-            lcn_lo = CLl[(size_t)(x + dx) * 32];
-            lcn_hi = CLh[(size_t)(x + dx) * 32];
-        }
-        const CT* col_lo = CRl + (size_t)x * 32;   // col[-32*d] = R(x-d, y)
-        const CT* col_hi = CRh + (size_t)x * 32;
-        auto getR = [col_lo, col_hi](int d, CT& lo, CT& hi) {
-            lo = col_lo[-32 * d];
-            hi = col_hi[-32 * d];
-        };
         const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;
-        uint32_t mx;
-        if (x >= Dp - 1)
-            mx = wide ? sgm_pixel<false, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
-                      : sgm_pixel<false, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
-        else
-            mx = wide ? sgm_pixel<true, true, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi)
-                      : sgm_pixel<true, false, CT>(tstate, m, start, lc_lo, lc_hi, getR, x, x, k, row_lo, row_hi);
-        // Rows first..first+63, one vector per row at column x.
         const size_t pix0 = (size_t)first * W + x;
+        const uint8_t* cv_lo = CV + (act_lo ? (pix0 + (size_t)lane * W) * Dv : 0);
+        const uint8_t* cv_hi = CV + (act_hi ? (pix0 + (size_t)(lane + 32) * W) * Dv : 0);
+        const uint32_t mx = wide ? sgm_pixel_cv<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
+                                 : sgm_pixel_cv<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
+        // Rows first..first+63, one vector per row at column x.
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
-                     row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
+                         row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
     }
+    (void)Dp;
     (void)H;
 }
 

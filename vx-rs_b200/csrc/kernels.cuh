@@ -31,6 +31,7 @@ struct PairDev {
     uint16_t* shadow;      // num_paths slabs of H*W*Dp u16
     size_t shadow_stride;  // elements per shadow slab = H*W*Dp
     int wide_slabs;
+    uint8_t* costs;        // scanline-pair batches: the matching-cost volume, H*W vectors of Dv bytes
     uint32_t shadow_cap;   // 0: full shadow; else pool size in vectors
     uint32_t* esc_state;   // [0] vectors taken from the pool, [1] overflow flag
     float* out_f32;        // subpixel (or integer) disparity, pitch in bytes

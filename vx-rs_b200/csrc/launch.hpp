@@ -17,6 +17,11 @@ inline void count_launch(uint64_t n = 1) { g_kernel_launches.fetch_add(n, std::m
 cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
                           int max_ry, bool census64, cudaStream_t stream);
 
+// Matching-cost volume of every pair (cost.cu), for batches run by the
+// scanline-pair kernel: one CTA per image row of the batch.
+cudaError_t launch_costs(const PairDev* d_pairs, int num_pairs, int total_rows, int dp_max, bool census64,
+                         cudaStream_t stream);
+
 // Path aggregation: one persistent launch over `num_units` warp units of every
 // (pair, path) of a batch; warps pull units from `*counter` (zero on entry).
 // dp_max = largest padded disparity count of the batch. One CTA per SM with

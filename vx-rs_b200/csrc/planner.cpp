@@ -61,6 +61,10 @@ size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config
            align_up(shadow_vectors * dp * sizeof(uint16_t));
 }
 
+size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
+    return align_up((size_t)width * height * ((cfg.num_disparities + 15) / 16 * 16));
+}
+
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
     const size_t P = cfg.num_paths;
     const size_t units = P * (((size_t)width + height - 1 + 31) / 32);     // 32-scanline units at most
@@ -243,6 +247,15 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     }
     for (int job = 0; job < (int)pl.jobs.size(); ++job)
         for (int k = 0; k < pl.jobs[job].num_scanlines; k += pl.unit_scanlines) units.push_back({job, k});
+    // The scanline-pair kernel reads the matching costs from a per-pair byte
+    // volume (cost.cu), laid out after every pair's census, slab and shadow
+    // region; the single-scanline kernel forms them from the census words.
+    if (pl.unit_scanlines == kUnitScanlines)
+        for (int i = 0; i < n; ++i) {
+            PairDev& pd = pl.pairs[i];
+            pd.costs = reinterpret_cast<uint8_t*>(data);
+            data += pair_cost_bytes((uint32_t)pd.width, (uint32_t)pd.height, specs[i].cfg);
+        }
 
     // Longest work first inside each persistent launch (LPT order): a unit's
     // cost is its longest scanline times D.
@@ -299,6 +312,8 @@ void bind_plan(Plan& pl, char* base) {
         pd.census_lt = data + reinterpret_cast<size_t>(pd.census_lt);
         pd.census_rt = data + reinterpret_cast<size_t>(pd.census_rt);
         pd.slabs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.slabs));
+        if (pl.unit_scanlines == kUnitScanlines)
+            pd.costs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.costs));
         pd.shadow = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.shadow));
         pd.esc_state = reinterpret_cast<uint32_t*>(base + reinterpret_cast<size_t>(pd.esc_state));
     }
@@ -340,6 +355,10 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     if (ev) record(ev[0]);
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
+    if (pl.unit_scanlines == kUnitScanlines) {
+        e = launch_costs(d_pairs, n, pl.total_rows, pl.dp_max, pl.census64, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cost volume launch");
+    }
     if (ev) record(ev[1]);
     e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream, pl.compact);

@@ -178,7 +178,7 @@ struct vx_sgm_server {
     // all pairs when one pair needs them) and its share of the plan tables.
     static size_t request_bytes(uint32_t w, uint32_t h, const vx_sgm_config& cfg, bool i16, bool compact) {
         return buffer_bytes(w, h, i16) + pair_workspace_bytes(w, h, cfg, 8, compact) +
-               pair_table_bytes_bound(w, h, cfg);
+               pair_cost_bytes(w, h, cfg) + pair_table_bytes_bound(w, h, cfg);
     }
 
     bool host_get(Request* r);

@@ -184,7 +184,8 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
 
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg) {
     if (!cfg) return 0;
-    return pair_workspace_bytes(width, height, *cfg, census_bits(*cfg) > 32 ? 8 : 4);
+    return pair_workspace_bytes(width, height, *cfg, census_bits(*cfg) > 32 ? 8 : 4) +
+           pair_cost_bytes(width, height, *cfg);
 }
 
 vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const vx_image* right,

@@ -123,6 +123,8 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
 size_t pair_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg,
                             size_t census_word_bytes, bool compact_shadow = false);
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg);
+// Bytes of a pair's matching-cost volume (batches run by the scanline-pair kernel).
+size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg);
 // Points plan.pairs at the images and outputs of specs (same sizes and order
 // as the specs the plan was built from).
 void rebind_pointers(Plan& plan, const std::vector<PairSpec>& specs);
