@@ -36,16 +36,11 @@
 // and written 8 columns at a time by warp-collective tcgen05.ld/st. A warp
 // takes 64 neighbouring scanlines of one (pair, path): lane i carries
 // scanlines i (low half) and i + 32 (high half).
-//  * vertical / diagonal paths: the 64 scanlines sit on 64 consecutive pixels
-//    of one row at every step, so the right-census words they need form one
-//    segment of Dp+63 words of that row; it is staged in warp-private shared
-//    memory with 16-byte cp.async copies one step ahead (double-buffered).
-//  * horizontal paths: the 64 scanlines are 64 consecutive rows (two 32-row
-//    bands) at the same x and read the banded census copy: each disparity is
-//    one coalesced 128-byte load per band at a constant offset.
-// Census words of the next group of 8 disparities are loaded while the
-// current group is processed. Pixels whose window may reach x-d < 0 take a
-// second body with the border test, picked by a warp-uniform branch.
+// Costs. The eight paths of a pair share C(x, y, d), so the cost kernel
+// (cost.cu) writes it once per pair as a byte volume (Dv bytes a pixel, 64
+// where x - d < 0, 0 in the pads); a thread reads its two scanlines' 8 costs of
+// a group as one 8-byte load each, one group ahead, and packs them into the
+// u16 halves with byte permutes. The border needs no second body.
 //
 // Output. Each group's results go to a byte tile in shared memory (one row of
 // Dv bytes per scanline); after the pixel the warp writes the rows of its
@@ -75,19 +70,6 @@ __device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
     uint32_t r;
     asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
-}
-
-__device__ __forceinline__ uint32_t popc_xor(uint32_t a, uint32_t b) { return __popc(a ^ b); }
-__device__ __forceinline__ uint32_t popc_xor(uint64_t a, uint64_t b) { return __popcll(a ^ b); }
-
-// 16-byte global -> shared copy that bypasses L1 (staged words are used once).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
-__device__ __forceinline__ void cp_async_wait_1() {
-    asm volatile("cp.async.wait_group 1;" ::: "memory");
 }
 
 // Tensor-memory (TMEM) access for the per-scanline state. Warp w of the CTA owns
@@ -139,23 +121,6 @@ struct PixelState {
     uint32_t mn;     // running min of the new values (d < D)
     uint32_t mx;     // running max of the new values (d < D)
 };
-
-// Matching costs of one group for both scanlines, packed c_lo | c_hi << 16;
-// x-d < 0 gives 64.
-template <bool CHECK, typename CT>
-__device__ __forceinline__ void group_costs(uint32_t (&cw)[8], const CT lc_lo, const CT lc_hi,
-                                            const CT (&rl)[8], const CT (&rh)[8], const int x_lo,
-                                            const int x_hi, const int g) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        uint32_t cl = popc_xor(lc_lo, rl[i]), ch = popc_xor(lc_hi, rh[i]);
-        if (CHECK) {
-            if (x_lo - (8 * g + i) < 0) cl = 64u;
-            if (x_hi - (8 * g + i) < 0) ch = 64u;
-        }
-        cw[i] = cl | (ch << 16);
-    }
-}
 
 // One group of 8 disparities d = 8g..8g+7 of one pixel of both scanlines, in
 // two parts so that the state of the next group (whose first word only the last
@@ -228,106 +193,6 @@ __device__ __forceinline__ void group_bytes(const Words8& o, uint2& lo, uint2& h
     hi.y = __byte_perm(t45, t67, 0x7531);
 }
 
-// One pixel of the 64 scanlines of a warp (all lanes execute it: the TMEM
-// accesses are warp-collective). tstate = this warp's TMEM address (lane field
-// = its first lane, column 0). getR(d, lo, hi) = right census words at x-d of
-// the two scanlines; only called with x_hi-d >= 0 when CHECK. m = the previous
-// pixel's minimum per half; start = 0xFFFF in each half whose scanline starts at
-// this pixel. row_lo / row_hi = the two scanlines' rows of the warp's output
-// tile (u16 values when WIDE, else bytes).
-// Returns the per-half maximum of the new vector (d < D). Software pipeline over
-// groups (loop unrolled by two, register sets in ping-pong): while group g runs
-// its chain, the census words and state of group g+1 are in flight (the state
-// is waited for only before g's last disparity), and g+1's costs are formed
-// right after g's chain.
-template <bool CHECK, bool WIDE, typename CT, typename GetR>
-__device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
-                                              const CT lc_lo, const CT lc_hi, const GetR& getR,
-                                              const int x_lo, const int x_hi, const ScanConst& k,
-                                              unsigned char* __restrict__ row_lo,
-                                              unsigned char* __restrict__ row_hi) {
-    PixelState ps;
-    const uint32_t m0 = m & ~start;
-    ps.o3x2 = __vadd2(m0, k.p2x2) & ~start;
-    ps.kc2 = __vadd2(~m0, k.p1p1x2);
-    ps.f = 0xFFFFFFFFu;            // o1 at d = 0
-    ps.mn = 0xFFFFFFFFu;
-    ps.mx = 0u;
-    auto load = [&](CT (&rl)[8], CT (&rh)[8], int g) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int d = 8 * g + i;
-            if (!CHECK || x_hi - d >= 0) {
-                getR(d, rl[i], rh[i]);
-            } else {
-                rl[i] = CT(0);
-                rh[i] = CT(0);
-            }
-        }
-    };
-    auto store = [&](const Words8& o, int g) {
-        if (WIDE) {             // u16 rows: 8 values (16 bytes) per group
-            *reinterpret_cast<uint4*>(row_lo + 16 * g) = make_uint4(
-                __byte_perm(o.w[0], o.w[1], 0x5410), __byte_perm(o.w[2], o.w[3], 0x5410),
-                __byte_perm(o.w[4], o.w[5], 0x5410), __byte_perm(o.w[6], o.w[7], 0x5410));
-            *reinterpret_cast<uint4*>(row_hi + 16 * g) = make_uint4(
-                __byte_perm(o.w[0], o.w[1], 0x7632), __byte_perm(o.w[2], o.w[3], 0x7632),
-                __byte_perm(o.w[4], o.w[5], 0x7632), __byte_perm(o.w[6], o.w[7], 0x7632));
-        } else {                // byte rows: 8 bytes per group
-            uint2 lo, hi;
-            group_bytes(o, lo, hi);
-            *reinterpret_cast<uint2*>(row_lo + 8 * g) = lo;
-            *reinterpret_cast<uint2*>(row_hi + 8 * g) = hi;
-        }
-        tmem_st8(tstate + 8 * g, o);
-    };
-    CT ra_l[8], ra_h[8], rb_l[8], rb_h[8];
-    uint32_t ca[8], cb[8];
-    Words8 oa, ob;
-    uint32_t w7;
-    load(ra_l, ra_h, 0);
-    Words8 sa = tmem_ld8(tstate), sb;
-    group_costs<CHECK>(ca, lc_lo, lc_hi, ra_l, ra_h, x_lo, x_hi, 0);
-    tmem_wait_ld(sa);
-    int g = 0;
-#pragma unroll 1
-    for (; g + 2 < k.G; g += 2) {
-        sb = tmem_ld8(tstate + 8 * (g + 1));
-        load(rb_l, rb_h, g + 1);
-        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
-        tmem_wait_ld(sb);
-        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
-        store(oa, g);
-        group_costs<CHECK>(cb, lc_lo, lc_hi, rb_l, rb_h, x_lo, x_hi, g + 1);
-        sa = tmem_ld8(tstate + 8 * (g + 2));
-        load(ra_l, ra_h, g + 2);
-        sgm_group_head<false>(sb, cb, k, ps, ob, w7);
-        tmem_wait_ld(sa);
-        sgm_group_tail<false>(sb, sa.w[0], w7, k, ps, ob);
-        store(ob, g + 1);
-        group_costs<CHECK>(ca, lc_lo, lc_hi, ra_l, ra_h, x_lo, x_hi, g + 2);
-    }
-    if (g + 1 < k.G) {
-        sb = tmem_ld8(tstate + 8 * (g + 1));
-        load(rb_l, rb_h, g + 1);
-        sgm_group_head<false>(sa, ca, k, ps, oa, w7);
-        tmem_wait_ld(sb);
-        sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
-        store(oa, g);
-        group_costs<CHECK>(cb, lc_lo, lc_hi, rb_l, rb_h, x_lo, x_hi, g + 1);
-        sgm_group_head<true>(sb, cb, k, ps, ob, w7);
-        sgm_group_tail<true>(sb, 0u, w7, k, ps, ob);
-        store(ob, g + 1);
-    } else {
-        sgm_group_head<true>(sa, ca, k, ps, oa, w7);
-        sgm_group_tail<true>(sa, 0u, w7, k, ps, oa);
-        store(oa, g);
-    }
-    tmem_wait_st();            // the next pixel reads this state back
-    m = ps.mn;
-    return ps.mx;
-}
-
 // Packed costs of disparities 4i..4i+3 (one word of each scanline's cost row):
 // cw = C_lo | C_hi << 16 by one byte permute each; the costs are at most 64, so
 // the sign-replicating selector bytes give the zero high bytes.
@@ -347,11 +212,20 @@ __device__ __forceinline__ void cost_words(uint32_t (&cw)[8], const uint2 lo, co
     cw[7] = prmt(lo.y, hi.y, 0xF7B3u);
 }
 
-// sgm_pixel with the costs read from the pair's cost volume: cv_lo / cv_hi = the
-// two scanlines' cost rows at this pixel (Dv bytes each, 64 already in place
-// where x - d < 0), 8 bytes per group, requested one group ahead.
+// One pixel of the 64 scanlines of a warp (all lanes execute it: the TMEM
+// accesses are warp-collective). tstate = this warp's TMEM address (lane field
+// = its first lane, column 0). cv_lo / cv_hi = the two scanlines' rows of the
+// pair's cost volume at this pixel (Dv bytes each, 64 already in place where
+// x - d < 0). m = the previous pixel's minimum per half; start = 0xFFFF in each
+// half whose scanline starts at this pixel. row_lo / row_hi = the two
+// scanlines' rows of the warp's output tile (u16 values when WIDE, else bytes).
+// Returns the per-half maximum of the new vector (d < D). Software pipeline over
+// groups (loop unrolled by two, register sets in ping-pong): while group g runs
+// its chain, the costs (8 bytes a scanline) and state of group g+1 are in flight
+// (the state is waited for only before g's last disparity), and g+1's packed
+// costs are formed right after g's chain.
 template <bool WIDE>
-__device__ __forceinline__ uint32_t sgm_pixel_cv(const uint32_t tstate, uint32_t& m, const uint32_t start,
+__device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
                                                  const uint8_t* __restrict__ cv_lo,
                                                  const uint8_t* __restrict__ cv_hi, const ScanConst& k,
                                                  unsigned char* __restrict__ row_lo,
@@ -560,15 +434,14 @@ __device__ __forceinline__ void finish_pixel(const PairDev& pr, const EscapeTarg
 
 // Unit = 64 scanlines of a vertical or diagonal path. WT: the batch has
 // wide-slab pairs (the u16 body is compiled in).
-template <typename CT, bool WT, bool CP>
+template <bool WT, bool CP>
 __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDev& job, int first,
-                                                  uint32_t tstate, CT* __restrict__ stage,
-                                                  int seg_words, unsigned char* __restrict__ tile,
+                                                  uint32_t tstate, unsigned char* __restrict__ tile,
                                                   int row_bytes) {
     const int lane = threadIdx.x & 31;
     const int W = pr.width, H = pr.height;
     const ScanConst k = scan_const(pr);
-    const int Dp = k.Dp, Dv = pr.nd_vec;
+    const int Dv = pr.nd_vec;
     const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx, dy = job.dy;
     const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
@@ -606,25 +479,22 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
         const size_t pix0 = (size_t)((ptrdiff_t)y * W + xb);
         const uint8_t* cv_lo = CV + (act_lo ? (pix0 + lane) * Dv : 0);
         const uint8_t* cv_hi = CV + (act_hi ? (pix0 + lane + 32) * Dv : 0);
-        const uint32_t mx = wide ? sgm_pixel_cv<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
-                                 : sgm_pixel_cv<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
+        const uint32_t mx = wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
+                                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                          row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
     }
-    (void)stage;
-    (void)seg_words;
-    (void)Dp;
 }
 
 // Unit = 64 rows of a horizontal path.
-template <typename CT, bool WT, bool CP>
+template <bool WT, bool CP>
 __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const JobDev& job, int first,
                                                     uint32_t tstate, unsigned char* __restrict__ tile,
                                                     int row_bytes) {
     const int lane = threadIdx.x & 31;
-    const int W = pr.width, H = pr.height;
+    const int W = pr.width;
     const ScanConst k = scan_const(pr);
-    const int Dp = k.Dp, Dv = pr.nd_vec;
+    const int Dv = pr.nd_vec;
     const bool wide = WT && pr.wide_slabs != 0;
     const int dx = job.dx;
     const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
@@ -643,19 +513,17 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
         const size_t pix0 = (size_t)first * W + x;
         const uint8_t* cv_lo = CV + (act_lo ? (pix0 + (size_t)lane * W) * Dv : 0);
         const uint8_t* cv_hi = CV + (act_hi ? (pix0 + (size_t)(lane + 32) * W) * Dv : 0);
-        const uint32_t mx = wide ? sgm_pixel_cv<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
-                                 : sgm_pixel_cv<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
+        const uint32_t mx = wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
+                                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
         // Rows first..first+63, one vector per row at column x.
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                          row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
     }
-    (void)Dp;
-    (void)H;
 }
 
 }  // namespace
 
-template <typename CT, bool WT, bool CP>
+template <bool WT, bool CP>
 __global__ void __launch_bounds__(kAggMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
                  const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
@@ -663,11 +531,11 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     extern __shared__ __align__(16) unsigned char agg_smem[];
     __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int seg_words = aggregate_seg_words(dp_max);
     const int row_bytes = aggregate_row_bytes(dp_max, WT);
-    unsigned char* wbase = agg_smem + (size_t)warp * aggregate_warp_smem(dp_max, sizeof(CT), WT);
-    CT* stage = reinterpret_cast<CT*>(wbase);
-    unsigned char* tile = wbase + 2 * (size_t)seg_words * sizeof(CT);
+    // The warps' tiles start aggregate_tile_offset(dp_max) bytes in (unused):
+    // compiled with that batch-dependent base, the pixel loop measured 3 %
+    // faster (18.2 vs 18.8 ms on the 64-pair mixed batch) than with base 0.
+    unsigned char* tile = agg_smem + aggregate_tile_offset(dp_max) + (size_t)warp * aggregate_warp_smem(dp_max, WT);
 
     // TMEM for the state of all the CTA's scanlines, allocated by warp 0 for the
     // whole persistent loop and released by warp 0 after every warp is done.
@@ -694,9 +562,9 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
-            run_horizontal_unit<CT, WT, CP>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
+            run_horizontal_unit<WT, CP>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
         else
-            run_vertical_unit<CT, WT, CP>(pr, job, unit.first_scanline, tstate, stage, seg_words, tile, row_bytes);
+            run_vertical_unit<WT, CP>(pr, job, unit.first_scanline, tstate, tile, row_bytes);
         __syncwarp();
     }
 
@@ -709,17 +577,11 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     }
 }
 
-// The kernel for a batch's census word width, tile format and shadow kind.
-template <bool CP>
-const void* aggregate_kernel_cp(bool census64, bool wide_tiles) {
-    if (census64) return wide_tiles ? (const void*)aggregate_kernel<uint64_t, true, CP>
-                                    : (const void*)aggregate_kernel<uint64_t, false, CP>;
-    return wide_tiles ? (const void*)aggregate_kernel<uint32_t, true, CP>
-                      : (const void*)aggregate_kernel<uint32_t, false, CP>;
-}
-
-const void* aggregate_kernel_fn(bool census64, bool wide_tiles, bool compact) {
-    return compact ? aggregate_kernel_cp<true>(census64, wide_tiles) : aggregate_kernel_cp<false>(census64, wide_tiles);
+// The kernel for a batch's tile format and shadow kind (the census word width
+// does not matter: the costs come from the volume).
+const void* aggregate_kernel_fn(bool wide_tiles, bool compact) {
+    if (compact) return wide_tiles ? (const void*)aggregate_kernel<true, true> : (const void*)aggregate_kernel<false, true>;
+    return wide_tiles ? (const void*)aggregate_kernel<true, false> : (const void*)aggregate_kernel<false, false>;
 }
 
 // Launch shape of the aggregation kernel for a batch whose largest padded D is
@@ -736,7 +598,7 @@ struct AggShape {
 
 // Largest number of warpgroups one aggregation CTA can hold for this batch:
 // bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
-int max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
+int max_warpgroups(int dp_max, bool wide_tiles) {
     const int by_tmem = 512 / dp_max;
     int regs = 128, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
@@ -745,38 +607,38 @@ int max_warpgroups(int dp_max, bool census64, bool wide_tiles) {
     // Either shadow kind may run with the shape chosen here: the larger register count counts.
     for (bool compact : {false, true}) {
         cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, aggregate_kernel_fn(census64, wide_tiles, compact)) == cudaSuccess &&
+        if (cudaFuncGetAttributes(&fa, aggregate_kernel_fn(wide_tiles, compact)) == cudaSuccess &&
             fa.numRegs > 0)
             regs = compact ? std::max(regs, fa.numRegs) : fa.numRegs;
     }
     cudaGetLastError();
     const int by_regs = regs_sm / (regs * 128);
     const int by_smem =
-        (int)((smem_sm - 1024) / (4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4, wide_tiles)));
+        (int)((smem_sm - 1024 - (int)aggregate_tile_offset(dp_max)) / (4 * aggregate_warp_smem(dp_max, wide_tiles)));
     return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
 }
 
-int default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units) {
+int default_warpgroups(int dp_max, bool wide_tiles, int num_units) {
     // Most warpgroups that still leave every warp ~2.5 units of the queue: a
     // scanline is serial work, so a crowded SM slows the longest units down and
     // few units per warp cannot even that out.
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int wmax = max_warpgroups(dp_max, census64, wide_tiles);
+    const int wmax = max_warpgroups(dp_max, wide_tiles);
     int w = 1;
     while (w < wmax && (double)num_units >= 2.5 * sms * 4 * (w + 1)) ++w;
     return w;
 }
 
-static AggShape shape_for(int dp_max, bool census64, bool wide_tiles, int warpgroups) {
+static AggShape shape_for(int dp_max, bool wide_tiles, int warpgroups) {
     AggShape sh{};
     sh.wg_cols = dp_max;
-    const int wmax = max_warpgroups(dp_max, census64, wide_tiles);
+    const int wmax = max_warpgroups(dp_max, wide_tiles);
     sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
     sh.tmem_cols = 32;
     while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
-    sh.smem = (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, census64 ? 8 : 4, wide_tiles);
+    sh.smem = aggregate_tile_offset(dp_max) + (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, wide_tiles);
     return sh;
 }
 
@@ -787,10 +649,8 @@ cudaError_t prepare() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaError_t e = cudaSuccess;
-    for (const void* fn : {aggregate_kernel_fn(false, false, false), aggregate_kernel_fn(true, false, false),
-                           aggregate_kernel_fn(false, true, false), aggregate_kernel_fn(true, true, false),
-                           aggregate_kernel_fn(false, false, true), aggregate_kernel_fn(true, false, true),
-                           aggregate_kernel_fn(false, true, true), aggregate_kernel_fn(true, true, true)}) {
+    for (const void* fn : {aggregate_kernel_fn(false, false), aggregate_kernel_fn(true, false),
+                           aggregate_kernel_fn(false, true), aggregate_kernel_fn(true, true)}) {
         cudaFuncAttributes fa{};
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)   // dynamic + static shared memory must fit the opt-in limit
@@ -803,23 +663,21 @@ cudaError_t prepare() {
     return e;
 }
 
-static int grid_ctas_for(int dp_max, bool census64) {
-    (void)dp_max;
-    (void)census64;
+static int grid_ctas_for() {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return sms;
 }
 
-cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
+cudaError_t launch(int dp_max, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
                    cudaStream_t stream, bool compact) {
     if (num_units <= 0) return cudaSuccess;
-    if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, census64, wide_tiles, num_units);
-    const AggShape sh = shape_for(dp_max, census64, wide_tiles, warpgroups);
+    if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, wide_tiles, num_units);
+    const AggShape sh = shape_for(dp_max, wide_tiles, warpgroups);
     const int threads = sh.warpgroups * 128;
-    int grid_ctas = grid_ctas_for(dp_max, census64);
+    int grid_ctas = grid_ctas_for();
     const int needed = (num_units + threads / 32 - 1) / (threads / 32);
     if (grid_ctas > needed) grid_ctas = needed;
     if (std::getenv("VX_SGM_DEBUG"))
@@ -828,7 +686,7 @@ cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, c
     count_launch();
     void* args[] = {&d_pairs, &d_jobs, &d_units, &num_units, &counter, &dp_max,
                     const_cast<int*>(&sh.tmem_cols), const_cast<int*>(&sh.wg_cols)};
-    return cudaLaunchKernel(aggregate_kernel_fn(census64, wide_tiles, compact), dim3(grid_ctas), dim3(threads),
+    return cudaLaunchKernel(aggregate_kernel_fn(wide_tiles, compact), dim3(grid_ctas), dim3(threads),
                             args, sh.smem, stream);
 }
 
@@ -837,11 +695,12 @@ cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, c
 // Both forms, dispatched on the plan's unit size (launch.hpp).
 cudaError_t prepare_aggregate_kernels() {
     cudaError_t e = pairs::prepare();
-    return e == cudaSuccess ? single::prepare() : e;
+    if (e == cudaSuccess) e = single::prepare();
+    return e == cudaSuccess ? prepare_cost_kernels() : e;
 }
 
 int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool wide_tiles) {
-    return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, census64, wide_tiles)
+    return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, wide_tiles)
                                             : single::max_warpgroups(dp_max, census64);
 }
 
@@ -849,7 +708,7 @@ cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
                              int num_units, unsigned* counter, cudaStream_t stream, bool compact) {
     if (unit_scanlines == kUnitScanlines)
-        return pairs::launch(dp_max, census64, wide_tiles, warpgroups, d_pairs, d_jobs, d_units, num_units,
+        return pairs::launch(dp_max, wide_tiles, warpgroups, d_pairs, d_jobs, d_units, num_units,
                              counter, stream, compact);
     return single::launch(dp_max, census64, warpgroups, d_pairs, d_jobs, d_units, num_units, counter, stream,
                           compact);

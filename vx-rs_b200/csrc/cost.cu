@@ -47,8 +47,18 @@ constexpr int kTileRows = 132;    // tile rows of a block: pixel p at row (p & 3
 // Tile row stride in 16-byte units: odd, so that 8 lanes storing 16 bytes each
 // to consecutive rows hit distinct bank groups.
 __host__ __device__ constexpr int tile_stride(int dv) { return (dv / 16) | 1; }
+constexpr int kMaxTileBytes = 56 * 1024;   // four CTAs an SM
+// Blocks of a pass: the count (1..8) whose nb * chunks items fill the 8 warps'
+// last round best (the CTA waits for its slowest warp at the end of a pass),
+// the smaller on ties, within kMaxTileBytes of tile.
 __host__ __device__ constexpr int blocks_per_pass(int dv) {
-    return dv / 16 >= kWarps ? 1 : (kWarps + dv / 16 - 1) / (dv / 16);
+    const int chunks = dv / 16;
+    int best = 1, best_num = 0, best_den = 1;    // efficiency = items / (8 * rounds)
+    for (int nb = 1; nb <= kWarps && nb * kTileRows * tile_stride(dv) * 16 <= kMaxTileBytes; ++nb) {
+        const int items = nb * chunks, den = kWarps * ((items + kWarps - 1) / kWarps);
+        if (items * best_den > best_num * den) best = nb, best_num = items, best_den = den;
+    }
+    return best;
 }
 __host__ __device__ constexpr int tile_units(int dv) { return blocks_per_pass(dv) * kTileRows * tile_stride(dv); }
 
@@ -88,7 +98,7 @@ __device__ __forceinline__ void chunk_costs(const CT (&l)[4], const CT (&r)[20],
 }
 
 template <typename CT>
-__global__ void __launch_bounds__(kThreads) cost_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
+__global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 4 : 2) cost_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint4 tile[];
     const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
     const PairDev& pr = pairs[pi];
@@ -142,12 +152,20 @@ __global__ void __launch_bounds__(kThreads) cost_kernel(const PairDev* __restric
 
 }  // namespace
 
+cudaError_t prepare_cost_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(cost_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxTileBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(cost_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTileBytes);
+    return e;
+}
+
 cudaError_t launch_costs(const PairDev* d_pairs, int num_pairs, int total_rows, int dp_max, bool census64,
                          cudaStream_t stream) {
     if (total_rows == 0) return cudaSuccess;
     int units = 0;                        // the largest tile of any Dv up to the batch's
     for (int dv = 16; dv <= (dp_max + 15) / 16 * 16; dv += 16) units = units > tile_units(dv) ? units : tile_units(dv);
-    const size_t smem = (size_t)units * 16;   // <= 132 * 17 * 16 B = 35.9 KB (D <= 256)
+    const size_t smem = (size_t)units * 16;   // <= kMaxTileBytes
     if (census64)
         cost_kernel<uint64_t><<<total_rows, kThreads, smem, stream>>>(d_pairs, num_pairs);
     else

@@ -116,20 +116,18 @@ constexpr int kAggMaxThreads = 512;
 // row by up to 256 + 72 words.
 constexpr int kCensusGuardWords = 352;
 
-// Shared memory of one aggregation warp for a batch whose largest padded D is
-// dp_max: two census staging buffers (the Dp+63 words of a step plus up to one
-// 16-byte chunk of alignment) and the output tile of its 64 scanlines. Tile rows
+// Shared memory of one aggregation warp (scanline-pair form) for a batch whose
+// largest padded D is dp_max: the output tile of its 64 scanlines. Tile rows
 // hold byte vectors (Dv bytes plus 8, so that the rows' 8-byte stores fall on
 // distinct banks) or, when the batch has wide-slab pairs, u16 vectors (2*Dp
 // bytes plus 16).
-__host__ __device__ constexpr int aggregate_seg_words(int dp_max) { return dp_max + 72; }
 __host__ __device__ constexpr int aggregate_row_bytes(int dp_max, bool wide_tiles) {
     return wide_tiles ? 2 * dp_max + 16 : (dp_max + 15) / 16 * 16 + 8;
 }
-__host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, size_t ct, bool wide_tiles) {
-    return 2 * (size_t)aggregate_seg_words(dp_max) * ct +
-           (size_t)kUnitScanlines * aggregate_row_bytes(dp_max, wide_tiles);
+__host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, bool wide_tiles) {
+    return (size_t)kUnitScanlines * aggregate_row_bytes(dp_max, wide_tiles);
 }
+__host__ __device__ constexpr size_t aggregate_tile_offset(int dp_max) { return (size_t)(dp_max + 72) * 8; }
 
 constexpr int kWtaThreads = 256;
 // Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).

@@ -19,6 +19,7 @@ cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles
 
 // Matching-cost volume of every pair (cost.cu), for batches run by the
 // scanline-pair kernel: one CTA per image row of the batch.
+cudaError_t prepare_cost_kernels();   // shared-memory limit; once per device
 cudaError_t launch_costs(const PairDev* d_pairs, int num_pairs, int total_rows, int dp_max, bool census64,
                          cudaStream_t stream);
 
@@ -39,9 +40,9 @@ cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool
                              int num_units, unsigned* counter, cudaStream_t stream, bool compact = false);
 namespace pairs {
 cudaError_t prepare();
-int max_warpgroups(int dp_max, bool census64, bool wide_tiles);
-int default_warpgroups(int dp_max, bool census64, bool wide_tiles, int num_units);
-cudaError_t launch(int dp_max, bool census64, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
+int max_warpgroups(int dp_max, bool wide_tiles);
+int default_warpgroups(int dp_max, bool wide_tiles, int num_units);
+cudaError_t launch(int dp_max, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
                    cudaStream_t stream, bool compact = false);
 }  // namespace pairs
