@@ -99,18 +99,35 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
         v[p] = act ? __ldcs(reinterpret_cast<const uint2*>(base + rv.slab_stride * p)) : make_uint2(0u, 0u);
     constexpr uint32_t M = 0x00FF00FFu;
     uint32_t a[4] = {0u, 0u, 0u, 0u};               // (0,2) (1,3) (4,6) (5,7)
-    unsigned em = 0u;
 #pragma unroll
     for (int p = 0; p < NP; p += 2) {
         a[0] += (v[p].x & M) + (v[p + 1].x & M);
         a[1] += __byte_perm(v[p].x, 0u, 0x4341) + __byte_perm(v[p + 1].x, 0u, 0x4341);
         a[2] += (v[p].y & M) + (v[p + 1].y & M);
         a[3] += __byte_perm(v[p].y, 0u, 0x4341) + __byte_perm(v[p + 1].y, 0u, 0x4341);
-        em |= ((v[p].x & 0xFFu) == 0xFFu ? 1u : 0u) << p;
-        em |= ((v[p + 1].x & 0xFFu) == 0xFFu ? 1u : 0u) << (p + 1);
     }
-    em = __shfl_sync(kFull, em, lead);              // the pixel's markers (its lane c = 0)
-    if (__any_sync(kFull, em != 0u)) {
+    // Any marker among the paths: their bytes 0 gathered four to a word (byte
+    // permutes); a byte 0xFF is a zero byte of the complement, which the
+    // borrow test (~g - 0x01..01) & g & 0x80..80 finds exactly. Only the
+    // pixel's lane c = 0 holds markers; exact per-path flags are formed in the
+    // rare branch.
+    uint32_t ff = 0u;
+#pragma unroll
+    for (int p = 0; p < NP; p += 4) {
+        uint32_t g;
+        if (NP == 2) {
+            g = __byte_perm(v[p].x, v[p + 1].x, 0x4040);
+        } else {
+            g = __byte_perm(__byte_perm(v[p].x, v[p + 1].x, 0x0040), __byte_perm(v[p + 2].x, v[p + 3].x, 0x0040),
+                            0x5410);
+        }
+        ff |= (~g - 0x01010101u) & g & 0x80808080u;
+    }
+    if (__any_sync(kFull, c == 0 && ff != 0u)) {
+        unsigned em = 0u;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) em |= ((v[p].x & 0xFFu) == 0xFFu ? 1u : 0u) << p;
+        em = __shfl_sync(kFull, em, lead);          // the pixel's markers (its lane c = 0)
         // Every escaped byte vector out first (plain subtractions are exact only
         // while no half has wrapped), then the shadow values in.
 #pragma unroll
@@ -164,8 +181,8 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const bool lr = pr.lr_check != 0;
 
     uint32_t* right_key = smem;                               // W keys (LR only)
-    int* best_d = reinterpret_cast<int*>(smem + W);           // W
-    float* disp = reinterpret_cast<float*>(smem + 2 * W);     // W
+    uint32_t* best_key = smem + W;                            // W: S(bd) << 8 | bd
+    uint32_t* nbr = smem + 2 * W;                             // W: S(bd-1) | S(bd+1) << 16
 
     if (lr)
         for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
@@ -224,14 +241,8 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
                 if (j < nr) atomicMin(&right_key[xr - j], key[j]);
         }
         if (c == 0 && x < W) {
-            float v = (float)bd;
-            if (subpixel && bd > 0 && bd < D - 1) {
-                const float f0 = (float)c0, f1 = (float)(best >> 8), f2 = (float)c2;
-                const float denom = 2.0f * (f0 + f2 - 2.0f * f1);
-                if (fabsf(denom) > 1e-6f) v = __fadd_rn(v, __fdiv_rn(f0 - f2, denom));
-            }
-            best_d[x] = bd;
-            disp[x] = v;
+            best_key[x] = best;
+            nbr[x] = c0 | (c2 << 16);
         }
     }
     __syncthreads();
@@ -244,18 +255,28 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         ? reinterpret_cast<float*>(reinterpret_cast<char*>(pr.out_depth) + (size_t)y * pr.out_depth_pitch)
         : nullptr;
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
-        const int dl = best_d[x];
+        // The parabola step here, one pixel a thread, rather than in the lanes
+        // c = 0 of the disparity loop.
+        const uint32_t best = best_key[x];
+        const int dl = (int)(best & 0xFFu);
+        float v = (float)dl;
+        if (subpixel && dl > 0 && dl < D - 1) {
+            const uint32_t n = nbr[x];
+            const float f0 = (float)(n & 0xFFFFu), f1 = (float)(best >> 8), f2 = (float)(n >> 16);
+            const float denom = 2.0f * (f0 + f2 - 2.0f * f1);
+            if (fabsf(denom) > 1e-6f) v = __fadd_rn(v, __fdiv_rn(f0 - f2, denom));
+        }
         bool valid = true;
         if (lr) {
             const int xr = x - dl;
             valid = xr >= 0 && abs(dl - (int)(right_key[xr] & 0xFFu)) <= pr.lr_tolerance;
         }
-        out[x] = valid ? disp[x] : pr.invalid_value;
+        out[x] = valid ? v : pr.invalid_value;
         if (out_i) out_i[x] = (int16_t)(valid ? dl : -1);
         // Depth epilogue: depth = fx * baseline / disparity (the conversion the
         // reference leaves to its caller, kernels/sgm.rs:284-286).
         if (out_z)
-            out_z[x] = (valid && disp[x] > 0.0f) ? __fdiv_rn(pr.depth_scale, disp[x]) : pr.depth_invalid;
+            out_z[x] = (valid && v > 0.0f) ? __fdiv_rn(pr.depth_scale, v) : pr.depth_invalid;
     }
 }
 
