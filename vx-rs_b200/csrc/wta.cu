@@ -223,9 +223,14 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         }
         const int nb = (act ? D : 0) - (int)d0;     // this lane's keys j < nb take part
         uint32_t best = 0xFFFFFFFFu;
+        if (nb >= 8) {                              // no pads: three-way minima
+            best = min(__vimin3_u32(key[0], key[1], key[2]), __vimin3_u32(key[3], key[4], key[5]));
+            best = __vimin3_u32(best, key[6], key[7]);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (j < nb) best = min(best, key[j]);
+            for (int j = 0; j < 8; ++j)
+                if (j < nb) best = min(best, key[j]);
+        }
         for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
         const int bd = (int)(best & 0xFFu);
         // S(bd-1) and S(bd+1) from the lanes that hold them (only used when
@@ -236,9 +241,14 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
         if (lr && act) {
             const int xr = x - 8 * c;               // right-view column of this lane's d = 8c
             const int nr = min(D - 8 * c, xr + 1);  // j < nr: d < D and x - d >= 0
+            if (nr >= 8) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                if (j < nr) atomicMin(&right_key[xr - j], key[j]);
+                for (int j = 0; j < 8; ++j) atomicMin(&right_key[xr - j], key[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (j < nr) atomicMin(&right_key[xr - j], key[j]);
+            }
         }
         if (c == 0 && x < W) {
             best_key[x] = best;
