@@ -163,10 +163,11 @@ def cpu_reference_rate(items, pairs, max_pd, threads):
     return done_pd / secs / 1e9, n, done_pd, secs
 
 
-# DRAM bytes (read + write) one aggregation launch of the 64-pair workload moved
-# per path-pixel-disparity: 31.75 GB over 8 x 3.738 G path-pd (ncu capture,
-# dram__bytes_read.sum 1.80 GB + dram__bytes_write.sum 29.95 GB).
-AGG_DRAM_BYTES_PER_PATH_PD = 31.75e9 / (8 * 3737760000)
+# DRAM bytes (read + write) one aggregation launch (scanline-pair form) of the
+# 64-pair workload moved per path-pixel-disparity: 55.79 GB over 8 x 3.738 G
+# path-pd (ncu capture, dram__bytes_read.sum 25.83 GB of cost-volume reads, the
+# rest of the 29.90 GB served by L2, + dram__bytes_write.sum 29.96 GB of slabs).
+AGG_DRAM_BYTES_PER_PATH_PD = 55.79e9 / (8 * 3737760000)
 
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
@@ -490,14 +491,15 @@ def run_single_pair(args, local_rank):
         e1.record(stream)
         e1.synchronize()
         lat.append(e0.elapsed_time(e1))
-    census_ms, agg_ms, wta_ms = ctx.stage_times()
+    census_ms, costs_ms, agg_ms, wta_ms = ctx.stage_times_detail()
     ctx.enable_stage_timing(False)
     pd = w * h * d
     print(json.dumps({"config": "single pair", "pair": f"{w}x{h} D={d}, {paths} paths", "calls": args.steps,
                       "value": pd / (float(np.mean(lat)) * 1e-3) / 1e9, "unit": UNIT,
                       "latency_ms_p50": float(np.percentile(lat, 50)),
                       "latency_ms_p99": float(np.percentile(lat, 99)),
-                      "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms}}), flush=True)
+                      "stages_ms": {"census": census_ms, "costs": costs_ms, "aggregate": agg_ms,
+                                    "wta": wta_ms}}), flush=True)
 
 
 def run_reference(args, rank, world):
@@ -645,7 +647,7 @@ def main():
         e1.record(stream)
         e1.synchronize()
     launches = vx_sgm.kernel_launch_count() - launches0
-    census_ms, agg_ms, wta_ms = ctx.stage_times()
+    census_ms, costs_ms, agg_ms, wta_ms = ctx.stage_times_detail()
     ctx.enable_stage_timing(False)
     torch.cuda.synchronize()
     barrier()
@@ -655,7 +657,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms,
                               "workload": args.workload, "stages_ms": {
-                                  "census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
+                                  "census": census_ms, "costs": costs_ms, "aggregate": agg_ms, "wta": wta_ms},
                               "autotuned_warpgroups": tuned_wg, "autotune_aggregate_ms": tuned_ms,
                               "autotuned_unit_scanlines": tuned_unit,
                               "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
@@ -759,17 +761,24 @@ def main():
         peak_src = "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    # Algorithmic bytes (P2 = 120: byte path slabs, Dv = D rounded up to 16):
-    # aggregation writes one byte per path-pixel-disparity and reads the left
-    # and right census word of every pixel once per path; the pipeline adds the
-    # census pass (images in, row-major and banded planes out) and the WTA
-    # (slabs in, f32 + i16 disparities out).
+    # Algorithmic bytes (P2 = 120: byte path slabs, Dv = D rounded up to 16).
+    # Scanline-pair form: the cost kernel reads the left and right census and
+    # writes the cost volume (one byte per pixel-disparity); the aggregation
+    # reads the volume once per path and writes one byte per path-pd.
+    # Single-scanline form: the aggregation reads the census words once per path
+    # instead. The pipeline adds the census pass (images in, row-major and banded
+    # planes out) and the WTA (slabs in, f32 + i16 disparities out).
     census_bytes = 4  # 5x5 census: one u32 word per pixel
     dv = lambda d: (d + 15) // 16 * 16
-    agg_bytes = sum(8 * (w * h * dv(d) + 2 * w * h * census_bytes) for (w, h, d, _) in items)
+    if tuned_unit == 64:
+        agg_bytes = sum(8 * 2 * w * h * dv(d) for (w, h, d, _) in items)
+        costs_bytes = sum(w * h * dv(d) + 2 * w * h * census_bytes for (w, h, d, _) in items)
+    else:
+        agg_bytes = sum(8 * (w * h * dv(d) + 2 * w * h * census_bytes) for (w, h, d, _) in items)
+        costs_bytes = 0
     agg_gbs = agg_bytes / (agg_ms * 1e-3) / 1e9
-    pipeline_bytes = sum(2 * 8 * w * h * dv(d) + 2 * w * h + 4 * w * h * census_bytes + 6 * w * h
-                         for (w, h, d, _) in items)
+    pipeline_bytes = agg_bytes + costs_bytes + sum(8 * w * h * dv(d) + 6 * w * h + 2 * w * h + 4 * w * h * census_bytes
+                                                   for (w, h, d, _) in items)
     slab_bytes = sum(8 * w * h * dv(d) for (w, h, d, _) in items)
 
     result = {
@@ -792,7 +801,7 @@ def main():
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "copies": "pinned host buffers, every step; double-buffered on two copy streams, "
                           "overlapping the neighbouring steps' batches"},
-        "stages_ms": {"census": census_ms, "aggregate": agg_ms, "wta": wta_ms},
+        "stages_ms": {"census": census_ms, "costs": costs_ms, "aggregate": agg_ms, "wta": wta_ms},
         "roofline": {"bound": "hbm", "kernel": "path aggregation (all pairs, all paths)",
                      "achieved": agg_gbs, "peak": peak, "unit": "GB/s", "frac": agg_gbs / peak,
                      "peak_source": peak_src,
@@ -800,8 +809,9 @@ def main():
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                        "aggregation launch of this workload, per path-pixel-disparity",
                      "algorithmic_bytes_per_launch": agg_bytes,
-                     "issue_bound": "the recurrence is integer-issue bound (about 19 instructions "
-                                    "per path-pixel-disparity); HBM is not its limit"},
+                     "bound_note": "the recurrence is latency-bound (two warps a scheduler: tensor "
+                                   "memory holds two warpgroups' state at D <= 256; each pixel's "
+                                   "chain is serial over d); HBM is not its limit"},
         "pipeline_roofline": {"bytes_per_step": pipeline_bytes,
                               "achieved_gbs": pipeline_bytes / (ms * 1e-3) / 1e9,
                               "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / peak},

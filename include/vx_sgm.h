@@ -223,12 +223,17 @@ vx_status vx_sgm_debug_dump(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, cons
 /* Per-stage device timing (no reference counterpart; the reference only times
  * whole calls with Instant, examples/depth_to_cloud_demo.rs:48-53). Enabling
  * (re)starts a record: every later batch records CUDA events on its stream
- * around its census, path aggregation and WTA launches (the first 256 batches
- * are kept). vx_ctx_stage_times waits for those events and returns the mean
- * duration per batch of each stage in milliseconds (VX_ERR_NOT_READY when no
- * batch ran since timing was enabled). */
+ * around its census, cost-volume, path aggregation and WTA launches (the first
+ * 256 batches are kept; batches run by the single-scanline kernel have no
+ * cost-volume launch, its time is 0). vx_ctx_stage_times waits for those
+ * events and returns the mean duration per batch of each stage in
+ * milliseconds, census_ms covering the census and the cost volume
+ * (VX_ERR_NOT_READY when no batch ran since timing was enabled);
+ * vx_ctx_stage_times_detail returns the cost volume on its own. */
 vx_status vx_ctx_enable_stage_timing(vx_ctx* ctx, int enable);
 vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms, float* wta_ms);
+vx_status vx_ctx_stage_times_detail(vx_ctx* ctx, float* census_ms, float* costs_ms, float* aggregate_ms,
+                                    float* wta_ms);
 
 /* ---- Serving loop (no reference counterpart) ----------------------------
  * Continuous batching of stereo requests of any size and config under a

@@ -89,3 +89,35 @@ def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
         other.tuning_load(os.path.join(tmp_path, "missing.json"))
     other.close()
     sgm.close()
+
+
+@pytest.mark.parametrize("form", ["pairs", "single"])
+def test_stage_times_through_graphs(gpu_ctx, monkeypatch, form):
+    """Stage timing of graph-launched batches: every stage's events are recorded;
+    the cost-volume stage exists in the scanline-pair form only, and the launch
+    counter counts its kernel."""
+    monkeypatch.setenv("VX_SGM_AGG_FORM", form)
+    pairs, cfgs = _pairs(4, 13)
+    plain = vx_sgm.SGMStereo(gpu_ctx)
+    want = run_batch(gpu_ctx, plain, pairs, cfgs)
+    plain.close()
+    sgm = vx_sgm.SGMStereo(gpu_ctx)
+    sgm.set_graph_cache(2)
+    tl, tr, of, oi = _textures(gpu_ctx, pairs)
+    sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)   # captures the bucket's graph
+    gpu_ctx.enable_stage_timing(True)
+    before = vx_sgm.kernel_launch_count()
+    for _ in range(2):
+        sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)
+    launches = vx_sgm.kernel_launch_count() - before
+    census, costs, agg, wta = gpu_ctx.stage_times_detail()
+    gpu_ctx.enable_stage_timing(False)
+    assert census > 0 and agg > 0 and wta > 0
+    if form == "pairs":
+        assert costs > 0 and launches == 2 * 4
+    else:
+        assert costs < 0.01 and launches == 2 * 3
+    for f, i, ww in zip(of, oi, want):
+        assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what=f"graph {form}")
+    sgm.set_graph_cache(0)
+    sgm.close()

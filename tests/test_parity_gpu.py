@@ -126,4 +126,4 @@ def test_kernels_actually_launch(gpu_ctx, sgm):
     L, R, _ = vx_sgm.synth_pair(0, 64, 32, 1, 20, 3)
     before = vx_sgm.kernel_launch_count()
     run_pair(gpu_ctx, sgm, L, R, vx_sgm.SGMStereoConfig(num_disparities=32, num_paths=8))
-    assert vx_sgm.kernel_launch_count() - before >= 3  # census, aggregation, WTA
+    assert vx_sgm.kernel_launch_count() - before >= 3  # census, [cost volume,] aggregation, WTA

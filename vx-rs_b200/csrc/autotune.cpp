@@ -69,7 +69,7 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
     for (uint32_t i = 0; i < n; ++i)
         specs[i] = {left[i], right[i], out_f32[i], out_i16 ? out_i16[i] : nullptr, cfgs[i]};
     DeviceGuard g(ctx->device);
-    cudaEvent_t ev[4] = {};
+    cudaEvent_t ev[vx_ctx::kStageEvents] = {};
     for (auto& x : ev) cudaEventCreate(&x);
     vx_status st = VX_OK;
     int best_w = 0, best_unit = 0;
@@ -100,9 +100,9 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
             for (uint32_t it = 0; it <= iterations && st == VX_OK; ++it) {  // first run untimed
                 st = run_plan(plan, ws, ctx->stream, ev, w);
                 if (st != VX_OK) break;
-                e = cudaEventSynchronize(ev[3]);
+                e = cudaEventSynchronize(ev[4]);
                 float ms = 0.0f;
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[1], ev[2]);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[2], ev[3]);
                 if (e != cudaSuccess) st = cuda_fail(e, "autotune timing");
                 if (it > 0) total += ms;
             }

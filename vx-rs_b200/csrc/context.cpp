@@ -109,7 +109,7 @@ vx_status vx_ctx_enable_stage_timing(vx_ctx* ctx, int enable) {
     DeviceGuard g(ctx->device);
     std::lock_guard<std::mutex> lk(ctx->timing_mu);
     if (enable && ctx->stage_ev.empty()) {
-        ctx->stage_ev.resize(vx_ctx::kTimingSlots * 4);
+        ctx->stage_ev.resize(vx_ctx::kTimingSlots * vx_ctx::kStageEvents);
         for (auto& ev : ctx->stage_ev) {
             cudaError_t e = cudaEventCreate(&ev);
             if (e != cudaSuccess) return cuda_fail(e, "creating timing events");
@@ -123,23 +123,25 @@ vx_status vx_ctx_enable_stage_timing(vx_ctx* ctx, int enable) {
 cudaEvent_t* vx_ctx::next_timing_slot() {
     std::lock_guard<std::mutex> lk(timing_mu);
     if (!timing || stage_ev.empty()) return nullptr;
-    cudaEvent_t* slot = &stage_ev[(size_t)(timing_batches % kTimingSlots) * 4];
+    cudaEvent_t* slot = &stage_ev[(size_t)(timing_batches % kTimingSlots) * kStageEvents];
     ++timing_batches;
     return slot;
 }
 
-vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms, float* wta_ms) {
+vx_status vx_ctx_stage_times_detail(vx_ctx* ctx, float* census_ms, float* costs_ms, float* aggregate_ms,
+                                    float* wta_ms) {
     if (!ctx) return fail(VX_ERR_INVALID_ARGUMENT, "vx_ctx_stage_times: ctx is NULL");
     DeviceGuard g(ctx->device);
     std::lock_guard<std::mutex> lk(ctx->timing_mu);
     const int n = std::min(ctx->timing_batches, (int)vx_ctx::kTimingSlots);
     if (ctx->stage_ev.empty() || n == 0)
         return fail(VX_ERR_NOT_READY, "vx_ctx_stage_times: no timed batch since timing was enabled");
-    double sum[3] = {0, 0, 0};
+    constexpr int kStages = vx_ctx::kStageEvents - 1;
+    double sum[kStages] = {};
     for (int b = 0; b < n; ++b) {
-        cudaEvent_t* ev = &ctx->stage_ev[(size_t)b * 4];
-        cudaError_t e = cudaEventSynchronize(ev[3]);
-        for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+        cudaEvent_t* ev = &ctx->stage_ev[(size_t)b * vx_ctx::kStageEvents];
+        cudaError_t e = cudaEventSynchronize(ev[kStages]);
+        for (int i = 0; i < kStages && e == cudaSuccess; ++i) {
             float t = 0;
             e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
             sum[i] += t;
@@ -147,9 +149,17 @@ vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms,
         if (e != cudaSuccess) return cuda_fail(e, "reading stage timing events");
     }
     if (census_ms) *census_ms = (float)(sum[0] / n);
-    if (aggregate_ms) *aggregate_ms = (float)(sum[1] / n);
-    if (wta_ms) *wta_ms = (float)(sum[2] / n);
+    if (costs_ms) *costs_ms = (float)(sum[1] / n);
+    if (aggregate_ms) *aggregate_ms = (float)(sum[2] / n);
+    if (wta_ms) *wta_ms = (float)(sum[3] / n);
     return VX_OK;
+}
+
+vx_status vx_ctx_stage_times(vx_ctx* ctx, float* census_ms, float* aggregate_ms, float* wta_ms) {
+    float census = 0, costs = 0;
+    vx_status st = vx_ctx_stage_times_detail(ctx, &census, &costs, aggregate_ms, wta_ms);
+    if (st == VX_OK && census_ms) *census_ms = census + costs;
+    return st;
 }
 
 vx_status vx_ctx_set_workspace_limit(vx_ctx* ctx, size_t bytes) {

@@ -84,7 +84,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
             bind_plan(e->plan, e->ws);
             st = upload_plan(e->plan, e->ws, stream, false);
         }
-        for (int i = 0; i < 4 && st == VX_OK; ++i) {
+        for (int i = 0; i < vx_ctx::kStageEvents && st == VX_OK; ++i) {
             err = cudaEventCreate(&e->baked[i]);
             if (err != cudaSuccess) st = cuda_fail(err, "graph timing events");
         }
@@ -100,8 +100,8 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
             else if (err != cudaSuccess) st = cuda_fail(err, "ending graph capture");
         }
         if (st == VX_OK) {
-            // The four stage-timing event nodes, so each launch can point them at
-            // the context's timing events.
+            // The stage-timing event nodes, so each launch can point them at the
+            // context's timing events.
             size_t num = 0;
             cudaGraphGetNodes(e->graph, nullptr, &num);
             std::vector<cudaGraphNode_t> nodes(num);
@@ -112,7 +112,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
                     continue;
                 cudaEvent_t ev = nullptr;
                 cudaGraphEventRecordNodeGetEvent(nd, &ev);
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < vx_ctx::kStageEvents; ++i)
                     if (ev == e->baked[i]) e->ev_nodes[i] = nd;
             }
             err = cudaGraphInstantiate(&e->exec, e->graph, 0);
@@ -139,11 +139,12 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
     entry->last_use = ++sgm->graph_clock;
 
     cudaEvent_t* slot = ctx->next_timing_slot();
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < vx_ctx::kStageEvents; ++i)
         if (entry->ev_nodes[i])
             cudaGraphExecEventRecordNodeSetEvent(entry->exec, entry->ev_nodes[i],
                                                  slot ? slot[i] : entry->baked[i]);
-    count_launch(3);
+    // census, the cost volume (scanline-pair form), aggregation, WTA
+    count_launch(entry->plan.unit_scanlines == kUnitScanlines ? 4 : 3);
     err = cudaGraphLaunch(entry->exec, stream);
     if (err != cudaSuccess) return cuda_fail(err, "launching the batch graph");
     if (synchronous) {

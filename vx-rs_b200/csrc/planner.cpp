@@ -355,18 +355,19 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     if (ev) record(ev[0]);
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
+    if (ev) record(ev[1]);
     if (pl.unit_scanlines == kUnitScanlines) {
         e = launch_costs(d_pairs, n, pl.total_rows, pl.dp_max, pl.census64, stream);
         if (e != cudaSuccess) return cuda_fail(e, "cost volume launch");
     }
-    if (ev) record(ev[1]);
+    if (ev) record(ev[2]);
     e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream, pl.compact);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
-    if (ev) record(ev[2]);
+    if (ev) record(ev[3]);
     e = launch_wta(d_pairs, n, pl.total_rows, pl.max_width, stream);
     if (e != cudaSuccess) return cuda_fail(e, "WTA launch");
-    if (ev) record(ev[3]);
+    if (ev) record(ev[4]);
     return VX_OK;
 }
 

@@ -28,9 +28,10 @@ struct vx_ctx {
     // Stage timing: per batch, 4 events bracket census | aggregation | WTA.
     // Batches since the last enable take consecutive slots of the ring.
     static constexpr int kTimingSlots = 256;
+    static constexpr int kStageEvents = 5;  // before census, cost volume, aggregation, WTA; after WTA
     bool timing = false;
     int timing_batches = 0;
-    std::vector<cudaEvent_t> stage_ev;  // kTimingSlots * 4 when enabled
+    std::vector<cudaEvent_t> stage_ev;  // kTimingSlots * kStageEvents when enabled
     std::mutex timing_mu;
     cudaEvent_t* next_timing_slot();
 };
@@ -130,10 +131,11 @@ size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg
 void rebind_pointers(Plan& plan, const std::vector<PairSpec>& specs);
 // Resolves the workspace-relative pointers of plan.pairs against `base`.
 void bind_plan(Plan& plan, char* base);
-// Issues the whole batch (census, aggregation, WTA) on `stream` with the
-// workspace at `base` (plan must be bound to it).
-// stage_events: null, or 4 events recorded before census, before aggregation,
-// before WTA and after WTA. warpgroups: aggregation CTA size (0 = default).
+// Issues the whole batch (census, cost volume, aggregation, WTA) on `stream`
+// with the workspace at `base` (plan must be bound to it).
+// stage_events: null, or vx_ctx::kStageEvents events recorded before census,
+// before the cost volume, before aggregation, before WTA and after WTA.
+// warpgroups: aggregation CTA size (0 = default).
 vx_status run_plan(const Plan& plan, char* base, cudaStream_t stream,
                    cudaEvent_t* stage_events = nullptr, int warpgroups = 0);
 // The two halves of run_plan: copy the plan tables into the workspace (all of
@@ -196,8 +198,8 @@ struct vx_sgm {
         char* ws = nullptr;         // resident workspace of the bucket
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        cudaEvent_t baked[4] = {};  // events the stage-timing nodes were captured with
-        cudaGraphNode_t ev_nodes[4] = {};
+        cudaEvent_t baked[vx_ctx::kStageEvents] = {};  // events the stage-timing nodes were captured with
+        cudaGraphNode_t ev_nodes[vx_ctx::kStageEvents] = {};
         uint64_t last_use = 0;
     };
     std::mutex graph_mu;

@@ -105,8 +105,8 @@ _ctx_destroy = _sig("vx_ctx_destroy", None, _P)
 _ctx_stream = _sig("vx_ctx_stream", _P, _P)
 _ctx_sync = _sig("vx_ctx_synchronize", ctypes.c_int, _P)
 _ctx_timing = _sig("vx_ctx_enable_stage_timing", ctypes.c_int, _P, ctypes.c_int)
-_ctx_times = _sig("vx_ctx_stage_times", ctypes.c_int, _P, ctypes.POINTER(ctypes.c_float),
-                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float))
+_ctx_times = _sig("vx_ctx_stage_times_detail", ctypes.c_int, _P, ctypes.POINTER(ctypes.c_float),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float))
 _img_create = _sig("vx_image_create", ctypes.c_int, _P, ctypes.c_uint32, ctypes.c_uint32,
                    ctypes.c_int, ctypes.POINTER(_P))
 _img_wrap = _sig("vx_image_wrap_device", ctypes.c_int, _P, _P, ctypes.c_size_t, ctypes.c_uint32,
@@ -218,10 +218,16 @@ class Context:
         _check(_ctx_timing(self._h, int(bool(on))))
 
     def stage_times(self):
-        """(census_ms, aggregate_ms, wta_ms) of the last batch, from CUDA events."""
-        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
-        _check(_ctx_times(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
-        return a.value, b.value, c.value
+        """(census_ms, aggregate_ms, wta_ms), the mean per timed batch from CUDA events;
+        census_ms includes the cost volume (stage_times_detail has it apart)."""
+        a, b, c, d = self.stage_times_detail()
+        return a + b, c, d
+
+    def stage_times_detail(self):
+        """(census_ms, costs_ms, aggregate_ms, wta_ms), the mean per timed batch."""
+        a, b, c, d = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _check(_ctx_times(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
 
     def close(self):
         if self._h:
