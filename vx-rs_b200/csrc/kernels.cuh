@@ -130,6 +130,9 @@ __host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, bool wide_t
 __host__ __device__ constexpr size_t aggregate_tile_offset(int dp_max) { return (size_t)(dp_max + 72) * 8; }
 
 constexpr int kWtaThreads = 256;
+// u16 sums per WTA warp in shared memory: its pixels (32 / lanes per pixel) x
+// their padded disparities (8 x lanes per pixel x rounds) <= 4 x 256.
+constexpr int kWtaSumsPerWarp = 1024;
 // Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).
 constexpr int kMaxWidth = 16384;
 

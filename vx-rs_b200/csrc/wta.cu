@@ -72,9 +72,9 @@ __device__ __forceinline__ void add_u16_split(uint32_t (&a)[4], const uint4 v) {
 // byte 0 of the pixel's lane c = 0, shadow slot in its bytes 4..7) are taken
 // out again and replaced by their exact u16 values from the shadow with
 // per-half wrapping adds (rare).
-template <int NP, bool WIDE>
+template <int NP, bool WIDE, bool FIRST>
 __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, bool act, int lead,
-                                          uint32_t (&acc)[4]) {
+                                          unsigned& em, uint32_t (&acc)[4]) {
     const bool in_dp = act && 8 * c < rv.Dp;        // lanes past Dp (Dv = Dp + 8) read no shadow
     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
     if (WIDE) {
@@ -113,7 +113,7 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
     // rare branch.
     uint32_t ff = 0u;
 #pragma unroll
-    for (int p = 0; p < NP; p += 4) {
+    for (int p = 0; p < (FIRST ? NP : 0); p += 4) {
         uint32_t g;
         if (NP == 2) {
             g = __byte_perm(v[p].x, v[p + 1].x, 0x4040);
@@ -123,11 +123,16 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
         }
         ff |= (~g - 0x01010101u) & g & 0x80808080u;
     }
-    if (__any_sync(kFull, c == 0 && ff != 0u)) {
-        unsigned em = 0u;
+    if (FIRST) {                                    // round 0: the lanes c = 0 hold chunk 0
+        em = 0u;
+        if (__any_sync(kFull, c == 0 && ff != 0u)) {
+            unsigned e = 0u;
 #pragma unroll
-        for (int p = 0; p < NP; ++p) em |= ((v[p].x & 0xFFu) == 0xFFu ? 1u : 0u) << p;
-        em = __shfl_sync(kFull, em, lead);          // the pixel's markers (its lane c = 0)
+            for (int p = 0; p < NP; ++p) e |= ((v[p].x & 0xFFu) == 0xFFu ? 1u : 0u) << p;
+            em = __shfl_sync(kFull, e, lead);       // the pixel's markers (its lane c = 0)
+        }
+    }
+    if (__any_sync(kFull, em != 0u)) {
         // Every escaped byte vector out first (plain subtractions are exact only
         // while no half has wrapped), then the shadow values in.
 #pragma unroll
@@ -162,18 +167,10 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
     acc[3] = __byte_perm(a[2], a[3], 0x7632);
 }
 
-// s[i] for a lane-dependent i in 0..7 without local memory (select tree).
-__device__ __forceinline__ uint32_t pick8(const uint32_t (&s)[8], int i) {
-    const uint32_t a0 = (i & 1) ? s[1] : s[0], a1 = (i & 1) ? s[3] : s[2];
-    const uint32_t a2 = (i & 1) ? s[5] : s[4], a3 = (i & 1) ? s[7] : s[6];
-    const uint32_t b0 = (i & 2) ? a1 : a0, b1 = (i & 2) ? a3 : a2;
-    return (i & 4) ? b1 : b0;
-}
-
 // Four CTAs per SM (at most 64 registers a thread, no spills) keep enough slab loads in flight.
 __global__ void __launch_bounds__(kWtaThreads, 4)
 wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
-    extern __shared__ uint32_t smem[];
+    extern __shared__ __align__(16) uint32_t smem[];
     const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
     const PairDev pr = pairs[pi];                  // fields live in registers
     const int y = blockIdx.x - pr.row_begin;
@@ -183,6 +180,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     uint32_t* right_key = smem;                               // W keys (LR only)
     uint32_t* best_key = smem + W;                            // W: S(bd) << 8 | bd
     uint32_t* nbr = smem + 2 * W;                             // W: S(bd-1) | S(bd+1) << 16
+                                                              // then the warps' sums
 
     if (lr)
         for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
@@ -190,7 +188,8 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
 
     const int chunks = pr.nd_vec / 8;               // 8-disparity chunks per pixel
     int seg = 1;
-    while (seg < chunks) seg <<= 1;                 // lanes per pixel (power of two)
+    while (seg < chunks && seg < 8) seg <<= 1;      // lanes per pixel (power of two, at most 8)
+    const int rounds = (chunks + seg - 1) / seg;    // chunks per lane (D = 192: 8 lanes x 3)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
     const int sub = lane / seg, c = lane % seg;
@@ -199,61 +198,82 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const RowView rv{pr.slabs, pr.shadow, pr.slab_stride, pr.shadow_stride, pr.nd_pad, pr.nd_vec, pr.shadow_cap};
     const bool subpixel = pr.subpixel != 0;
 
+    // This warp's sums of the current pixels: ppw rows of 8 * seg * rounds u16
+    // (S(d) at d), read back for S(bd-1) and S(bd+1).
+    // (16-byte aligned: the three W-word arrays end on a 4-byte boundary only.)
+    uint16_t* const srow_p = reinterpret_cast<uint16_t*>(smem + ((3 * W + 3) & ~3)) + warp * kWtaSumsPerWarp +
+                             sub * (8 * seg * rounds);
     for (int xb = warp * ppw; xb < W; xb += nwarps * ppw) {
         const int x = xb + sub;
-        const bool act = x < W && c < chunks;
-        const size_t pix = (size_t)y * W + (act ? x : 0);
-        uint32_t acc[4] = {0u, 0u, 0u, 0u};         // acc[k] = S(8c+2k) | S(8c+2k+1) << 16
-        switch (kind) {                             // uniform over the CTA
-            case 0: sum_paths<2, false>(rv, pix, c, act, sub * seg, acc); break;
-            case 1: sum_paths<4, false>(rv, pix, c, act, sub * seg, acc); break;
-            case 2: sum_paths<8, false>(rv, pix, c, act, sub * seg, acc); break;
-            case 3: sum_paths<2, true>(rv, pix, c, act, sub * seg, acc); break;
-            case 4: sum_paths<4, true>(rv, pix, c, act, sub * seg, acc); break;
-            default: sum_paths<8, true>(rv, pix, c, act, sub * seg, acc); break;
-        }
-        // key = S(d) << 8 | d (one byte permute: d in byte 0, S in bytes 1-2;
-        // d = 8c + j < 256), whose minimum is the first minimum.
-        const uint32_t d0 = 8u * (uint32_t)c;
-        uint32_t key[8];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            key[2 * k] = __byte_perm(acc[k], d0 + 2 * k, 0x5104);
-            key[2 * k + 1] = __byte_perm(acc[k], d0 + 2 * k + 1, 0x5324);
-        }
-        const int nb = (act ? D : 0) - (int)d0;     // this lane's keys j < nb take part
+        const bool actx = x < W;
+        const size_t pix = (size_t)y * W + (actx ? x : 0);
         uint32_t best = 0xFFFFFFFFu;
-        if (nb >= 8) {                              // no pads: three-way minima
-            best = min(__vimin3_u32(key[0], key[1], key[2]), __vimin3_u32(key[3], key[4], key[5]));
-            best = __vimin3_u32(best, key[6], key[7]);
-        } else {
+        unsigned em = 0u;                           // escaped paths of the pixel (from round 0)
+        for (int r = 0; r < rounds; ++r) {
+            const int cc = r * seg + c;             // this lane's chunk: d = 8cc..8cc+7
+            const bool act = actx && cc < chunks;
+            uint32_t acc[4] = {0u, 0u, 0u, 0u};     // acc[k] = S(8cc+2k) | S(8cc+2k+1) << 16
+            if (r == 0) {
+                switch (kind) {                     // uniform over the CTA
+                    case 0: sum_paths<2, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 1: sum_paths<4, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 2: sum_paths<8, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 3: sum_paths<2, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 4: sum_paths<4, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    default: sum_paths<8, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
+                }
+            } else {
+                switch (kind) {
+                    case 0: sum_paths<2, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 1: sum_paths<4, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 2: sum_paths<8, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 3: sum_paths<2, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    case 4: sum_paths<4, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                    default: sum_paths<8, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
+                }
+            }
+            *reinterpret_cast<uint4*>(srow_p + 8 * cc) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+            // key = S(d) << 8 | d (one byte permute: d in byte 0, S in bytes 1-2;
+            // d = 8cc + j < 256), whose minimum is the first minimum.
+            const uint32_t d0 = 8u * (uint32_t)cc;
+            uint32_t key[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                if (j < nb) best = min(best, key[j]);
-        }
-        for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
-        const int bd = (int)(best & 0xFFu);
-        // S(bd-1) and S(bd+1) from the lanes that hold them (only used when
-        // 0 < bd < D-1, so both exist).
-        const int dm = max(bd - 1, 0), dq = min(bd + 1, D - 1);
-        const uint32_t c0 = __shfl_sync(kFull, pick8(key, dm & 7), sub * seg + (dm >> 3)) >> 8;
-        const uint32_t c2 = __shfl_sync(kFull, pick8(key, dq & 7), sub * seg + (dq >> 3)) >> 8;
-        if (lr && act) {
-            const int xr = x - 8 * c;               // right-view column of this lane's d = 8c
-            const int nr = min(D - 8 * c, xr + 1);  // j < nr: d < D and x - d >= 0
-            if (nr >= 8) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) atomicMin(&right_key[xr - j], key[j]);
+            for (int k = 0; k < 4; ++k) {
+                key[2 * k] = __byte_perm(acc[k], d0 + 2 * k, 0x5104);
+                key[2 * k + 1] = __byte_perm(acc[k], d0 + 2 * k + 1, 0x5324);
+            }
+            const int nb = (act ? D : 0) - (int)d0; // this lane's keys j < nb take part
+            if (nb >= 8) {                          // no pads: three-way minima
+                best = __vimin3_u32(best, __vimin3_u32(key[0], key[1], key[2]), __vimin3_u32(key[3], key[4], key[5]));
+                best = __vimin3_u32(best, key[6], key[7]);
             } else {
 #pragma unroll
                 for (int j = 0; j < 8; ++j)
-                    if (j < nr) atomicMin(&right_key[xr - j], key[j]);
+                    if (j < nb) best = min(best, key[j]);
+            }
+            if (lr && act) {
+                const int xr = x - 8 * cc;          // right-view column of this lane's d = 8cc
+                const int nr = min(D - 8 * cc, xr + 1);   // j < nr: d < D and x - d >= 0
+                if (nr >= 8) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) atomicMin(&right_key[xr - j], key[j]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        if (j < nr) atomicMin(&right_key[xr - j], key[j]);
+                }
             }
         }
-        if (c == 0 && x < W) {
+        for (int o = seg >> 1; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
+        __syncwarp();                               // the pixel's sums are in shared memory
+        if (c == 0 && actx) {
+            // S(bd-1) and S(bd+1) (only used when 0 < bd < D-1, so both exist).
+            const int bd = (int)(best & 0xFFu);
+            const uint32_t c0 = srow_p[max(bd - 1, 0)], c2 = srow_p[min(bd + 1, D - 1)];
             best_key[x] = best;
             nbr[x] = c0 | (c2 << 16);
         }
+        __syncwarp();                               // before the next pixels' sums
     }
     __syncthreads();
 
@@ -292,7 +312,10 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
 
 }  // namespace
 
-size_t wta_smem_bytes(int max_width) { return (size_t)max_width * 3 * sizeof(uint32_t); }
+size_t wta_smem_bytes(int max_width) {
+    return ((size_t)max_width * 3 + 3) / 4 * 4 * sizeof(uint32_t) +
+           (size_t)(kWtaThreads / 32) * kWtaSumsPerWarp * sizeof(uint16_t);
+}
 
 cudaError_t prepare_wta_kernel() {
     return cudaFuncSetAttribute(wta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
