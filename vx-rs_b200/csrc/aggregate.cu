@@ -227,8 +227,10 @@ __device__ __forceinline__ void cost_words(uint32_t (&cw)[8], const uint2 lo, co
 template <bool WIDE>
 __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
                                                  const uint8_t* __restrict__ cv_lo,
-                                                 const uint8_t* __restrict__ cv_hi, const ScanConst& k,
-                                                 unsigned char* __restrict__ row_lo,
+                                                 const uint8_t* __restrict__ cv_hi,
+                                                 const uint8_t* __restrict__ nx_lo,
+                                                 const uint8_t* __restrict__ nx_hi, uint2& g0_lo, uint2& g0_hi,
+                                                 const ScanConst& k, unsigned char* __restrict__ row_lo,
                                                  unsigned char* __restrict__ row_hi) {
     PixelState ps;
     const uint32_t m0 = m & ~start;
@@ -257,11 +259,10 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
         }
         tmem_st8(tstate + 8 * g, o);
     };
-    uint2 pa_l, pa_h, pb_l, pb_h;
+    uint2 pa_l = g0_lo, pa_h = g0_hi, pb_l, pb_h;     // group 0, loaded during the previous pixel
     uint32_t ca[8], cb[8];
     Words8 oa, ob;
     uint32_t w7;
-    load(pa_l, pa_h, 0);
     Words8 sa = tmem_ld8(tstate), sb;
     cost_words(ca, pa_l, pa_h);
     tmem_wait_ld(sa);
@@ -283,6 +284,9 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
         store(ob, g + 1);
         cost_words(ca, pa_l, pa_h);
     }
+    // The next pixel's group 0 (nx_lo / nx_hi: its rows, or any valid row).
+    g0_lo = __ldcs(reinterpret_cast<const uint2*>(nx_lo));
+    g0_hi = __ldcs(reinterpret_cast<const uint2*>(nx_hi));
     if (g + 1 < k.G) {
         sb = tmem_ld8(tstate + 8 * (g + 1));
         load(pb_l, pb_h, g + 1);
@@ -471,16 +475,28 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     unsigned char* row_lo = tile + lane * row_bytes;
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
+    // Cost rows of step t's two scanlines (pixel 0's row for a half outside its scanline).
+    auto rows_at = [&](int t, const uint8_t*& lo, const uint8_t*& hi) {
+        const size_t p0 = (size_t)((ptrdiff_t)(y0 + dy * t) * W + k0 + dx * t);
+        lo = CV + (t >= tb_lo && t < te_lo ? (p0 + lane) * Dv : 0);
+        hi = CV + (t >= tb_hi && t < te_hi ? (p0 + lane + 32) * Dv : 0);
+    };
+    const uint8_t *cv_lo, *cv_hi;
+    rows_at(t_lo, cv_lo, cv_hi);
+    uint2 g0_lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi));
     for (int t = t_lo; t < t_hi; ++t) {
         const bool act_lo = t >= tb_lo && t < te_lo, act_hi = t >= tb_hi && t < te_hi;
         const uint32_t start = (t == tb_lo ? 0x0000FFFFu : 0u) | (t == tb_hi ? 0xFFFF0000u : 0u);
         const int xb = k0 + dx * t;             // x of tile row 0
         const int y = y0 + dy * t;
         const size_t pix0 = (size_t)((ptrdiff_t)y * W + xb);
-        const uint8_t* cv_lo = CV + (act_lo ? (pix0 + lane) * Dv : 0);
-        const uint8_t* cv_hi = CV + (act_hi ? (pix0 + lane + 32) * Dv : 0);
-        const uint32_t mx = wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
-                                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
+        const uint8_t *nx_lo = CV, *nx_hi = CV;
+        if (t + 1 < t_hi) rows_at(t + 1, nx_lo, nx_hi);
+        const uint32_t mx =
+            wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, nx_lo, nx_hi, g0_lo, g0_hi, k, row_lo, row_hi)
+                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, nx_lo, nx_hi, g0_lo, g0_hi, k, row_lo, row_hi);
+        cv_lo = nx_lo;
+        cv_hi = nx_hi;
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                          row_hi, pix0, 1, pix0 + lane, pix0 + lane + 32, lane);
     }
@@ -507,14 +523,23 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
     const int x0 = dx > 0 ? 0 : W - 1;
+    // Column x's cost rows of the two scanlines (pixel 0's row for a row past the image).
+    const uint8_t* cv_lo = CV + (act_lo ? ((size_t)(first + lane) * W + x0) * Dv : 0);
+    const uint8_t* cv_hi = CV + (act_hi ? ((size_t)(first + 32 + lane) * W + x0) * Dv : 0);
+    const ptrdiff_t step_lo = act_lo ? (ptrdiff_t)dx * Dv : 0, step_hi = act_hi ? (ptrdiff_t)dx * Dv : 0;
+    uint2 g0_lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi));
     for (int t = 0; t < W; ++t) {
         const int x = x0 + dx * t;
         const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;
         const size_t pix0 = (size_t)first * W + x;
-        const uint8_t* cv_lo = CV + (act_lo ? (pix0 + (size_t)lane * W) * Dv : 0);
-        const uint8_t* cv_hi = CV + (act_hi ? (pix0 + (size_t)(lane + 32) * W) * Dv : 0);
-        const uint32_t mx = wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi)
-                                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, k, row_lo, row_hi);
+        const bool more = t + 1 < W;
+        const uint8_t* nx_lo = more ? cv_lo + step_lo : CV;
+        const uint8_t* nx_hi = more ? cv_hi + step_hi : CV;
+        const uint32_t mx =
+            wide ? sgm_pixel<true>(tstate, m, start, cv_lo, cv_hi, nx_lo, nx_hi, g0_lo, g0_hi, k, row_lo, row_hi)
+                 : sgm_pixel<false>(tstate, m, start, cv_lo, cv_hi, nx_lo, nx_hi, g0_lo, g0_hi, k, row_lo, row_hi);
+        cv_lo = nx_lo;
+        cv_hi = nx_hi;
         // Rows first..first+63, one vector per row at column x.
         finish_pixel<CP>(pr, et, job.path, wide, Dv, tstate, k.G, mx, act_lo, act_hi, tile, row_bytes, row_lo,
                          row_hi, pix0, (size_t)W, pix0 + (size_t)lane * W, pix0 + (size_t)(lane + 32) * W, lane);
