@@ -164,10 +164,10 @@ def cpu_reference_rate(items, pairs, max_pd, threads):
 
 
 # DRAM bytes (read + write) one aggregation launch (scanline-pair form) of the
-# 64-pair workload moved per path-pixel-disparity: 55.79 GB over 8 x 3.738 G
-# path-pd (ncu capture, dram__bytes_read.sum 25.83 GB of cost-volume reads, the
+# 64-pair workload moved per path-pixel-disparity: 56.00 GB over 8 x 3.738 G
+# path-pd (ncu capture, dram__bytes_read.sum 26.04 GB of cost-volume reads, the
 # rest of the 29.90 GB served by L2, + dram__bytes_write.sum 29.96 GB of slabs).
-AGG_DRAM_BYTES_PER_PATH_PD = 55.79e9 / (8 * 3737760000)
+AGG_DRAM_BYTES_PER_PATH_PD = 56.00e9 / (8 * 3737760000)
 
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
