@@ -96,7 +96,7 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
     uint2 v[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p)
-        v[p] = act ? __ldcs(reinterpret_cast<const uint2*>(base + rv.slab_stride * p)) : make_uint2(0u, 0u);
+        v[p] = act ? __ldg(reinterpret_cast<const uint2*>(base + rv.slab_stride * p)) : make_uint2(0u, 0u);
     constexpr uint32_t M = 0x00FF00FFu;
     uint32_t a[4] = {0u, 0u, 0u, 0u};               // (0,2) (1,3) (4,6) (5,7)
 #pragma unroll
