@@ -240,8 +240,8 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
     ps.mn = 0xFFFFFFFFu;
     ps.mx = 0u;
     auto load = [&](uint2& lo, uint2& hi, int g) {
-        lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo + 8 * g));
-        hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi + 8 * g));
+        lo = __ldg(reinterpret_cast<const uint2*>(cv_lo + 8 * g));
+        hi = __ldg(reinterpret_cast<const uint2*>(cv_hi + 8 * g));
     };
     auto store = [&](const Words8& o, int g) {
         if (WIDE) {             // u16 rows: 8 values (16 bytes) per group
@@ -285,8 +285,8 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
         cost_words(ca, pa_l, pa_h);
     }
     // The next pixel's group 0 (nx_lo / nx_hi: its rows, or any valid row).
-    g0_lo = __ldcs(reinterpret_cast<const uint2*>(nx_lo));
-    g0_hi = __ldcs(reinterpret_cast<const uint2*>(nx_hi));
+    g0_lo = __ldg(reinterpret_cast<const uint2*>(nx_lo));
+    g0_hi = __ldg(reinterpret_cast<const uint2*>(nx_hi));
     if (g + 1 < k.G) {
         sb = tmem_ld8(tstate + 8 * (g + 1));
         load(pb_l, pb_h, g + 1);
@@ -483,7 +483,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     };
     const uint8_t *cv_lo, *cv_hi;
     rows_at(t_lo, cv_lo, cv_hi);
-    uint2 g0_lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi));
+    uint2 g0_lo = __ldg(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint2*>(cv_hi));
     for (int t = t_lo; t < t_hi; ++t) {
         const bool act_lo = t >= tb_lo && t < te_lo, act_hi = t >= tb_hi && t < te_hi;
         const uint32_t start = (t == tb_lo ? 0x0000FFFFu : 0u) | (t == tb_hi ? 0xFFFF0000u : 0u);
@@ -527,7 +527,7 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const uint8_t* cv_lo = CV + (act_lo ? ((size_t)(first + lane) * W + x0) * Dv : 0);
     const uint8_t* cv_hi = CV + (act_hi ? ((size_t)(first + 32 + lane) * W + x0) * Dv : 0);
     const ptrdiff_t step_lo = act_lo ? (ptrdiff_t)dx * Dv : 0, step_hi = act_hi ? (ptrdiff_t)dx * Dv : 0;
-    uint2 g0_lo = __ldcs(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldcs(reinterpret_cast<const uint2*>(cv_hi));
+    uint2 g0_lo = __ldg(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint2*>(cv_hi));
     for (int t = 0; t < W; ++t) {
         const int x = x0 + dx * t;
         const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;
