@@ -1,0 +1,137 @@
+"""CPU replays of the index arithmetic of two kernels, run before their GPU use.
+
+cost.cu (cost volume): every (x, d) of a row is written exactly once with the
+matching cost (popcount of the census XOR, 64 where x - d < 0, 0 in the pads),
+every census load stays inside the planes' guard words and is 16-byte aligned,
+and every shared-memory tile index stays inside the launch's allocation.
+
+wta.cu (per-warp sums): every 16-byte store into the sums rows is aligned and
+inside the dynamic shared memory, for odd widths too.
+
+The constants mirror the kernels' (cost.cu: kBlockPx, kTileRows, kMaxTileBytes;
+kernels.cuh: kCensusGuardWords, kWtaThreads, kWtaSumsPerWarp)."""
+import random
+
+K_BLOCK_PX, K_WARPS, K_TILE_ROWS, K_MAX_TILE_BYTES = 128, 8, 132, 56 * 1024
+K_GUARD_WORDS = 352
+K_WTA_THREADS, K_WTA_SUMS_PER_WARP = 256, 1024
+
+
+def _tile_stride(dv):
+    return (dv // 16) | 1
+
+
+def _blocks_per_pass(dv):
+    chunks = dv // 16
+    best, best_num, best_den = 1, 0, 1
+    for nb in range(1, K_WARPS + 1):
+        if nb * K_TILE_ROWS * _tile_stride(dv) * 16 > K_MAX_TILE_BYTES:
+            break
+        items = nb * chunks
+        den = K_WARPS * ((items + K_WARPS - 1) // K_WARPS)
+        if items * best_den > best_num * den:
+            best, best_num, best_den = nb, items, den
+    return best
+
+
+def _tile_units(dv):
+    return _blocks_per_pass(dv) * K_TILE_ROWS * _tile_stride(dv)
+
+
+def _replay_cost_row(W, H, D, y, dp_max, cl, cr):
+    dv = (D + 15) // 16 * 16
+    chunks, ts, nb = dv // 16, _tile_stride(dv), _blocks_per_pass(dv)
+    units = max(_tile_units(v) for v in range(16, (dp_max + 15) // 16 * 16 + 1, 16))
+    assert units * 16 <= K_MAX_TILE_BYTES                     # the launch's smem bound
+    row0 = y * W
+    out = {}
+    xb = -(row0 & 3)
+    while xb < W:
+        tile = {}
+        for it in range(nb * chunks):
+            blk, ch = divmod(it, chunks)
+            for lane in range(32):
+                x4 = xb + blk * K_BLOCK_PX + 4 * lane
+                if x4 >= W:
+                    continue
+                a = row0 + x4
+                assert a % 4 == 0 and a >= 0
+                base = a - 16 * ch - 16                  # 20 right words, 5 aligned vectors
+                assert base % 4 == 0
+                assert -K_GUARD_WORDS <= base and base + 19 < H * W + K_GUARD_WORDS
+                assert a + 3 < H * W + K_GUARD_WORDS
+                n0, dmax = x4 - 16 * ch, D - 16 * ch
+                check = not (n0 >= 15 and dmax >= 16)
+                for i in range(4):
+                    v = []
+                    for e in range(16):
+                        c = bin(cl[a + i] ^ cr[base + i - e + 16]).count("1")
+                        if check:
+                            c = 0 if e >= dmax else (64 if e > n0 + i else c)
+                        v.append(c)
+                    idx = (blk * K_TILE_ROWS + lane) * ts + ch + i * 33 * ts
+                    assert 0 <= idx < units and idx not in tile
+                    tile[idx] = v
+        p0, p1 = max(xb, 0) - xb, min(nb * K_BLOCK_PX, W - xb)
+        for q in range((p1 - p0) * chunks):
+            pq, c = divmod(q, chunks)
+            pp = pq + p0
+            row = (pp >> 7) * K_TILE_ROWS + (pp & 3) * 33 + ((pp & 127) >> 2)
+            x, cc = divmod((xb + p0) * dv + 16 * q, dv)
+            assert cc == 16 * c and x == xb + pp and 0 <= x < W
+            for e in range(16):
+                assert (x, 16 * c + e) not in out
+                out[(x, 16 * c + e)] = tile[row * ts + c][e]
+        xb += nb * K_BLOCK_PX
+    assert len(out) == W * dv
+    for x in range(W):
+        for d in range(dv):
+            want = 0 if d >= D else (64 if x < d else bin(cl[row0 + x] ^ cr[row0 + x - d]).count("1"))
+            assert out[(x, d)] == want, (W, D, y, x, d)
+
+
+def test_cost_kernel_mapping_covers_rows_in_bounds():
+    rng = random.Random(7)
+    for (W, H, D, dp_max) in [(1, 2, 1, 8), (5, 3, 16, 16), (37, 3, 64, 256), (130, 2, 80, 80),
+                              (129, 2, 256, 256), (300, 2, 144, 144), (77, 3, 40, 256), (261, 2, 48, 64),
+                              (97, 2, 33, 40), (200, 2, 192, 192)]:
+        cl = {i: rng.getrandbits(24) for i in range(-K_GUARD_WORDS, H * W + K_GUARD_WORDS)}
+        cr = {i: rng.getrandbits(24) for i in range(-K_GUARD_WORDS, H * W + K_GUARD_WORDS)}
+        for y in range(H):
+            _replay_cost_row(W, H, D, y, dp_max, cl, cr)
+
+
+def test_cost_kernel_passes_fill_the_warps():
+    # The pass sizes chosen for the disparity counts of the benchmark mix leave no
+    # warp idle at the pass barrier, within four CTAs' worth of tile an SM.
+    for D in (64, 128, 192, 256):
+        dv = (D + 15) // 16 * 16
+        assert (_blocks_per_pass(dv) * (dv // 16)) % K_WARPS == 0, D
+    for dv in range(16, 257, 16):
+        assert _tile_units(dv) * 16 <= K_MAX_TILE_BYTES
+
+
+def _wta_smem_bytes(max_width):
+    return ((max_width * 3 + 3) // 4 * 4) * 4 + (K_WTA_THREADS // 32) * K_WTA_SUMS_PER_WARP * 2
+
+
+def test_wta_sums_rows_aligned_and_in_bounds():
+    for D in range(1, 257):
+        dv = (D + 15) // 16 * 16
+        chunks = dv // 8
+        seg = 1
+        while seg < chunks and seg < 8:
+            seg <<= 1
+        rounds = (chunks + seg - 1) // seg
+        assert (32 // seg) * 8 * seg * rounds <= K_WTA_SUMS_PER_WARP
+        for W in (1, 2, 3, 5, 7, 33, 1241, 1242, 16383):
+            base = ((3 * W + 3) & ~3) * 4                # bytes
+            assert base % 16 == 0
+            for warp in range(K_WTA_THREADS // 32):
+                for lane in range(32):
+                    sub, c = divmod(lane, seg)
+                    row = base + (warp * K_WTA_SUMS_PER_WARP + sub * 8 * seg * rounds) * 2
+                    for r in range(rounds):
+                        off = row + 16 * (r * seg + c)
+                        assert off % 16 == 0 and off + 16 <= _wta_smem_bytes(W)
+                    assert row + 2 * D <= _wta_smem_bytes(W)   # the S(bd +- 1) reads
