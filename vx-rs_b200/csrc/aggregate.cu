@@ -328,8 +328,8 @@ __device__ __forceinline__ ScanConst scan_const(const PairDev& pr) {
 // rows' 8-byte chunks are distributed over the lanes in address order (chunk
 // c = (r - la) * V + h, walked with a running (r, h): no division per chunk),
 // so consecutive lanes write consecutive 8 bytes of a vector. Streaming stores:
-// the slabs are read once by the WTA kernel and must not push the census
-// planes, which every path re-reads, out of L2.
+// the slabs are read once by the WTA kernel and must not push the cost volume,
+// which every path of the pair re-reads, out of L2.
 __device__ __forceinline__ void flush_tile(const unsigned char* __restrict__ tile, int row_bytes, int vb,
                                            int la, int lb, unsigned char* __restrict__ dst0, size_t stride,
                                            int lane) {
@@ -618,7 +618,7 @@ struct AggShape {
     int warpgroups;
     int wg_cols;     // columns per warpgroup
     int tmem_cols;   // allocation (power of two >= warpgroups * wg_cols)
-    size_t smem;     // census staging + byte tiles
+    size_t smem;     // output tiles (after a batch-dependent base offset)
 };
 
 // Largest number of warpgroups one aggregation CTA can hold for this batch:
@@ -668,8 +668,8 @@ static AggShape shape_for(int dp_max, bool wide_tiles, int warpgroups) {
 }
 
 cudaError_t prepare() {
-    // Dynamic shared memory up to the largest staging area, and the smallest
-    // shared-memory carveout: the rest of the SM's L1 caches the census windows.
+    // Dynamic shared memory up to the largest tile area, and the smallest
+    // shared-memory carveout: the rest of the SM is L1.
     int dev = 0, max_bytes = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);

@@ -16,8 +16,9 @@
 // census planes' guard words keep the reads at either end of the plane in
 // bounds). Items go to a shared-memory tile of the pass's vectors, which the
 // CTA then writes as one contiguous run of the volume with coalesced 16-byte
-// stores. A pass covers enough 128-pixel blocks to give all 8 warps an item
-// when the chunks are fewer than 8.
+// stores. A pass covers as many 128-pixel blocks as fill the 8 warps' last
+// round of items best (D = 192: 2 blocks, 24 items), within four CTAs' worth of
+// shared memory an SM.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
