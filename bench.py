@@ -144,23 +144,88 @@ class ClockSampler:
                 "samples": len(self.rows), "source": "nvml", "reasons": reasons}
 
 
-def cpu_reference_rate(items, pairs, max_pd, threads):
-    """The oracle (CPU restatement of the reference algorithm) on a bounded sample:
-    leading pairs of the workload until max_pd pixel-disparities."""
+def oracle_config(oracle, d):
+    return oracle.config(num_disparities=d, p1=10, p2=120, census_radius_x=2, census_radius_y=2,
+                         num_paths=8, subpixel=True, lr_check=True)
+
+
+def strata(items):
+    """Indices of the workload's pairs grouped by (W, H, D): pairs of one stratum are the
+    same amount of work (seeded scenes of one generator)."""
+    groups = {}
+    for i, (w, h, d, _) in enumerate(items):
+        groups.setdefault((w, h, d), []).append(i)
+    return groups
+
+
+def cpu_stratified(items, get_pair, threads, rounds, first_round=0, keep_outputs=False):
+    """The oracle (CPU restatement of the reference algorithm) on a size-stratified
+    sample of the workload: round r runs the r-th pair (cycling) of every (W, H, D)
+    stratum. The whole workload's CPU time is estimated as the sum over strata of
+    (pairs in the stratum) x (mean time of its sampled pairs), so the rate refers to
+    the same 64-pair workload as the GPU numbers. Returns (rate Gpd/s, sampled pairs,
+    sampled pd, sampled seconds, {index: oracle outputs} when keep_outputs)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    done_pd, secs, n = 0, 0.0, 0
-    for (w, h, d, _), (L, R) in zip(items, pairs):
-        cfg = oracle.config(num_disparities=d, p1=10, p2=120, census_radius_x=2,
-                            census_radius_y=2, num_paths=8, subpixel=True, lr_check=True)
-        t0 = time.perf_counter()
-        oracle.sgm(L, R, cfg, nthreads=threads)
-        secs += time.perf_counter() - t0
-        done_pd += w * h * d
-        n += 1
-        if done_pd >= max_pd:
-            break
-    return done_pd / secs / 1e9, n, done_pd, secs
+    groups = strata(items)
+    times = {k: [] for k in groups}
+    outputs = {}
+    n = pd = 0
+    secs = 0.0
+    for r in range(first_round, first_round + rounds):
+        for key, idx in groups.items():
+            i = idx[r % len(idx)]
+            w, h, d, _ = items[i]
+            L, R = get_pair(i)
+            t0 = time.perf_counter()
+            out = oracle.sgm(L, R, oracle_config(oracle, d), nthreads=threads)
+            dt = time.perf_counter() - t0
+            times[key].append(dt)
+            secs += dt
+            n += 1
+            pd += w * h * d
+            if keep_outputs:
+                outputs[i] = out
+    est = sum(len(groups[k]) * float(np.mean(v)) for k, v in times.items())
+    total_pd = sum(w * h * d for (w, h, d, _) in items)
+    return total_pd / est / 1e9, n, pd, secs, outputs
+
+
+def stratified_sample_text(items, n, pd, secs, threads):
+    return (f"{n} pairs: one of each of the {len(strata(items))} (W, H, D) strata of the {len(items)}-pair "
+            f"workload per round ({pd / 1e6:.0f} M pd, {secs:.1f} s, oracle on {threads} threads); "
+            f"workload time = sum over strata of pairs x the stratum's sampled time")
+
+
+def barrier(dist):
+    """All ranks meet (no-op on one process)."""
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, v, device="cuda"):
+    """The largest of every rank's value (the job's time is its slowest rank's)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, v, device="cuda"):
+    """The sum of every rank's value (each replica's pairs differ, and so does its work)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(job_pd, ms_per_step):
+    """Whole-job Gpd/s: all ranks' pixel-disparities of a step over the slowest rank's step time."""
+    return job_pd / (ms_per_step * 1e-3) / 1e9
 
 
 # DRAM bytes (read + write) one aggregation launch (scanline-pair form) of the
@@ -172,24 +237,31 @@ AGG_DRAM_BYTES_PER_PATH_PD = 56.00e9 / (8 * 3737760000)
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
 
-def served(vx_sgm, ctx, sgm, rates, num_requests, max_batch=32, slots=2):
-    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, 40 GB budget."""
+SERVED_KEYS = ("rate_per_s", "requests", "completed", "latency_ms_p50", "latency_ms_p99",
+               "throughput_gpd_s", "achieved_rate_per_s", "mean_batch", "max_batches_in_flight")
+
+
+def served(vx_sgm, ctx, sgm, rates, max_batch=32, slots=2):
+    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, 40 GB budget.
+    rates: (requests per second, number of requests) per point; a fresh server per
+    point so that each point's counters are its own."""
     import loadgen
     reqs = loadgen.make_requests(48)
-    srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=max_batch,
-                        max_inflight_batches=slots)
-    loadgen.run_poisson(srv, reqs, 100.0, 16)  # warm the pool and the planner
     out = []
-    for r in rates:
+    for r, num_requests in rates:
+        srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=max_batch,
+                            max_inflight_batches=slots)
+        loadgen.run_poisson(srv, reqs, 100.0, 16)  # warm the pool and the planner
         before = srv.stats()
         res = loadgen.run_poisson(srv, reqs, r, num_requests)
         after = srv.stats()
+        srv.close()
         res["server"] = after
         batches = after["batches"] - before["batches"]
         res["mean_batch"] = (after["completed"] - before["completed"]) / batches if batches else None
+        res["max_batches_in_flight"] = after["max_batches_in_flight"]
         res["max_batch"], res["slots"] = max_batch, slots
         out.append(res)
-    srv.close()
     return out
 
 
@@ -198,7 +270,8 @@ def run_serve_sweep(args, local_rank):
     ctx = vx_sgm.Context(local_rank)
     sgm = vx_sgm.SGMStereo(ctx)
     rates = [float(x) for x in args.serve_sweep.split(",") if x]
-    for res in served(vx_sgm, ctx, sgm, rates, args.serve_requests, args.serve_max_batch, args.serve_slots):
+    for res in served(vx_sgm, ctx, sgm, [(r, args.serve_requests) for r in rates], args.serve_max_batch,
+                      args.serve_slots):
         print(json.dumps({"metric": "served SGM", "unit": UNIT, "budget_bytes": SERVE_BUDGET,
                           "workload": "Poisson arrivals, sizes {640x480,1242x375,1280x720,1920x1080} "
                                       "x D{64,128,192}, 8 paths", **res}), flush=True)
@@ -502,28 +575,45 @@ def run_single_pair(args, local_rank):
                                     "wta": wta_ms}}), flush=True)
 
 
+WORKLOAD_DESC = ("c2: 64 mixed pairs {320x240,640x480,1242x375,1280x720} x D{64,128,192}, "
+                 "8 paths, 5x5 census, P1=10 P2=120, subpixel, LR tol 1")
+
+
 def run_reference(args, rank, world):
+    """The reference algorithm on the host cores: the oracle restatement (the reference's
+    own path is Metal and cannot run here) on every host thread, same workload and
+    metric as the GPU arm. Each step is a size-stratified sample: one pair of every
+    (W, H, D) stratum, a different pair of each stratum every step. Loads the pair
+    generator alone (vx_synth), no CUDA code."""
     if rank != 0:
         return
-    import vx_sgm
+    import vx_synth
     items = workload(0)
     threads = os.cpu_count() or 1
-    pairs = make_pairs(vx_sgm, items[:8])
-    rates = []
+    cache = {}
+
+    def get_pair(i):
+        if i not in cache:
+            cache[i] = make_pairs(vx_synth, [items[i]])[0]
+        return cache[i]
+    rates, n, pd, secs = [], 0, 0, 0.0
     for step in range(args.warmup + args.steps):
-        rate, n, pd, secs = cpu_reference_rate(items, pairs, 3e8, threads)
+        rate, n1, pd1, secs1, _ = cpu_stratified(items, get_pair, threads, 1, first_round=step)
         if step >= args.warmup:
             rates.append(rate)
+            n, pd, secs = n + n1, pd + pd1, secs + secs1
     value = float(np.mean(rates))
-    sample = f"leading {n} pairs of the workload per step ({pd / 1e6:.0f} M pd, {secs:.1f} s)"
+    total_pd = sum(w * h * d for (w, h, d, _) in items)
+    sample = stratified_sample_text(items, n // max(args.steps, 1), pd // max(args.steps, 1),
+                                    secs / max(args.steps, 1), threads) + f", {args.steps} rounds"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * pd / 1e9 / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * total_pd / 1e9 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": "64 mixed pairs (c2), CPU sample", "paths": 8},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": sample},
+        "config": {"workload": WORKLOAD_DESC, "pairs_per_rank": NUM_PAIRS, "pd_per_rank": total_pd,
+                   "parallelism": f"replicas x{world}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -541,6 +631,11 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served measurement (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-sat-rate", type=float, default=1500.0,
+                    help="arrival rate of the saturated served point (requests/s)")
+    ap.add_argument("--serve-sat-requests", type=int, default=500)
+    ap.add_argument("--cpu-rounds", type=int, default=2,
+                    help="stratified CPU-baseline rounds (one pair of every (W, H, D) stratum each)")
     ap.add_argument("--serve-max-batch", type=int, default=32, help="server: requests per batch at most")
     ap.add_argument("--serve-slots", type=int, default=2, help="server: batches in flight at most")
     ap.add_argument("--serve-sweep", default="",
@@ -613,17 +708,6 @@ def main():
     of = [ctx.texture_output_r32float(w, h) for (w, h, _, _) in items]
     oi = [ctx.texture_output_i16(w, h) for (w, h, _, _) in items]
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def batch():
         sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
 
@@ -635,7 +719,7 @@ def main():
     for _ in range(args.warmup):
         batch()
     ctx.synchronize()
-    barrier()
+    barrier(dist)
     torch.cuda.synchronize()
     ctx.enable_stage_timing(True)
     launches0 = vx_sgm.kernel_launch_count()
@@ -650,9 +734,12 @@ def main():
     census_ms, costs_ms, agg_ms, wta_ms = ctx.stage_times_detail()
     ctx.enable_stage_timing(False)
     torch.cuda.synchronize()
-    barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
-    value = world * total_pd / (ms * 1e-3) / 1e9
+    barrier(dist)
+    ms = max_over_ranks(dist, e0.elapsed_time(e1)) / args.steps
+    job_pd = sum_over_ranks(dist, float(total_pd))
+    value = job_rate(job_pd, ms)
+    # The timed batch's own results, kept for the parity check against the oracle.
+    batch_out = [(f.read_r32float(), i.download()) for f, i in zip(of, oi)]
     if args.kernels_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms,
@@ -724,20 +811,20 @@ def main():
 
     e2e_run(3)
     torch.cuda.synchronize()
-    barrier()
+    barrier(dist)
     e0.record(h2d_s)
     e2e_run(args.steps)
     stream.wait_stream(d2h_s)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
-    e2e_value = world * total_pd / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(dist, e0.elapsed_time(e1)) / args.steps
+    e2e_value = job_rate(job_pd, e2e_ms)
 
     # ---- plain per-pair path (synchronous call per pair, like the reference) ----
     lat = []
     pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     plain_sgm.compute_disparity(ctx, tl[0], tr[0], of[0], cfgs[0], output_i16=oi[0])
-    barrier()
+    barrier(dist)
     plain_ms = 0.0
     for _ in range(args.plain_steps):
         for i in range(len(items)):
@@ -748,11 +835,14 @@ def main():
             t = pe0.elapsed_time(pe1)
             lat.append(t)
             plain_ms += t
-    plain_ms = max_over_ranks(plain_ms / args.plain_steps)
-    plain_value = world * total_pd / (plain_ms * 1e-3) / 1e9
+    plain_ms = max_over_ranks(dist, plain_ms / args.plain_steps)
+    plain_value = job_rate(job_pd, plain_ms)
 
     # ---- served: continuous batching under a 40 GB budget, Poisson arrivals ----
-    serve = served(vx_sgm, ctx, sgm, [args.serve_rate], args.serve_requests)[0]
+    # One point at a moderate rate and one past saturation (arrivals faster than the
+    # service rate: the queue grows, batches fill and several run at once).
+    serve, serve_sat = served(vx_sgm, ctx, sgm, [(args.serve_rate, args.serve_requests),
+                                                 (args.serve_sat_rate, args.serve_sat_requests)])
 
     # ---- roofline of the dominant kernel (path aggregation) ----
     peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
@@ -785,8 +875,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": "c2: 64 mixed pairs {320x240,640x480,1242x375,1280x720} x D{64,128,192}, "
-                               "8 paths, 5x5 census, P1=10 P2=120, subpixel, LR tol 1",
+        "config": {"workload": WORKLOAD_DESC,
                    "pairs_per_rank": NUM_PAIRS, "pd_per_rank": total_pd, "pixels_per_rank": total_px,
                    "parallelism": f"replicas x{world}",
                    "l2": "working set larger than L2 (byte path slabs %.1f GB per step)" % (
@@ -795,8 +884,8 @@ def main():
                   "latency_ms_p50": float(np.percentile(lat, 50)),
                   "latency_ms_p99": float(np.percentile(lat, 99)),
                   "batched_over_plain": value / plain_value},
-        "served": {k: serve[k] for k in ("rate_per_s", "requests", "completed", "latency_ms_p50",
-                                          "latency_ms_p99", "throughput_gpd_s", "achieved_rate_per_s")},
+        "served": {k: serve[k] for k in SERVED_KEYS},
+        "served_saturated": {k: serve_sat[k] for k in SERVED_KEYS},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "copies": "pinned host buffers, every step; double-buffered on two copy streams, "
@@ -825,10 +914,20 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, n, pd, secs = cpu_reference_rate(items, pairs, 1.0e9, threads)
+        rate, n, pd, secs, outs = cpu_stratified(items, lambda i: pairs[i], threads, args.cpu_rounds,
+                                                 keep_outputs=True)
         result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                  "sample": f"leading {n} of the 64 pairs ({pd / 1e6:.0f} M pd, "
-                                            f"{secs:.1f} s), oracle with {threads} threads"}
+                                  "sample": stratified_sample_text(items, n, pd, secs, threads)}
+        # Parity of the timed batch: the sampled pairs' oracle results against the
+        # batched run's (integer disparity exact, subpixel within 1e-4 px).
+        int_ok, sub = True, 0.0
+        for i, (d, di, _) in outs.items():
+            gf, gi = batch_out[i]
+            int_ok &= bool(np.array_equal(gi, di))
+            sub = max(sub, float(np.abs(gf.astype(np.float64) - d.astype(np.float64)).max()))
+        result["parity"] = {"pairs_checked": len(outs), "of": len(items), "against": "oracle",
+                            "integer_exact": int_ok, "subpixel_max_abs_diff_px": sub,
+                            "subpixel_tolerance_px": 1e-4, "ok": int_ok and sub <= 1e-4}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if dist is not None:

@@ -268,6 +268,8 @@ typedef struct vx_server_stats {
     uint64_t max_pinned_alloc_us;         /* longest pinned allocation past the arena */
     uint64_t staging_overflows;           /* requests staged past the pinned arena */
     uint64_t shadow_reruns;               /* requests recomputed after their escape pool ran out */
+    uint64_t max_batches_in_flight;       /* most batches unfinished on the GPU at once, counted
+                                             when a batch is launched (itself included) */
 } vx_server_stats;
 
 vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config* cfg,
@@ -414,6 +416,10 @@ vx_status vx_stereo_matcher_run_frames_device(vx_stereo_matcher* matcher, vx_ctx
 
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);
+/* Number of memory allocations this library has requested since load (all
+ * threads): device pool allocations, cudaMalloc*, pinned host cudaMallocHost.
+ * Lets a caller check that a call allocated nothing. */
+uint64_t vx_memory_allocation_count(void);
 
 #ifdef __cplusplus
 }

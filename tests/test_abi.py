@@ -101,3 +101,60 @@ def test_status_names_cover_header():
     src = open(os.path.join(REPO, "include", "vx_sgm.h")).read()
     codes = {int(v): k for k, v in re.findall(r"(VX_(?:OK|ERR_\w+))\s*=\s*(\d+)", src)}
     assert codes == vx_sgm.STATUS_NAMES
+
+
+def test_noalloc_rejects_misaligned_outputs_before_any_launch():
+    """vx_sgm_compute_disparity_noalloc checks the output planes' alignment itself
+    (the WTA kernel stores whole floats and int16s): an odd pointer or pitch is
+    VX_ERR_INVALID_ARGUMENT, returned before any device work. The pointers here are
+    never dereferenced."""
+    lib = ctypes.CDLL(vx_sgm.LIB_PATH)
+    fn = lib.vx_sgm_compute_disparity_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32,
+                   ctypes.c_uint32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                   ctypes.c_void_p, ctypes.c_void_p]
+    cfg = vx_sgm.SGMStereoConfig(num_disparities=16).to_c()
+    w, h = 33, 8
+    launches = vx_sgm.kernel_launch_count()
+    base = 1 << 20                                    # aligned stand-in addresses
+    cases = [
+        (base + 2, 4 * w, 0, 0),                      # f32 plane not 4-byte aligned
+        (base, 4 * w + 2, 0, 0),                      # f32 pitch not a multiple of 4
+        (base, 4 * w, base + 1, 2 * w),               # i16 plane not 2-byte aligned
+        (base, 4 * w, base, 2 * w + 1),               # i16 pitch odd
+    ]
+    for f32, f32_pitch, i16, i16_pitch in cases:
+        r = fn(base, w, base, w, w, h, f32, f32_pitch, i16 or None, i16_pitch, ctypes.addressof(cfg), None)
+        assert r == 10, (f32, f32_pitch, i16, i16_pitch)        # VX_ERR_INVALID_ARGUMENT
+        assert "misaligned" in vx_sgm.last_error()
+    assert vx_sgm.kernel_launch_count() == launches
+
+
+def test_noalloc_wrapper_checks_sizes_and_formats():
+    """The Python wrapper passes one width and height for all planes, so it rejects
+    textures of other sizes or formats before calling the library."""
+    T = vx_sgm.Texture
+    left = T(None, None, 40, 20, vx_sgm.FORMAT_U8)
+    right = T(None, None, 40, 20, vx_sgm.FORMAT_U8)
+    out = T(None, None, 40, 20, vx_sgm.FORMAT_F32)
+    cfg = vx_sgm.SGMStereoConfig(num_disparities=16)
+    bad = [
+        dict(right=T(None, None, 39, 20, vx_sgm.FORMAT_U8)),              # narrower right image
+        dict(output=T(None, None, 40, 19, vx_sgm.FORMAT_F32)),            # shorter output
+        dict(output_i16=T(None, None, 20, 20, vx_sgm.FORMAT_I16)),        # smaller integer output
+        dict(output=T(None, None, 40, 20, vx_sgm.FORMAT_I16)),            # wrong output format
+        dict(right=T(None, None, 40, 20, vx_sgm.FORMAT_F32)),             # wrong input format
+        dict(output_i16=T(None, None, 40, 20, vx_sgm.FORMAT_F32)),
+    ]
+    for b in bad:
+        args = dict(left=left, right=right, output=out, output_i16=None, **{})
+        args.update(b)
+        with pytest.raises(vx_sgm.VxError) as e:
+            vx_sgm.compute_disparity_noalloc(args["left"], args["right"], args["output"], cfg,
+                                             output_i16=args["output_i16"])
+        assert e.value.status in (5, 10), b      # VX_ERR_SIZE_MISMATCH / VX_ERR_INVALID_ARGUMENT
+
+
+def test_allocation_counter_is_exported():
+    assert vx_sgm.memory_allocation_count() >= 0

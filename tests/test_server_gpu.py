@@ -38,6 +38,24 @@ def test_served_results_equal_solo(gpu_ctx, sgm):
         assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="served vs solo")
 
 
+def test_batches_overlap_on_the_device(gpu_ctx, sgm):
+    """Continuous batching: with memory for two batches and two stream slots, a batch is
+    launched while the previous one is still running on the GPU (the server counts the
+    unfinished batches at every launch), and every result still equals the solo result."""
+    reqs = [_request(i) for i in range(3, 3 + 16)]
+    biggest = max(vx_sgm.workspace_bytes(L.shape[1], L.shape[0], c) for L, _, c in reqs)
+    srv = vx_sgm.Server(sgm, gpu_ctx, memory_budget_bytes=10 * biggest, max_batch=4,
+                        max_inflight_batches=2)
+    ids = [srv.submit(L, R, c) for L, R, c in reqs]
+    results = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["failed"] == 0 and st["batches"] >= 4
+    assert st["max_batches_in_flight"] == 2, st
+    for (L, R, c), (d, di, _) in zip(reqs, results):
+        assert_disparity_equal((d, di), run_pair(gpu_ctx, sgm, L, R, c), tol=0.0, what="overlapped vs solo")
+
+
 @pytest.mark.parametrize("pool", [None, "1"])
 def test_escape_pool_and_reruns(gpu_ctx, sgm, monkeypatch, pool):
     """Served requests keep their escaped path vectors in a pool of 1/16 of their

@@ -85,6 +85,7 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
         if (st != VX_OK) break;
         key = tune_key(plan);
         char* ws = nullptr;
+        count_alloc();
         cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool,
                                                 ctx->stream);
         if (e != cudaSuccess) {

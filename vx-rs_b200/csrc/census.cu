@@ -8,10 +8,12 @@
 //
 // Layout: each 32x8 tile of one view is staged once in shared memory with its
 // (rx, ry) apron (clamped coordinates), then every thread builds one
-// descriptor from shared memory. Descriptors are written twice: row-major
-// (read by vertical and diagonal paths) and in 32-row bands, x-major inside a
-// band, word (x, y) at ((y/32)*W + x)*32 + y%32 (read by horizontal paths: the
-// 32 scanlines of a warp are the 32 rows of a band, so each column is 128
+// descriptor from shared memory. Descriptors are written row-major (read by
+// the cost-volume kernel and by the vertical and diagonal paths of the
+// single-scanline aggregation) and, for batches run by the single-scanline
+// aggregation only, a second time in 32-row bands, x-major inside a band, word
+// (x, y) at ((y/32)*W + x)*32 + y%32 (read by its horizontal paths: the 32
+// scanlines of a warp are the 32 rows of a band, so each column is 128
 // contiguous bytes). Output word: u32 when the window has <= 32 bits, else u64.
 #include <cuda_runtime.h>
 
@@ -56,7 +58,7 @@ __device__ __forceinline__ uint64_t window_bits(const uint8_t* __restrict__ tile
     return bits;
 }
 
-template <typename CT>
+template <typename CT, bool BANDED>
 __global__ void __launch_bounds__(kCensusTileW * kCensusTileH)
 census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint8_t tile_px[];
@@ -93,8 +95,9 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, sw, cx, cy, rx, ry);
     else bits = window_bits<-1, -1>(tile_px, sw, cx, cy, rx, ry);
     CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
-    CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
     if (x < W && y < H) rm[(size_t)y * W + x] = (CT)bits;
+    if constexpr (!BANDED) return;   // the scanline-pair aggregation reads the cost volume instead
+    CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
     // Banded copy: the tile's 8 rows of one column are 8 consecutive words
     // there, so the descriptors go through shared memory and thread t writes
     // column t / 8, row t % 8: eight threads fill one contiguous run.
@@ -109,15 +112,18 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
 }  // namespace
 
 cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
-                          int max_ry, bool census64, cudaStream_t stream) {
+                          int max_ry, bool census64, bool banded, cudaStream_t stream) {
     if (total_tiles == 0) return cudaSuccess;
     const dim3 block(kCensusTileW, kCensusTileH);
     const size_t smem = (size_t)(kCensusTileW + 2 * max_rx) * (kCensusTileH + 2 * max_ry);
     count_launch();
-    if (census64)
-        census_kernel<uint64_t><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
-    else
-        census_kernel<uint32_t><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+    if (census64) {
+        if (banded) census_kernel<uint64_t, true><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+        else census_kernel<uint64_t, false><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+    } else {
+        if (banded) census_kernel<uint32_t, true><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+        else census_kernel<uint32_t, false><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);
+    }
     return cudaGetLastError();
 }
 

@@ -8,6 +8,7 @@
 namespace vxsgm {
 
 std::atomic<uint64_t> g_kernel_launches{0};
+std::atomic<uint64_t> g_memory_allocs{0};
 
 namespace {
 thread_local std::string t_last_error;
@@ -49,6 +50,8 @@ extern "C" {
 const char* vx_last_error(void) { return t_last_error.c_str(); }
 
 uint64_t vx_kernel_launch_count(void) { return g_kernel_launches.load(); }
+
+uint64_t vx_memory_allocation_count(void) { return g_memory_allocs.load(); }
 
 vx_status vx_ctx_create(int device_ordinal, vx_ctx** out) {
     if (!out) return fail(VX_ERR_INVALID_ARGUMENT, "vx_ctx_create: out is NULL");
@@ -188,6 +191,7 @@ vx_status vx_image_create(vx_ctx* ctx, uint32_t width, uint32_t height, vx_forma
     DeviceGuard g(ctx->device);
     void* ptr = nullptr;
     size_t pitch = 0;
+    count_alloc();
     cudaError_t e = cudaMallocPitch(&ptr, &pitch, (size_t)width * eb, height);
     if (e != cudaSuccess) {
         cudaGetLastError();

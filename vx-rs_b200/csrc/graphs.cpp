@@ -72,6 +72,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
         e->key = key;
         st = sgm->plan_batch(specs, &e->plan);
         if (st == VX_OK) {
+            count_alloc();
             err = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&e->ws), e->plan.ws_bytes, ctx->pool,
                                           stream);
             if (err != cudaSuccess) {

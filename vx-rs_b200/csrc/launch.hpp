@@ -12,10 +12,15 @@ namespace vxsgm {
 // Kernel launches issued by this library since load (bench/test evidence).
 extern std::atomic<uint64_t> g_kernel_launches;
 inline void count_launch(uint64_t n = 1) { g_kernel_launches.fetch_add(n, std::memory_order_relaxed); }
+// Device and pinned-host memory allocations this library has requested since
+// load (pool allocations, cudaMalloc*, cudaMallocHost), successful or not.
+extern std::atomic<uint64_t> g_memory_allocs;
+inline void count_alloc() { g_memory_allocs.fetch_add(1, std::memory_order_relaxed); }
 
-// Census of both views of every pair: one CTA per 32x8 tile.
+// Census of both views of every pair: one CTA per 32x8 tile. banded: also
+// write the 32-row banded copy (read only by the single-scanline aggregation).
 cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
-                          int max_ry, bool census64, cudaStream_t stream);
+                          int max_ry, bool census64, bool banded, cudaStream_t stream);
 
 // Matching-cost volume of every pair (cost.cu), for batches run by the
 // scanline-pair kernel: one CTA per image row of the batch.

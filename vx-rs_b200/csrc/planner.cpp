@@ -353,7 +353,8 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     unsigned* counters = reinterpret_cast<unsigned*>(base + pl.off_counters);
 
     if (ev) record(ev[0]);
-    e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64, stream);
+    e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64,
+                      pl.unit_scanlines != kUnitScanlines, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) record(ev[1]);
     if (pl.unit_scanlines == kUnitScanlines) {

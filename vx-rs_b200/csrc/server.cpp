@@ -202,6 +202,7 @@ bool vx_sgm_server::host_get(Request* r) {
     // Staging arena full: pin a buffer for this request alone (slow path).
     const auto t0 = Clock::now();
     void* p = nullptr;
+    count_alloc();
     if (cudaMallocHost(&p, r->host_bytes) != cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -423,11 +424,18 @@ void vx_sgm_server::run() {
             }
         }
         if (!batch.empty()) {
+            // Batches of other slots still running on the GPU when this one is
+            // issued: their work and this batch's can overlap on the device.
+            uint64_t in_flight = 1;
+            for (Slot& o : slots)
+                if (&o != free_slot && o.busy && cudaEventQuery(o.done) == cudaErrorNotReady) ++in_flight;
+            cudaGetLastError();
             const auto t0 = Clock::now();
             launch(*free_slot, batch);
             const uint64_t us = (uint64_t)(ms_since(t0, Clock::now()) * 1e3);
             std::lock_guard<std::mutex> lk(mu);
             stats.max_launch_us = std::max(stats.max_launch_us, us);
+            stats.max_batches_in_flight = std::max(stats.max_batches_in_flight, in_flight);
             stats.inflight_bytes = dev_alloc.used();
         }
     }
@@ -475,6 +483,7 @@ vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config*
     for (auto& sl : s->slots) {
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        count_alloc();
         if (e == cudaSuccess)
             e = cudaMallocHost(reinterpret_cast<void**>(&sl.esc_host), 2 * sizeof(uint32_t) * cfg->max_batch);
         if (e != cudaSuccess) {
@@ -484,6 +493,7 @@ vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config*
         }
     }
     // The device arena: the whole budget, held for the server's lifetime.
+    count_alloc();
     cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->dev_arena), s->budget, ctx->pool,
                                             ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -498,6 +508,7 @@ vx_status vx_sgm_server_create(vx_sgm* sgm, vx_ctx* ctx, const vx_server_config*
     size_t staging = cfg->host_staging_bytes;
     if (staging == 0) staging = std::min<size_t>(std::max<size_t>(s->budget / 16, 256u << 20), (size_t)4 << 30);
     staging = block_align(staging);
+    count_alloc();
     if (cudaMallocHost(reinterpret_cast<void**>(&s->host_arena), staging) != cudaSuccess) {
         cudaGetLastError();
         s->host_arena = nullptr;

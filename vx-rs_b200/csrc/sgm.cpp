@@ -47,6 +47,7 @@ vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs
     }
     DeviceGuard g(ctx->device);
     char* ws = nullptr;
+    count_alloc();
     cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -82,6 +82,14 @@ extern "C" vx_status vx_sgm_compute_disparity_noalloc(
     if (left_pitch < width || right_pitch < width || out_f32_pitch < width * sizeof(float) ||
         (out_i16 && out_i16_pitch < width * sizeof(int16_t)))
         return fail(VX_ERR_INVALID_ARGUMENT, "compute_disparity_noalloc: pitch smaller than a row");
+    // The WTA kernel stores whole floats and int16s: a plane or pitch that is not
+    // a multiple of the element size would make it store to misaligned addresses
+    // (the same rule vx_image_wrap_device applies to caller-owned planes).
+    if ((uintptr_t)out_f32 % sizeof(float) != 0 || out_f32_pitch % sizeof(float) != 0 ||
+        (out_i16 && ((uintptr_t)out_i16 % sizeof(int16_t) != 0 || out_i16_pitch % sizeof(int16_t) != 0)))
+        return fail(VX_ERR_INVALID_ARGUMENT,
+                    "compute_disparity_noalloc: misaligned output plane (F32 planes and pitches must be "
+                    "multiples of 4 bytes, I16 ones of 2)");
 
     // Plain descriptors of the caller's planes (no device allocation behind them).
     vx_image l{}, r{}, of{}, oi{};

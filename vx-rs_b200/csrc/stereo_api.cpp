@@ -52,6 +52,7 @@ vx_status ensure_scratch(vx_stereo_matcher* m, uint32_t n_left, const StereoMatc
         if (m->scratch) cudaFreeAsync(m->scratch, stream);
         m->scratch = nullptr;
         m->cap_left = m->cap_tiles = 0;
+        count_alloc();
         cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->scratch),
                                                 (cap_left + 2 * cap_tiles) * sizeof(uint32_t), m->ctx->pool, stream);
         if (e != cudaSuccess) return cuda_fail(e, "stereo matcher scratch");
@@ -95,6 +96,7 @@ vx_status ensure_band(vx_stereo_matcher* m, uint32_t n_right, cudaStream_t strea
         if (m->band) cudaFreeAsync(m->band, stream);
         m->band = nullptr;
         m->band_cap_right = 0;
+        count_alloc();
         cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->band), kBandTableBytes + 44 * cap,
                                                 m->ctx->pool, stream);
         if (e != cudaSuccess) return cuda_fail(e, "stereo matcher band scratch");
@@ -278,6 +280,7 @@ vx_status vx_stereo_matcher_run_frames_device(vx_stereo_matcher* m, vx_ctx* ctx,
         if (m->frame_offsets) cudaFreeAsync(m->frame_offsets, s);
         m->frame_offsets = nullptr;
         m->frame_offsets_cap = 0;
+        count_alloc();
         cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->frame_offsets), cap * sizeof(uint32_t),
                                                 ctx->pool, s);
         if (e != cudaSuccess) return cuda_fail(e, "stereo frames offsets");
@@ -343,6 +346,7 @@ vx_status vx_stereo_matcher_run(vx_stereo_matcher* m, vx_ctx* ctx, const vx_corn
         }
         m->host_io = nullptr;
         m->host_io_bytes = 0;
+        count_alloc();
         if (cudaMallocHost(reinterpret_cast<void**>(&m->host_io), total) != cudaSuccess)
             return fail(VX_ERR_BUFFER_ALLOC, "stereo match: %zu bytes of pinned staging", total);
         m->host_io_bytes = total;
@@ -351,6 +355,7 @@ vx_status vx_stereo_matcher_run(vx_stereo_matcher* m, vx_ctx* ctx, const vx_corn
         if (m->dev_io) cudaFreeAsync(m->dev_io, s);
         m->dev_io = nullptr;
         m->dev_io_bytes = 0;
+        count_alloc();
         cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&m->dev_io), total, ctx->pool, s);
         if (e != cudaSuccess) return cuda_fail(e, "stereo match device staging");
         m->dev_io_bytes = total;

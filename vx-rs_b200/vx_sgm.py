@@ -23,7 +23,6 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvx_sgm.so")
-SYNTH_PATH = os.path.join(_HERE, "libvx_synth.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}` "
@@ -100,6 +99,7 @@ def _sig(name, restype, *argtypes):
 
 _last_error = _sig("vx_last_error", ctypes.c_char_p)
 _launch_count = _sig("vx_kernel_launch_count", ctypes.c_uint64)
+_alloc_count = _sig("vx_memory_allocation_count", ctypes.c_uint64)
 _ctx_create = _sig("vx_ctx_create", ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P))
 _ctx_destroy = _sig("vx_ctx_destroy", None, _P)
 _ctx_stream = _sig("vx_ctx_stream", _P, _P)
@@ -157,6 +157,12 @@ def last_error() -> str:
 def kernel_launch_count() -> int:
     """Kernel launches this library has issued since it was loaded."""
     return int(_launch_count())
+
+
+def memory_allocation_count() -> int:
+    """Device and pinned-host memory allocations this library has requested since it
+    was loaded (pool allocations, cudaMalloc*, cudaMallocHost)."""
+    return int(_alloc_count())
 
 
 @dataclass
@@ -636,7 +642,8 @@ class ServerStats(ctypes.Structure):
                 ("completed_pixel_disparities", ctypes.c_uint64),
                 ("pool_reserved_bytes", ctypes.c_uint64), ("pinned_bytes", ctypes.c_uint64),
                 ("max_launch_us", ctypes.c_uint64), ("max_pinned_alloc_us", ctypes.c_uint64),
-                ("staging_overflows", ctypes.c_uint64), ("shadow_reruns", ctypes.c_uint64)]
+                ("staging_overflows", ctypes.c_uint64), ("shadow_reruns", ctypes.c_uint64),
+                ("max_batches_in_flight", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -717,7 +724,21 @@ def compute_disparity_noalloc(left: Texture, right: Texture, output: Texture,
                               config: SGMStereoConfig, output_i16: Texture | None = None,
                               stream: int | None = None):
     """vx_sgm_compute_disparity_noalloc on the planes of existing textures: for callers that
-    cannot allocate device memory during the call (scratch is a static 64 MiB device array)."""
+    cannot allocate device memory during the call (scratch is a static 64 MiB device array).
+
+    The C entry point takes one width and height for all four planes, so the
+    textures' sizes and formats are checked here: U8 left and right, F32 output,
+    I16 integer output, all of the left image's size (VX_ERR_SIZE_MISMATCH /
+    VX_ERR_INVALID_ARGUMENT otherwise, raised before anything runs)."""
+    planes = [("left", left, FORMAT_U8), ("right", right, FORMAT_U8), ("output", output, FORMAT_F32)]
+    if output_i16 is not None:
+        planes.append(("output_i16", output_i16, FORMAT_I16))
+    for name, tex, fmt in planes:
+        if tex.format != fmt:
+            raise VxError(10, f"compute_disparity_noalloc: {name} has format {tex.format}, expected {fmt}")
+        if (tex.width, tex.height) != (left.width, left.height):
+            raise VxError(5, f"compute_disparity_noalloc: {name} is {tex.width}x{tex.height}, "
+                             f"left is {left.width}x{left.height}")
     c = config.to_c()
     _check(_sgm_noalloc(_P(left.device_ptr), left.pitch, _P(right.device_ptr), right.pitch,
                         left.width, left.height, _P(output.device_ptr), output.pitch,
@@ -737,26 +758,7 @@ def workspace_bytes(width: int, height: int, config: SGMStereoConfig) -> int:
 
 # ---------------------------------------------------------------------------
 # Synthetic pairs (libvx_synth.so): R(x - d, y) = L(x, y), the shader's convention.
-SCENE_PLANES, SCENE_SLANTED, SCENE_SURFACE = 0, 1, 2
-_synth = None
-
-
-def synth_pair(scene: int, width: int, height: int, d_lo: float, d_hi: float, seed: int):
-    """Returns (left u8, right u8, ground-truth disparity f32), each (H, W)."""
-    global _synth
-    if _synth is None:
-        _synth = ctypes.CDLL(SYNTH_PATH)
-        _synth.vx_synth_pair.restype = ctypes.c_int
-        _synth.vx_synth_pair.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
-                                         ctypes.c_float, ctypes.c_uint64, _P, _P, _P]
-    L = np.empty((height, width), np.uint8)
-    R = np.empty((height, width), np.uint8)
-    G = np.empty((height, width), np.float32)
-    r = _synth.vx_synth_pair(scene, width, height, d_lo, d_hi, seed, L.ctypes.data,
-                             R.ctypes.data, G.ctypes.data)
-    if r != 0:
-        raise ValueError("vx_synth_pair rejected its arguments")
-    return L, R, G
+from vx_synth import SCENE_PLANES, SCENE_SLANTED, SCENE_SURFACE, synth_pair  # noqa: E402,F401
 
 
 def synth_orb_stereo(n_left: int, n_right: int, seed: int, width: int = 752, height: int = 480,
