@@ -121,3 +121,32 @@ def test_stage_times_through_graphs(gpu_ctx, monkeypatch, form):
         assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what=f"graph {form}")
     sgm.set_graph_cache(0)
     sgm.close()
+
+
+@pytest.mark.parametrize("warpgroups", [1, 2, 3, 4])
+def test_queue_classes_match_the_oracle(gpu_ctx, monkeypatch, warpgroups):
+    """The scanline-pair kernel on a batch mixing D = 192, 128 and 64 with every CTA
+    size: from 3 warpgroups up the warpgroups get TMEM budgets of different disparity
+    classes (e.g. 192 + 192 + 128 columns) and the units come from one queue per
+    class, so warps of a smaller budget never run a unit of a larger D. Every pair
+    equals the oracle."""
+    import oracle
+    from gpu_helpers import cfg_pair
+    monkeypatch.setenv("VX_SGM_AGG_FORM", "pairs")
+    monkeypatch.setenv("VX_SGM_AGG_WARPGROUPS", str(warpgroups))
+    rng = np.random.default_rng(21)
+    pairs, cfgs, ocfgs = [], [], []
+    for i in range(12):
+        w, h = int(rng.choice([97, 160, 233])), int(rng.choice([40, 75, 130]))
+        nd = [192, 128, 64, 100][i % 4]
+        L, R, _ = vx_sgm.synth_pair(i % 3, w, h, 0, nd - 8, 700 + i)
+        pairs.append((L, R))
+        c, o = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2, num_paths=8, lr_check=True)
+        cfgs.append(c)
+        ocfgs.append(o)
+    sgm = vx_sgm.SGMStereo(gpu_ctx)
+    got = run_batch(gpu_ctx, sgm, pairs, cfgs)
+    sgm.close()
+    for k, ((L, R), o, g) in enumerate(zip(pairs, ocfgs, got)):
+        d, di, _ = oracle.sgm(L, R, o)
+        assert_disparity_equal(g, (d, di), what=f"pair {k} D={o.num_disparities} with {warpgroups} warpgroups")

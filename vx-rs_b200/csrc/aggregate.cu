@@ -55,6 +55,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
 
 #include "kernels.cuh"
 #include "launch.hpp"
@@ -548,11 +549,18 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
 
 }  // namespace
 
+// Unit range of queue class c (c < kMaxQueueClasses), read with constant
+// indices so that the parameter struct stays in the constant bank.
+__device__ __forceinline__ void class_range(const AggQueues& q, int c, int& b, int& e) {
+    b = c == 0 ? q.begin[0] : c == 1 ? q.begin[1] : c == 2 ? q.begin[2] : q.begin[3];
+    e = c == 0 ? q.begin[1] : c == 1 ? q.begin[2] : c == 2 ? q.begin[3] : q.begin[4];
+}
+
 template <bool WT, bool CP>
 __global__ void __launch_bounds__(kAggMaxThreads)
 aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs,
-                 const UnitDev* __restrict__ units, int num_units, unsigned* __restrict__ counter,
-                 int dp_max, int tmem_cols, int wg_cols) {
+                 const UnitDev* __restrict__ units, const AggQueues q, unsigned* __restrict__ counters,
+                 int dp_max, int tmem_cols) {
     extern __shared__ __align__(16) unsigned char agg_smem[];
     __shared__ uint32_t tmem_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -565,7 +573,7 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     // TMEM for the state of all the CTA's scanlines, allocated by warp 0 for the
     // whole persistent loop and released by warp 0 after every warp is done.
     // Warp w owns TMEM lanes 32*(w%4).. (its lane quarter) and, inside them, the
-    // columns of its warpgroup w/4: [ (w/4)*wg_cols, (w/4+1)*wg_cols ).
+    // columns of its warpgroup w/4, from q.col0[w/4] on (its class budget).
     if (warp == 0) {
         const unsigned slot = (unsigned)__cvta_generic_to_shared(&tmem_base);
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
@@ -575,15 +583,23 @@ aggregate_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ j
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tstate =
-        tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * wg_cols);
+    const int wg = warp >> 2;
+    const int col0 = wg == 0 ? q.col0[0] : wg == 1 ? q.col0[1] : wg == 2 ? q.col0[2] : q.col0[3];
+    const uint32_t tstate = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col0;
 
+    int c = wg == 0 ? q.first_class[0] : wg == 1 ? q.first_class[1] : wg == 2 ? q.first_class[2] : q.first_class[3];
+    int cb, ce;
+    class_range(q, c, cb, ce);
     for (;;) {
         int u = 0;
-        if (lane == 0) u = (int)atomicAdd(counter, 1u);
+        if (lane == 0) u = (int)atomicAdd(&counters[c], 1u);
         u = __shfl_sync(kFull, u, 0);
-        if (u >= num_units) break;
-        const UnitDev unit = units[u];
+        if (u >= ce - cb) {          // this class is empty: the next smaller one
+            if (++c >= q.n_classes) break;
+            class_range(q, c, cb, ce);
+            continue;
+        }
+        const UnitDev unit = units[cb + u];
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         if (job.dy == 0)
@@ -609,22 +625,21 @@ const void* aggregate_kernel_fn(bool wide_tiles, bool compact) {
     return wide_tiles ? (const void*)aggregate_kernel<true, false> : (const void*)aggregate_kernel<false, false>;
 }
 
-// Launch shape of the aggregation kernel for a batch whose largest padded D is
-// dp_max: one CTA per SM (the CUDA occupancy calculator allows one CTA per SM
-// for a kernel that allocates tensor memory) with as many warpgroups as the
-// SM's 512 TMEM columns, registers and shared memory hold. A warpgroup's 4
-// warps cover the 128 TMEM lanes (256 scanlines) and need dp_max columns.
-struct AggShape {
-    int warpgroups;
-    int wg_cols;     // columns per warpgroup
-    int tmem_cols;   // allocation (power of two >= warpgroups * wg_cols)
-    size_t smem;     // output tiles (after a batch-dependent base offset)
-};
+// Launch shape of the aggregation kernel: one CTA per SM (the CUDA occupancy
+// calculator allows one CTA per SM for a kernel that allocates tensor memory)
+// with as many warpgroups as the SM's 512 TMEM columns, registers and shared
+// memory hold. A warpgroup's 4 warps cover the 128 TMEM lanes (256 scanlines)
+// and need one column per padded disparity of the units they run: its column
+// budget. Budgets are per warpgroup, so a batch mixing D = 192 with smaller D
+// can run three warpgroups (192 + 192 + 128 columns) where uniform budgets of
+// the largest D would allow two.
 
-// Largest number of warpgroups one aggregation CTA can hold for this batch:
-// bounded by the 512 TMEM columns, the registers and the shared memory of an SM.
-int max_warpgroups(int dp_max, bool wide_tiles) {
-    const int by_tmem = 512 / dp_max;
+// Largest number of warpgroups one aggregation CTA can hold for a batch whose
+// padded D lie in [dp_min, dp_max]: one budget of dp_max and the rest of the
+// 512 TMEM columns in budgets of dp_min, the registers, and the shared memory
+// of an SM (every warp's output tile is sized for dp_max).
+int max_warpgroups(int dp_max, int dp_min, bool wide_tiles) {
+    const int by_tmem = 1 + (512 - dp_max) / std::max(dp_min, 8);
     int regs = 128, regs_sm = 65536, dev = 0, smem_sm = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
@@ -640,31 +655,83 @@ int max_warpgroups(int dp_max, bool wide_tiles) {
     const int by_regs = regs_sm / (regs * 128);
     const int by_smem =
         (int)((smem_sm - 1024 - (int)aggregate_tile_offset(dp_max)) / (4 * aggregate_warp_smem(dp_max, wide_tiles)));
-    return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxThreads / 128}));
+    return std::max(1, std::min({by_tmem, by_regs, by_smem, kAggMaxWarpgroups}));
 }
 
-int default_warpgroups(int dp_max, bool wide_tiles, int num_units) {
-    // Most warpgroups that still leave every warp ~2.5 units of the queue: a
-    // scanline is serial work, so a crowded SM slows the longest units down and
-    // few units per warp cannot even that out.
+// Column budgets of `warpgroups` warpgroups for a batch whose units need the
+// padded disparity counts dps[0] > dps[1] > ... (n_dps distinct values) with
+// work[i] the share of the queued work (sum of longest scanline x D over the
+// units) of the units needing dps[i]. Budgets are non-increasing, each one of
+// dps (the first dps[0]), and sum to at most 512 columns. The units needing
+// dps[j] or more can only run on warpgroups whose budget is at least dps[j]:
+// with n_j such warpgroups out of W and a share F_j of the work, they need
+// F_j * W / n_j of the time a perfectly shared queue would take. The budgets
+// minimise the largest such ratio (ties: larger budgets, more flexible); the
+// ratio (>= 1) is returned, and the budgets in cols[0..warpgroups-1]. Returns
+// 0 when no budgets of that many warpgroups fit the 512 columns.
+double budgets_for(const int* dps, const double* work, int n_dps, int warpgroups, int* cols) {
+    double total = 0.0;
+    for (int i = 0; i < n_dps; ++i) total += work[i];
+    if (total <= 0.0) total = 1.0;
+    double best = 0.0;
+    int best_sum = -1;
+    int pick[kAggMaxWarpgroups] = {};
+    // Non-increasing index sequences pick[0] = 0 <= pick[1] <= ... < n_dps.
+    std::function<void(int, int, int)> rec = [&](int w, int lo, int sum) {
+        if (sum > 512) return;
+        if (w == warpgroups) {
+            double ratio = 0.0, cum = 0.0;
+            for (int j = 0; j < n_dps; ++j) {
+                cum += work[j] / total;
+                int n = 0;
+                for (int k = 0; k < warpgroups; ++k) n += dps[pick[k]] >= dps[j];
+                ratio = std::max(ratio, cum * warpgroups / n);
+            }
+            if (best_sum < 0 || ratio < best - 1e-9 || (ratio < best + 1e-9 && sum > best_sum)) {
+                best = ratio;
+                best_sum = sum;
+                for (int k = 0; k < warpgroups; ++k) cols[k] = dps[pick[k]];
+            }
+            return;
+        }
+        for (int i = lo; i < n_dps; ++i) {
+            pick[w] = i;
+            rec(w + 1, i, sum + dps[i]);
+        }
+    };
+    if (warpgroups < 1 || warpgroups > kAggMaxWarpgroups || n_dps < 1) return 0.0;
+    pick[0] = 0;
+    rec(1, 0, dps[0]);
+    return best_sum < 0 ? 0.0 : best;
+}
+
+int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, int num_units) {
+    // The count with the most balanced capacity (warpgroups / budgets_for's
+    // ratio), among those that still leave every warp ~2.5 units of the queue:
+    // a scanline is serial work, so a crowded SM slows the longest units down
+    // and few units per warp cannot even that out.
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int wmax = max_warpgroups(dp_max, wide_tiles);
-    int w = 1;
-    while (w < wmax && (double)num_units >= 2.5 * sms * 4 * (w + 1)) ++w;
-    return w;
+    const int wmax = max_warpgroups(dps[0], dps[n_dps - 1], wide_tiles);
+    int best_w = 1;
+    double best_cap = 0.0;
+    for (int w = 1; w <= wmax; ++w) {
+        if (w > 1 && (double)num_units < 2.5 * sms * 4 * w) break;
+        int cols[kAggMaxWarpgroups];
+        const double ratio = budgets_for(dps, work, n_dps, w, cols);
+        if (ratio <= 0.0) break;
+        const double cap = w / ratio;
+        if (cap > best_cap * 1.03) {
+            best_cap = cap;
+            best_w = w;
+        }
+    }
+    return best_w;
 }
 
-static AggShape shape_for(int dp_max, bool wide_tiles, int warpgroups) {
-    AggShape sh{};
-    sh.wg_cols = dp_max;
-    const int wmax = max_warpgroups(dp_max, wide_tiles);
-    sh.warpgroups = std::max(1, std::min(warpgroups, wmax));
-    sh.tmem_cols = 32;
-    while (sh.tmem_cols < sh.warpgroups * sh.wg_cols) sh.tmem_cols <<= 1;
-    sh.smem = aggregate_tile_offset(dp_max) + (size_t)sh.warpgroups * 4 * aggregate_warp_smem(dp_max, wide_tiles);
-    return sh;
+static size_t smem_for(int dp_max, bool wide_tiles, int warpgroups) {
+    return aggregate_tile_offset(dp_max) + (size_t)warpgroups * 4 * aggregate_warp_smem(dp_max, wide_tiles);
 }
 
 cudaError_t prepare() {
@@ -695,24 +762,28 @@ static int grid_ctas_for() {
     return sms;
 }
 
-cudaError_t launch(int dp_max, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
-                   const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
+cudaError_t launch(int dp_max, bool wide_tiles, const AggLaunch& L, const PairDev* d_pairs,
+                   const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counters,
                    cudaStream_t stream, bool compact) {
     if (num_units <= 0) return cudaSuccess;
-    if (warpgroups <= 0) warpgroups = default_warpgroups(dp_max, wide_tiles, num_units);
-    const AggShape sh = shape_for(dp_max, wide_tiles, warpgroups);
-    const int threads = sh.warpgroups * 128;
+    const int threads = L.warpgroups * 128;
+    const size_t smem = smem_for(dp_max, wide_tiles, L.warpgroups);
     int grid_ctas = grid_ctas_for();
     const int needed = (num_units + threads / 32 - 1) / (threads / 32);
     if (grid_ctas > needed) grid_ctas = needed;
-    if (std::getenv("VX_SGM_DEBUG"))
-        std::fprintf(stderr, "vx_sgm: aggregation (pairs) %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem\n",
-                     grid_ctas, sh.warpgroups, sh.tmem_cols, sh.smem);
+    if (std::getenv("VX_SGM_DEBUG")) {
+        std::fprintf(stderr, "vx_sgm: aggregation (pairs) %d CTAs x %d warpgroups, %d TMEM cols, %zu B smem, "
+                     "%d queue classes, columns from", grid_ctas, L.warpgroups, L.tmem_cols, smem, L.queues.n_classes);
+        for (int w = 0; w < L.warpgroups; ++w)
+            std::fprintf(stderr, " %d (class %d)", L.queues.col0[w], L.queues.first_class[w]);
+        std::fprintf(stderr, "\n");
+    }
     count_launch();
-    void* args[] = {&d_pairs, &d_jobs, &d_units, &num_units, &counter, &dp_max,
-                    const_cast<int*>(&sh.tmem_cols), const_cast<int*>(&sh.wg_cols)};
+    int tmem_cols = L.tmem_cols;
+    AggQueues q = L.queues;
+    void* args[] = {&d_pairs, &d_jobs, &d_units, &q, &counters, &dp_max, &tmem_cols};
     return cudaLaunchKernel(aggregate_kernel_fn(wide_tiles, compact), dim3(grid_ctas), dim3(threads),
-                            args, sh.smem, stream);
+                            args, smem, stream);
 }
 
 }  // namespace pairs
@@ -724,18 +795,17 @@ cudaError_t prepare_aggregate_kernels() {
     return e == cudaSuccess ? prepare_cost_kernels() : e;
 }
 
-int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool wide_tiles) {
-    return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, wide_tiles)
+int aggregate_max_warpgroups(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles) {
+    return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, dp_min, wide_tiles)
                                             : single::max_warpgroups(dp_max, census64);
 }
 
-cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, int warpgroups,
+cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, const AggLaunch& L,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                             int num_units, unsigned* counter, cudaStream_t stream, bool compact) {
+                             int num_units, unsigned* counters, cudaStream_t stream, bool compact) {
     if (unit_scanlines == kUnitScanlines)
-        return pairs::launch(dp_max, wide_tiles, warpgroups, d_pairs, d_jobs, d_units, num_units,
-                             counter, stream, compact);
-    return single::launch(dp_max, census64, warpgroups, d_pairs, d_jobs, d_units, num_units, counter, stream,
+        return pairs::launch(dp_max, wide_tiles, L, d_pairs, d_jobs, d_units, num_units, counters, stream, compact);
+    return single::launch(dp_max, census64, L.warpgroups, d_pairs, d_jobs, d_units, num_units, counters, stream,
                           compact);
 }
 

@@ -3,8 +3,11 @@
 // The path-aggregation kernel runs one CTA per SM holding 1..N warpgroups (each
 // scanline is serial work: more warps per SM raise throughput until the
 // longest scanlines, slowed by a crowded SM, dominate). The best count depends
-// on the batch: its largest disparity count, its census word width and how many
-// 64-scanline units it queues. vx_sgm_autotune_batch times every candidate on
+// on the batch: its largest and smallest disparity counts (the scanline-pair
+// kernel gives each warpgroup a TMEM budget for one disparity class, so a mix
+// of D can hold more warpgroups than its largest D alone), its census word
+// width and how many units it queues. Each candidate count is timed with the
+// plan built for it (its queue classes order the units). vx_sgm_autotune_batch times every candidate on
 // a real batch with CUDA events around the aggregation launch and records the
 // fastest in the SGMStereo handle; later batches with the same key use it. The
 // table is saved to / loaded from a small JSON file.
@@ -26,6 +29,7 @@ TuneKey tune_key(const Plan& plan) {
     k.census64 = plan.census64 ? 1 : 0;
     k.units_log2 = plan.units32 <= 0 ? 0 : (int)std::floor(std::log2((double)plan.units32));
     k.wide = plan.wide_tiles ? 1 : 0;
+    k.dp_min = plan.dp_min;
     return k;
 }
 
@@ -36,23 +40,21 @@ using namespace vxsgm;
 vx_status vx_sgm::plan_batch(const std::vector<PairSpec>& specs, Plan* plan) {
     vx_status st = build_plan(specs, plan);
     if (st != VX_OK) return st;
-    int unit = 0;
+    Tuned t{0, 0, 0.0f};
     {
         std::lock_guard<std::mutex> lk(tune_mu);
         auto it = tuned.find(tune_key(*plan));
-        if (it != tuned.end()) unit = it->second.unit_scanlines;
+        if (it != tuned.end()) t = it->second;
     }
-    if (unit != 0 && unit != plan->unit_scanlines && !std::getenv("VX_SGM_AGG_FORM")) {
+    if (t.warpgroups == 0) return st;          // not tuned: the planner's heuristic
+    int unit = t.unit_scanlines;
+    if (std::getenv("VX_SGM_AGG_FORM")) unit = plan->unit_scanlines;   // the forced form wins
+    if (unit != plan->unit_scanlines || t.warpgroups != plan->agg.warpgroups) {
+        const int wg = unit == t.unit_scanlines ? t.warpgroups : 0;
         *plan = Plan();
-        st = build_plan(specs, plan, unit);
+        st = build_plan(specs, plan, unit, wg);
     }
     return st;
-}
-
-int vx_sgm::warpgroups_for(const Plan& plan) {
-    std::lock_guard<std::mutex> lk(tune_mu);
-    auto it = tuned.find(tune_key(plan));
-    return it == tuned.end() || it->second.unit_scanlines != plan.unit_scanlines ? 0 : it->second.warpgroups;
 }
 
 extern "C" {
@@ -84,22 +86,28 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
         st = build_plan(specs, &plan, unit);
         if (st != VX_OK) break;
         key = tune_key(plan);
+        const size_t ws_bytes = plan.ws_bytes;   // the same for every launch shape
         char* ws = nullptr;
         count_alloc();
-        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool,
+        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), ws_bytes, ctx->pool,
                                                 ctx->stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            st = fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
+            st = fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", ws_bytes);
             break;
         }
-        bind_plan(plan, ws);
-        const int wmax = aggregate_max_warpgroups(plan.unit_scanlines, plan.dp_max, plan.census64,
+        const int wmax = aggregate_max_warpgroups(plan.unit_scanlines, plan.dp_max, plan.dp_min, plan.census64,
                                                   plan.wide_tiles);
         for (int w = 1; w <= wmax && st == VX_OK; ++w) {
+            // The plan of this launch shape (its queue classes order the units).
+            Plan shaped;
+            st = build_plan(specs, &shaped, unit, w);
+            if (st != VX_OK) break;
+            if (shaped.agg.warpgroups != w || shaped.ws_bytes != ws_bytes) continue;  // not a shape of its own
+            bind_plan(shaped, ws);
             double total = 0.0;
             for (uint32_t it = 0; it <= iterations && st == VX_OK; ++it) {  // first run untimed
-                st = run_plan(plan, ws, ctx->stream, ev, w);
+                st = run_plan(shaped, ws, ctx->stream, ev);
                 if (st != VX_OK) break;
                 e = cudaEventSynchronize(ev[4]);
                 float ms = 0.0f;
@@ -137,7 +145,7 @@ vx_status vx_sgm_tuning_save(vx_sgm* sgm, const char* path) {
     f << "{\"version\": 1, \"entries\": [";
     bool first = true;
     for (const auto& kv : sgm->tuned) {
-        f << (first ? "" : ", ") << "{\"dp_max\": " << kv.first.dp_max
+        f << (first ? "" : ", ") << "{\"dp_max\": " << kv.first.dp_max << ", \"dp_min\": " << kv.first.dp_min
           << ", \"census64\": " << kv.first.census64 << ", \"units_log2\": " << kv.first.units_log2
           << ", \"wide\": " << kv.first.wide << ", \"unit_scanlines\": " << kv.second.unit_scanlines
           << ", \"warpgroups\": " << kv.second.warpgroups
@@ -176,8 +184,10 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
             field(pos, end, "aggregate_ms", &ms);
             field(pos, end, "wide", &wide);
             field(pos, end, "unit_scanlines", &us);
-            if (wg >= 1 && dp >= 8 && (us == 32 || us == kUnitScanlines)) {
-                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide}] = {(int)us, (int)wg, (float)ms};
+            double dmin = dp;   // files without dp_min: batches of one D
+            field(pos, end, "dp_min", &dmin);
+            if (wg >= 1 && dp >= 8 && dmin >= 8 && dmin <= dp && (us == 32 || us == kUnitScanlines)) {
+                sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide, (int)dmin}] = {(int)us, (int)wg, (float)ms};
                 ++loaded;
             }
         }

@@ -35,7 +35,7 @@ std::string bucket_key(const std::vector<PairSpec>& specs) {
     }
     // The planner's overrides of the slab format and the aggregation form
     // change the plan for the same shapes.
-    for (const char* v : {"VX_SGM_SLAB_FORMAT", "VX_SGM_AGG_FORM"})
+    for (const char* v : {"VX_SGM_SLAB_FORMAT", "VX_SGM_AGG_FORM", "VX_SGM_AGG_WARPGROUPS"})
         if (const char* e = std::getenv(v)) k << v << '=' << e << ';';
     return k.str();
 }
@@ -94,8 +94,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
             if (err != cudaSuccess) st = cuda_fail(err, "beginning graph capture");
         }
         if (st == VX_OK) {
-            const vx_status lst = launch_plan(e->plan, e->ws, stream, e->baked,
-                                              sgm->warpgroups_for(e->plan), true);
+            const vx_status lst = launch_plan(e->plan, e->ws, stream, e->baked, true);
             err = cudaStreamEndCapture(stream, &e->graph);
             if (lst != VX_OK) st = lst;
             else if (err != cudaSuccess) st = cuda_fail(err, "ending graph capture");

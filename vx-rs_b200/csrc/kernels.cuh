@@ -111,6 +111,23 @@ constexpr int kUnitScanlines = 64;
 constexpr long long kPairKernelMinUnits = 7500;
 // Largest aggregation CTA (4 warpgroups); keeps registers per thread <= 128.
 constexpr int kAggMaxThreads = 512;
+constexpr int kAggMaxWarpgroups = kAggMaxThreads / 128;
+
+// Work queues of one aggregation launch. The units are ordered in classes of
+// decreasing padded D, each class longest-first; class c is the range
+// [begin[c], begin[c + 1]) of the unit table and has its own counter. Warpgroup
+// w keeps its scanlines' state in TMEM columns [col0[w], col0[w] + its budget)
+// and pulls units from class first_class[w] (the largest class its budget
+// holds) until that is empty, then from the next smaller class, and so on. A
+// batch of one D (or any single-class plan) has one queue in plain
+// longest-first order.
+constexpr int kMaxQueueClasses = 4;
+struct AggQueues {
+    int n_classes;
+    int begin[kMaxQueueClasses + 1];
+    int col0[kAggMaxWarpgroups];
+    int first_class[kAggMaxWarpgroups];
+};
 // Guard words before and after every row-major census plane: the aggregation
 // kernel stages aligned 16-byte chunks that may extend past the first and last
 // row by up to 256 + 72 words.

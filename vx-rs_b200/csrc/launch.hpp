@@ -28,27 +28,34 @@ cudaError_t prepare_cost_kernels();   // shared-memory limit; once per device
 cudaError_t launch_costs(const PairDev* d_pairs, int num_pairs, int total_rows, int dp_max, bool census64,
                          cudaStream_t stream);
 
-// Path aggregation: one persistent launch over `num_units` warp units of every
-// (pair, path) of a batch; warps pull units from `*counter` (zero on entry).
-// dp_max = largest padded disparity count of the batch. One CTA per SM with
-// `warpgroups` warpgroups (0 = default for this batch; clamped to what an SM
-// holds), sharing one tensor-memory allocation for the scanline state.
+// Path aggregation: one persistent launch over the warp units of every (pair,
+// path) of a batch. One CTA per SM with `L.warpgroups` warpgroups sharing one
+// tensor-memory allocation for the scanline state; warps pull units from the
+// plan's queue classes (L.queues, counters[c] per class, zero on entry).
+// dp_max / dp_min = largest / smallest padded disparity count of the batch.
 // Two forms, picked by the plan's unit size: units of kUnitScanlines (64)
-// scanlines run the scanline-pair kernel (aggregate.cu), units of 32 the
-// single-scanline kernel (aggregate_single.cu). wide_tiles: the batch has
-// wide-slab pairs. compact: the batch has pairs with a shadow pool (their
-// kernels write the escape slot into the byte rows).
+// scanlines run the scanline-pair kernel (aggregate.cu, per-warpgroup TMEM
+// budgets and class queues), units of 32 the single-scanline kernel
+// (aggregate_single.cu, one queue). wide_tiles: the batch has wide-slab pairs.
+// compact: the batch has pairs with a shadow pool (their kernels write the
+// escape slot into the byte rows).
+struct AggLaunch {
+    int warpgroups = 1;
+    int tmem_cols = 32;     // scanline-pair kernel: TMEM allocation (power of two >= the budgets' sum)
+    AggQueues queues{};
+};
 cudaError_t prepare_aggregate_kernels();  // shared-memory limits of both; once per device
-int aggregate_max_warpgroups(int unit_scanlines, int dp_max, bool census64, bool wide_tiles);
-cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, int warpgroups,
+int aggregate_max_warpgroups(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles);
+cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, const AggLaunch& L,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                             int num_units, unsigned* counter, cudaStream_t stream, bool compact = false);
+                             int num_units, unsigned* counters, cudaStream_t stream, bool compact = false);
 namespace pairs {
 cudaError_t prepare();
-int max_warpgroups(int dp_max, bool wide_tiles);
-int default_warpgroups(int dp_max, bool wide_tiles, int num_units);
-cudaError_t launch(int dp_max, bool wide_tiles, int warpgroups, const PairDev* d_pairs,
-                   const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counter,
+int max_warpgroups(int dp_max, int dp_min, bool wide_tiles);
+double budgets_for(const int* dps, const double* work, int n_dps, int warpgroups, int* cols);
+int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, int num_units);
+cudaError_t launch(int dp_max, bool wide_tiles, const AggLaunch& L, const PairDev* d_pairs,
+                   const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counters,
                    cudaStream_t stream, bool compact = false);
 }  // namespace pairs
 namespace single {

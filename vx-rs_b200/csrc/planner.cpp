@@ -4,6 +4,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
 
 #include "vx_internal.hpp"
 
@@ -122,7 +124,86 @@ vx_status validate_pair(const PairSpec& p) {
     return VX_OK;
 }
 
-vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines) {
+// The aggregation launch shape of a plan whose units are in longest-first
+// order, and the queue classes that go with it (units reordered class by
+// class, longest-first inside each class).
+//  * Single-scanline form: one queue; `warpgroups` or the default count.
+//  * Scanline-pair form: warpgroups with per-class TMEM column budgets
+//    (pairs::budgets_for); class c holds the units whose padded D is at most
+//    the c-th largest budget and above the next one. With one budget value
+//    there is one class and the order stays plainly longest-first.
+template <typename CostFn>
+vx_status plan_queues(Plan& pl, int warpgroups, CostFn unit_cost) {
+    AggLaunch& L = pl.agg;
+    L = AggLaunch{};
+    AggQueues& q = L.queues;
+    const int nu = (int)pl.units.size();
+    auto unit_dp = [&](const UnitDev& u) { return pl.pairs[pl.jobs[u.job].pair].nd_pad; };
+    if (pl.unit_scanlines != kUnitScanlines) {
+        const int wmax = single::max_warpgroups(pl.dp_max, pl.census64);
+        L.warpgroups = warpgroups > 0 ? std::min(warpgroups, wmax)
+                                      : single::default_warpgroups(pl.dp_max, pl.census64, nu);
+        q.n_classes = 1;
+        q.begin[1] = nu;
+        for (int w = 0; w < L.warpgroups; ++w) q.col0[w] = w * (pl.dp_max / 2);
+        return VX_OK;
+    }
+    // Distinct padded D of the units (descending) and their shares of the work.
+    std::vector<int> dps;
+    std::vector<double> work;
+    {
+        std::map<int, double, std::greater<int>> w;
+        for (const UnitDev& u : pl.units) w[unit_dp(u)] += (double)unit_cost(u);
+        for (const auto& kv : w) {
+            dps.push_back(kv.first);
+            work.push_back(kv.second);
+        }
+    }
+    if (dps.empty()) {
+        dps.push_back(pl.dp_max);
+        work.push_back(1.0);
+    }
+    const int nd = (int)dps.size();
+    const int wmax = pairs::max_warpgroups(dps[0], dps[nd - 1], pl.wide_tiles);
+    int wg = warpgroups > 0 ? std::min(warpgroups, wmax)
+                            : pairs::default_warpgroups(dps.data(), work.data(), nd, pl.wide_tiles, nu);
+    int cols[kAggMaxWarpgroups] = {};
+    while (wg > 1 && pairs::budgets_for(dps.data(), work.data(), nd, wg, cols) <= 0.0) --wg;
+    if (wg == 1) cols[0] = dps[0];
+    L.warpgroups = wg;
+    // Classes: the distinct budgets, largest first (at most kAggMaxWarpgroups <= kMaxQueueClasses).
+    std::vector<int> cls;
+    for (int w = 0; w < wg; ++w)
+        if (cls.empty() || cls.back() != cols[w]) cls.push_back(cols[w]);
+    q.n_classes = (int)cls.size();
+    int sum = 0;
+    for (int w = 0; w < wg; ++w) {
+        q.col0[w] = sum;
+        sum += cols[w];
+        q.first_class[w] = (int)(std::find(cls.begin(), cls.end(), cols[w]) - cls.begin());
+    }
+    L.tmem_cols = 32;
+    while (L.tmem_cols < sum) L.tmem_cols <<= 1;
+    if (L.tmem_cols > 512) return fail(VX_ERR_GPU, "planner: TMEM budgets of %d columns exceed 512", sum);
+    // Class of a unit: the last class whose budget still holds its padded D.
+    auto class_of = [&](const UnitDev& u) {
+        const int dp = unit_dp(u);
+        int c = 0;
+        while (c + 1 < (int)cls.size() && cls[c + 1] >= dp) ++c;
+        return c;
+    };
+    std::stable_sort(pl.units.begin(), pl.units.end(),
+                     [&](const UnitDev& a, const UnitDev& b) { return class_of(a) < class_of(b); });
+    for (int c = 0, i = 0; c < q.n_classes; ++c) {
+        q.begin[c] = i;
+        while (i < nu && class_of(pl.units[i]) == c) ++i;
+        q.begin[c + 1] = i;
+    }
+    for (int c = q.n_classes + 1; c <= kMaxQueueClasses; ++c) q.begin[c] = nu;
+    return VX_OK;
+}
+
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines, int warpgroups) {
     Plan& pl = *plan;
     pl = Plan{};
     const int n = (int)specs.size();
@@ -211,6 +292,7 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
             return fail(VX_ERR_GPU, "planner: pair layout and its size formula disagree");
 
         pl.dp_max = std::max(pl.dp_max, Dp);
+        pl.dp_min = i == 0 ? Dp : std::min(pl.dp_min, Dp);
         for (int p = 0; p < P; ++p) {
             JobDev j{};
             j.pair = i;
@@ -285,6 +367,13 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
         pl.units.resize(units.size());
         for (size_t i = 0; i < units.size(); ++i) pl.units[i] = units[order[i].second];
     }
+    // VX_SGM_AGG_WARPGROUPS=<n> forces the aggregation CTA size of plans that
+    // were not given one (the tests run mixed-D batches with several queue
+    // classes through it).
+    if (warpgroups <= 0)
+        if (const char* f = std::getenv("VX_SGM_AGG_WARPGROUPS")) warpgroups = (int)std::strtol(f, nullptr, 10);
+    const vx_status qs = plan_queues(pl, warpgroups, unit_cost);
+    if (qs != VX_OK) return qs;
 
     size_t off = 0;
     pl.off_pairs = off;
@@ -293,12 +382,12 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     off = align_up(off + pl.jobs.size() * sizeof(JobDev));
     pl.off_units = off;
     off = align_up(off + pl.units.size() * sizeof(UnitDev));
-    // Counters: the aggregation work queue, then per pair the escape pool's
+    // Counters: the aggregation work queues, then per pair the escape pool's
     // taken count and overflow flag (all cleared by every launch).
     pl.off_counters = off;
     for (int i = 0; i < n; ++i)
-        pl.pairs[i].esc_state = reinterpret_cast<uint32_t*>(off + sizeof(unsigned) * (1 + 2 * (size_t)i));
-    off = align_up(off + sizeof(unsigned) * (1 + 2 * (size_t)n));
+        pl.pairs[i].esc_state = reinterpret_cast<uint32_t*>(pl.off_escape() + sizeof(unsigned) * 2 * (size_t)i);
+    off = align_up(off + pl.counter_bytes());
     pl.off_data = off;
     pl.ws_bytes = off + data;
     return VX_OK;
@@ -335,8 +424,7 @@ vx_status upload_plan(const Plan& pl, char* base, cudaStream_t stream, bool pair
     return e == cudaSuccess ? VX_OK : cuda_fail(e, "uploading the batch plan");
 }
 
-vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev,
-                      int warpgroups, bool capturing) {
+vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev, bool capturing) {
     // Under stream capture the timing events become event-record nodes.
     auto record = [&](cudaEvent_t e) {
         if (!e) return;
@@ -345,7 +433,7 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     };
     const int n = (int)pl.pairs.size();
     if (n == 0) return VX_OK;
-    cudaError_t e = cudaMemsetAsync(base + pl.off_counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)n), stream);
+    cudaError_t e = cudaMemsetAsync(base + pl.off_counters, 0, pl.counter_bytes(), stream);
     if (e != cudaSuccess) return cuda_fail(e, "clearing the work and escape counters");
     const PairDev* d_pairs = reinterpret_cast<const PairDev*>(base + pl.off_pairs);
     const JobDev* d_jobs = reinterpret_cast<const JobDev*>(base + pl.off_jobs);
@@ -362,7 +450,7 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
         if (e != cudaSuccess) return cuda_fail(e, "cost volume launch");
     }
     if (ev) record(ev[2]);
-    e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, warpgroups, d_pairs, d_jobs, d_units,
+    e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, pl.agg, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream, pl.compact);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) record(ev[3]);
@@ -372,11 +460,10 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
     return VX_OK;
 }
 
-vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev,
-                   int warpgroups) {
+vx_status run_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent_t* ev) {
     vx_status st = upload_plan(pl, base, stream, false);
     if (st != VX_OK) return st;
-    return launch_plan(pl, base, stream, ev, warpgroups, false);
+    return launch_plan(pl, base, stream, ev, false);
 }
 
 }  // namespace vxsgm

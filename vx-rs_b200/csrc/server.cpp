@@ -328,9 +328,9 @@ void vx_sgm_server::launch(Slot& s, std::vector<Request*>& batch) {
         char* ws = dev_arena + s.block_off + buf_total;
         rebind_pointers(plan, specs);
         bind_plan(plan, ws);
-        st = run_plan(plan, ws, s.stream, ctx->next_timing_slot(), sgm->warpgroups_for(plan));
+        st = run_plan(plan, ws, s.stream, ctx->next_timing_slot());
         if (st == VX_OK) {
-            cudaError_t e = cudaMemcpyAsync(s.esc_host, ws + plan.off_counters + sizeof(unsigned),
+            cudaError_t e = cudaMemcpyAsync(s.esc_host, ws + plan.off_escape(),
                                             2 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream);
             if (e != cudaSuccess) st = cuda_fail(e, "server: escape flags download");
         }

@@ -54,7 +54,7 @@ vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs
         return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
     }
     bind_plan(plan, ws);
-    st = run_plan(plan, ws, stream, ctx->next_timing_slot(), sgm->warpgroups_for(plan));
+    st = run_plan(plan, ws, stream, ctx->next_timing_slot());
     if (keep_ws && st == VX_OK) {
         *keep_ws = ws;
     } else {

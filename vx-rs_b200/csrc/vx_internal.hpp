@@ -107,16 +107,24 @@ struct Plan {
     int unit_scanlines = 32;        // 64: scanline-pair kernel, 32: single-scanline kernel
     long long units32 = 0;          // units the plan has at 32 scanlines (tuning key)
     int dp_max = 8;                 // largest padded disparity count
+    int dp_min = 8;                 // smallest padded disparity count
     int total_tiles = 0, total_rows = 0, max_width = 0, max_rx = 0, max_ry = 0;
-    // Workspace layout (byte offsets from the workspace base).
+    AggLaunch agg;                  // aggregation launch shape and its queue classes (units ordered for it)
+    // Workspace layout (byte offsets from the workspace base). The counter block
+    // holds kMaxQueueClasses work-queue counters, then per pair the escape pool's
+    // taken count and overflow flag (all cleared by every launch).
     size_t off_pairs = 0, off_jobs = 0, off_units = 0, off_counters = 0, off_data = 0;
     size_t ws_bytes = 0;
     std::vector<size_t> pair_data_off;  // per pair: census + slabs
+    size_t off_escape() const { return off_counters + kMaxQueueClasses * sizeof(unsigned); }
+    size_t counter_bytes() const { return sizeof(unsigned) * (kMaxQueueClasses + 2 * pairs.size()); }
 };
 
 // unit_scanlines: 32 or 64 forces the aggregation form (the autotuner's
-// choice); 0 picks it from the amount of work.
-vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines = 0);
+// choice); 0 picks it from the amount of work. warpgroups: aggregation CTA
+// size (the autotuner's choice, clamped to what an SM holds); 0 picks it from
+// the batch. The unit queue is ordered for the chosen shape.
+vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_scanlines = 0, int warpgroups = 0);
 // Workspace bytes of one pair's census planes and path slabs with census words
 // of census_word_bytes (a batch uses 8-byte words for all its pairs as soon as
 // one needs them), and an upper bound of its share of the plan tables.
@@ -135,26 +143,27 @@ void bind_plan(Plan& plan, char* base);
 // with the workspace at `base` (plan must be bound to it).
 // stage_events: null, or vx_ctx::kStageEvents events recorded before census,
 // before the cost volume, before aggregation, before WTA and after WTA.
-// warpgroups: aggregation CTA size (0 = default).
-vx_status run_plan(const Plan& plan, char* base, cudaStream_t stream,
-                   cudaEvent_t* stage_events = nullptr, int warpgroups = 0);
+vx_status run_plan(const Plan& plan, char* base, cudaStream_t stream, cudaEvent_t* stage_events = nullptr);
 // The two halves of run_plan: copy the plan tables into the workspace (all of
 // them, or the pair table alone), and the launch sequence itself (which is
 // what a CUDA graph of the batch captures).
 vx_status upload_plan(const Plan& plan, char* base, cudaStream_t stream, bool pairs_only);
 vx_status launch_plan(const Plan& plan, char* base, cudaStream_t stream, cudaEvent_t* stage_events,
-                      int warpgroups, bool capturing);
+                      bool capturing);
 
 // Autotuning key of a batch: the best aggregation form and launch shape depend
-// on the largest padded D, the census word width, the tile format and the
-// amount of queued work (log2 of its 32-scanline units).
+// on the largest and smallest padded D (the TMEM budgets), the census word
+// width, the tile format and the amount of queued work (log2 of its
+// 32-scanline units).
 struct TuneKey {
     int dp_max;
     int census64;
     int units_log2;
     int wide;
+    int dp_min;
     bool operator<(const TuneKey& o) const {
         if (dp_max != o.dp_max) return dp_max < o.dp_max;
+        if (dp_min != o.dp_min) return dp_min < o.dp_min;
         if (census64 != o.census64) return census64 < o.census64;
         if (wide != o.wide) return wide < o.wide;
         return units_log2 < o.units_log2;
@@ -185,10 +194,9 @@ struct vx_sgm {
     };
     std::mutex tune_mu;
     std::map<vxsgm::TuneKey, Tuned> tuned;
-    // Plan of a batch in the autotuned form (the planner's heuristic when the
-    // batch's key was not tuned), and the tuned launch shape (0 = default).
+    // Plan of a batch in the autotuned form and launch shape (the planner's
+    // heuristic when the batch's key was not tuned).
     vx_status plan_batch(const std::vector<vxsgm::PairSpec>& specs, vxsgm::Plan* plan);
-    int warpgroups_for(const vxsgm::Plan& plan);
 
     // CUDA graphs per shape bucket (see graphs.cpp): a bucket is the list of
     // every pair's size and config; image pointers may differ between calls.
