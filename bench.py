@@ -386,6 +386,38 @@ def run_config_table(args, local_rank):
                           "hbm_gbs": gbs, "hbm_frac": gbs / peak}), flush=True)
     filt.close()
 
+    # The depth chain's ends: RGBA -> gray ingest (5 bytes a pixel) and depth map ->
+    # point cloud (4 bytes a pixel read, 36 bytes a point written), 1920x1080,
+    # 50 back-to-back calls each (the device-buffer form for the cloud).
+    rgba = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    tin, tgray = ctx.texture_rgba8(rgba, w, h), ctx.texture_output_gray8(w, h)
+    conv = vx_sgm.ColorConvert(ctx)
+    depth = rng.uniform(0.0, 13.3, (h, w)).astype(np.float32)     # ~75 % inside [0.1, 10]
+    tdep = ctx.texture_r32float(depth, w, h)
+    d2c = vx_sgm.DepthToCloud(ctx)
+    cfg = vx_sgm.DepthToCloudConfig()
+    pts = torch.empty(w * h * 9, dtype=torch.int32, device=torch.device("cuda", local_rank))
+    cnt = torch.zeros(1, dtype=torch.int32, device=torch.device("cuda", local_rank))
+    for name, run, nbytes in (
+            ("rgba_to_gray", lambda: conv.rgba_to_gray(ctx, tin, tgray, stream=ctx.stream), lambda: 5 * w * h),
+            ("depth_to_cloud", lambda: d2c.compute_device(ctx, tdep, None, 1000.0, 1000.0, 960.0, 540.0, cfg,
+                                                          pts.data_ptr(), w * h, cnt.data_ptr(), stream=ctx.stream),
+             lambda: 4 * w * h + 36 * int(cnt.item()))):
+        for _ in range(5):
+            run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(50):
+            run()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 50
+        gbs = nbytes() / (ms * 1e-3) / 1e9
+        print(json.dumps({"config": "depth-chain", "kernel": name, "image": f"{w}x{h}", "ms_per_call": ms,
+                          "gpx_per_s": w * h / (ms * 1e-3) / 1e9, "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                          **({"points": int(cnt.item())} if name == "depth_to_cloud" else {})}), flush=True)
+    d2c.close()
+
 
 # Sparse ORB stereo matching (StereoMatcher): the reference example's size
 # (examples/orb_stereo_benchmark.rs: <= 512 keypoints per side, EuRoC

@@ -65,8 +65,10 @@ vx_status vx_ctx_synchronize(vx_ctx* ctx);
 vx_status vx_ctx_set_workspace_limit(vx_ctx* ctx, size_t bytes);
 
 /* Image formats: R8Unorm input (texture.rs:38 from_gray8), R32Float output
- * (texture.rs:324 output_r32float), and an int16 integer-disparity map. */
-typedef enum vx_format { VX_FORMAT_U8 = 0, VX_FORMAT_F32 = 1, VX_FORMAT_I16 = 2 } vx_format;
+ * (texture.rs:324 output_r32float), an int16 integer-disparity map, and
+ * RGBA8Unorm colour images (Context::texture_rgba8, context.rs:54; bytes r, g,
+ * b, a per pixel). */
+typedef enum vx_format { VX_FORMAT_U8 = 0, VX_FORMAT_F32 = 1, VX_FORMAT_I16 = 2, VX_FORMAT_RGBA8 = 3 } vx_format;
 
 /* Replaces Context::texture_gray8 / texture_output_r32float
  * (context.rs:39, context.rs:64): allocates a pitched device image. */
@@ -153,7 +155,11 @@ vx_status vx_sgm_compute(vx_sgm* sgm, vx_ctx* ctx, const vx_image* left, const v
  * reference only has the per-pair call, sgm.rs:108): n independent pairs of
  * any sizes and configs in one pass: one census launch, path aggregation as
  * persistent launches over a (pair, path, scanline-group) work queue, one
- * WTA launch. out_i16 may be NULL or contain NULLs. */
+ * WTA launch. out_i16 may be NULL or contain NULLs. A synchronous call (NULL
+ * stream, graph cache off) keeps each pair's rare escaped path vectors (values
+ * above a byte) in a pool of 1/16 of its vectors instead of a full u16 shadow,
+ * about a third of the workspace, and recomputes any pair whose pool ran out
+ * with a full shadow, so results are the same either way. */
 vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_image* const* left,
                                const vx_image* const* right, vx_image* const* out_f32,
                                vx_image* const* out_i16, const vx_sgm_config* cfgs,
@@ -413,6 +419,68 @@ vx_status vx_stereo_matcher_run_frames_device(vx_stereo_matcher* matcher, vx_ctx
                                               const uint32_t* left_desc_words, const uint32_t* right_desc_words,
                                               const vx_stereo_config* cfg, vx_stereo_match_result* matches,
                                               uint32_t* match_counts, vx_stream stream);
+
+/* ---- The depth chain around SGM: colour ingest and point clouds ----------
+ * Replaces ColorConvert::rgba_to_gray (vx-vision/src/kernels/color.rs:62,
+ * ColorConvert.metal:21-32): in RGBA8, out U8 of the same size; gray =
+ * 0.299 r + 0.587 g + 0.114 b on the unorm values (byte / 255) in single
+ * precision, in that order, stored as an 8-bit unorm (clamp to [0, 1], x 255,
+ * round to nearest even). The gray image feeds vx_sgm_compute_disparity.
+ * NULL stream = the context's stream, synchronous. */
+vx_status vx_color_rgba_to_gray(vx_ctx* ctx, const vx_image* in, vx_image* out, vx_stream stream);
+
+/* DepthToCloudConfig (vx-vision/src/kernels/depth_to_cloud.rs:23-59). Defaults:
+ * min_depth 0.1, max_depth 10, depth_scale 1, max_points 1 000 000. */
+typedef struct vx_depth_to_cloud_config {
+    float min_depth;
+    float max_depth;
+    float depth_scale;
+    uint32_t max_points;
+} vx_depth_to_cloud_config;
+void vx_depth_to_cloud_config_default(vx_depth_to_cloud_config* cfg);
+/* GpuPoint3D (vx-vision/src/types.rs:440-448), 36 bytes: the records the
+ * reference's PointCloud::from_gpu_points reads (types_3d.rs:63-73). */
+typedef struct vx_point3d {
+    float position[3];
+    float _pad0;
+    uint8_t color[4];
+    float normal[3];
+    float _pad1;
+} vx_point3d;
+typedef struct vx_depth_to_cloud vx_depth_to_cloud;
+/* Replaces DepthToCloud::new(&ctx) (depth_to_cloud.rs:66-80). */
+vx_status vx_depth_to_cloud_create(vx_ctx* ctx, vx_depth_to_cloud** out);
+void vx_depth_to_cloud_destroy(vx_depth_to_cloud* dc);
+/* Replaces DepthToCloud::compute_raw (depth_to_cloud.rs:104-188,
+ * DepthToCloud.metal:30-70): every pixel of the F32 depth map with d = depth *
+ * depth_scale inside [min_depth, max_depth] (NaN passes, as in the shader)
+ * becomes the point ((x - cx) d / fx, (y - cy) d / fy, d) (IEEE single
+ * precision, that order), colour (r, g, b, 255) from an RGBA8 color image,
+ * (v, 0, 0, 255) from a U8 one, (255, 255, 255, 255) when color is NULL or at
+ * most 1 pixel wide (the shader's test), normal 0. color must otherwise be the
+ * depth map's size. At most min(max_points, W*H) points, in row-major pixel
+ * order (the reference appends them atomically, in no fixed order); points
+ * must hold that many; *n_points gets their number. Synchronous. */
+vx_status vx_depth_to_cloud_compute_raw(vx_depth_to_cloud* dc, vx_ctx* ctx, const vx_image* depth,
+                                        const vx_image* color, float fx, float fy, float cx, float cy,
+                                        const vx_depth_to_cloud_config* cfg, vx_point3d* points, size_t capacity,
+                                        size_t* n_points);
+/* Replaces DepthToCloud::compute (depth_to_cloud.rs:86-101): compute_raw with
+ * the depth map's intrinsics (for example the DepthMap of vx_sgm_compute with
+ * its depth output). */
+vx_status vx_depth_to_cloud_compute(vx_depth_to_cloud* dc, vx_ctx* ctx, const vx_depth_map* depth,
+                                    const vx_image* color, const vx_depth_to_cloud_config* cfg, vx_point3d* points,
+                                    size_t capacity, size_t* n_points);
+/* The same on device memory (an addition for pipelines that keep the cloud on
+ * the GPU): the first min(max_points, W*H, capacity) points go to d_points,
+ * and *d_count (device) gets the number of pixels that passed (which may exceed
+ * it, like the reference's count buffer). Buffers 4-byte aligned. NULL stream =
+ * the context's stream, synchronous; otherwise asynchronous. Calls on one
+ * handle must be ordered (they share its tile counts). */
+vx_status vx_depth_to_cloud_compute_device(vx_depth_to_cloud* dc, vx_ctx* ctx, const vx_image* depth,
+                                           const vx_image* color, float fx, float fy, float cx, float cy,
+                                           const vx_depth_to_cloud_config* cfg, vx_point3d* d_points,
+                                           uint32_t capacity, uint32_t* d_count, vx_stream stream);
 
 /* Number of this library's kernel launches issued since load (all threads). */
 uint64_t vx_kernel_launch_count(void);

@@ -271,3 +271,71 @@ def ref_stereo_match(left_kpts, right_kpts, left_desc, right_desc, cfg=None) -> 
           c["max_epipolar"], c["min_disparity"], c["max_disparity"], int(c["max_hamming"]) & 0xFFFFFFFF,
           c["ratio_thresh"], c["fx"], c["fy"], c["cx"], c["cy"], c["baseline"], _P(out.ctypes.data))
     return out[:n].copy()
+
+
+# ---------------------------------------------------------------------------
+# Colour ingest and depth unprojection (vx-vision ColorConvert::rgba_to_gray,
+# DepthToCloud): tier 2 (cloud_oracle.cpp) and tier 1 (the shaders compiled
+# as C++, _ref/libcloud_ref.so).
+CLOUD_REF_SO = os.path.join(HERE, "_ref", "libcloud_ref.so")
+_cloud_ref = None
+POINT3D = np.dtype([("position", "<f4", (3,)), ("_pad0", "<f4"), ("color", "u1", (4,)),
+                    ("normal", "<f4", (3,)), ("_pad1", "<f4")])
+CLOUD_DEFAULTS = dict(min_depth=0.1, max_depth=10.0, depth_scale=1.0, max_points=1_000_000)
+
+
+def ref_cloud_available() -> bool:
+    return os.path.exists(CLOUD_REF_SO)
+
+
+def _cloud_ref_lib():
+    global _cloud_ref
+    if _cloud_ref is None:
+        _cloud_ref = ctypes.CDLL(CLOUD_REF_SO)
+        _cloud_ref.ref_depth_to_cloud.restype = ctypes.c_uint
+        _cloud_ref.ref_depth_to_cloud.argtypes = [_P, ctypes.c_uint, ctypes.c_uint, _P, ctypes.c_int] + \
+            [ctypes.c_float] * 7 + [ctypes.c_uint, _P]
+    return _cloud_ref
+
+
+def _color_args(color):
+    if color is None:
+        return None, 0
+    color = np.ascontiguousarray(color, np.uint8)
+    return color, (2 if color.ndim == 3 else 1)
+
+
+def rgba_to_gray(rgba: np.ndarray, ref: bool = False) -> np.ndarray:
+    """(H, W, 4) u8 -> (H, W) u8."""
+    rgba = np.ascontiguousarray(rgba, np.uint8)
+    h, w, _ = rgba.shape
+    out = np.zeros((h, w), np.uint8)
+    fn = _cloud_ref_lib().ref_rgba_to_gray if ref else lib().oracle_rgba_to_gray
+    r = fn(_P(rgba.ctypes.data), _P(out.ctypes.data), w, h)
+    if r != 0:
+        raise ValueError("rgba_to_gray rejected its arguments")
+    return out
+
+
+def depth_to_cloud(depth, color=None, fx=500.0, fy=500.0, cx=0.0, cy=0.0, min_depth=0.1, max_depth=10.0,
+                   depth_scale=1.0, max_points=1_000_000, ref: bool = False):
+    """Returns (points as POINT3D records, number of pixels that passed); colour: None,
+    (H, W) u8 or (H, W, 4) u8. Points in row-major pixel order, min(count, max_points,
+    W*H) of them."""
+    depth = np.ascontiguousarray(depth, np.float32)
+    h, w = depth.shape
+    cap = min(int(max_points), w * h)
+    pts = np.zeros(max(cap, 1), POINT3D)
+    col, fmt = _color_args(color)
+    cp = _P(col.ctypes.data) if col is not None else None
+    if ref:
+        n = _cloud_ref_lib().ref_depth_to_cloud(_P(depth.ctypes.data), w, h, cp, fmt, fx, fy, cx, cy, min_depth,
+                                                max_depth, depth_scale, cap, _P(pts.ctypes.data))
+    else:
+        fn = lib().oracle_depth_to_cloud
+        fn.restype = ctypes.c_long
+        fn.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int] + [ctypes.c_float] * 7 + \
+            [ctypes.c_uint, _P]
+        n = fn(_P(depth.ctypes.data), w, h, cp, fmt, fx, fy, cx, cy, min_depth, max_depth, depth_scale, cap,
+               _P(pts.ctypes.data))
+    return pts[:min(int(n), cap)].copy(), int(n)

@@ -27,10 +27,11 @@ def gpu_ctx():
     ctx.close()
 
 
-@pytest.fixture(params=["single", "pairs"])
+@pytest.fixture(params=["single", "pairs", "scan"])
 def agg_form(request, monkeypatch):
-    """Runs a test through each aggregation form: the single-scanline kernel (the
-    planner's choice for few units) and the scanline-pair kernel (large batches)."""
+    """Runs a test through each aggregation form: the single-scanline kernel, the
+    scanline-pair kernel (large batches) and the across-lanes scan kernel (few
+    units: single pairs, small batches)."""
     monkeypatch.setenv("VX_SGM_AGG_FORM", request.param)
     return request.param
 

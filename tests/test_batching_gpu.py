@@ -70,7 +70,7 @@ def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
     want = run_batch(gpu_ctx, sgm, pairs, cfgs)
     tl, tr, of, oi = _textures(gpu_ctx, pairs)
     w, ms, unit = sgm.autotune_batch(gpu_ctx, tl, tr, of, cfgs, oi, iterations=1)
-    assert w >= 1 and ms > 0 and unit in (32, 64)
+    assert w >= 1 and ms > 0 and unit in (1, 32, 64)
     for f, i, ww in zip(of, oi, want):
         assert_disparity_equal((f.read_r32float(), i.download()), ww, tol=0.0, what="autotune run")
     sgm.compute_batch(gpu_ctx, tl, tr, of, cfgs, outputs_i16=oi)  # uses the tuned shape
@@ -91,7 +91,7 @@ def test_autotune_and_tuning_file(gpu_ctx, tmp_path):
     sgm.close()
 
 
-@pytest.mark.parametrize("form", ["pairs", "single"])
+@pytest.mark.parametrize("form", ["pairs", "single", "scan"])
 def test_stage_times_through_graphs(gpu_ctx, monkeypatch, form):
     """Stage timing of graph-launched batches: every stage's events are recorded;
     the cost-volume stage exists in the scanline-pair form only, and the launch
@@ -113,7 +113,7 @@ def test_stage_times_through_graphs(gpu_ctx, monkeypatch, form):
     census, costs, agg, wta = gpu_ctx.stage_times_detail()
     gpu_ctx.enable_stage_timing(False)
     assert census > 0 and agg > 0 and wta > 0
-    if form == "pairs":
+    if form in ("pairs", "scan"):
         assert costs > 0 and launches == 2 * 4
     else:
         assert costs < 0.01 and launches == 2 * 3
@@ -150,3 +150,34 @@ def test_queue_classes_match_the_oracle(gpu_ctx, monkeypatch, warpgroups):
     for k, ((L, R), o, g) in enumerate(zip(pairs, ocfgs, got)):
         d, di, _ = oracle.sgm(L, R, o)
         assert_disparity_equal(g, (d, di), what=f"pair {k} D={o.num_disparities} with {warpgroups} warpgroups")
+
+
+@pytest.mark.parametrize("pool", [None, "1"])
+def test_synchronous_batch_escape_pools(gpu_ctx, monkeypatch, pool):
+    """Synchronous batch calls keep escaped path vectors in a pool of 1/16 of each pair's
+    vectors; with a pool of one vector (VX_SGM_SHADOW_POOL=1) every pair with two or
+    more escapes overflows and is recomputed with a full shadow. Both equal the oracle,
+    for every aggregation form."""
+    import oracle
+    from gpu_helpers import cfg_pair
+    if pool:
+        monkeypatch.setenv("VX_SGM_SHADOW_POOL", pool)
+    rng = np.random.default_rng(5)
+    pairs, cfgs, ocfgs = [], [], []
+    for i in range(6):
+        w, h = int(rng.choice([120, 203])), int(rng.choice([70, 101]))
+        nd = [64, 128, 96][i % 3]
+        L, R, _ = vx_sgm.synth_pair(2, w, h, 0, nd - 6, 900 + i)
+        c, o = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2, num_paths=8, lr_check=True,
+                        p1=float(rng.choice([2, 10])), p2=float(rng.choice([60, 120])))
+        pairs.append((L, R))
+        cfgs.append(c)
+        ocfgs.append(o)
+    for form in ("pairs", "single", "scan"):
+        monkeypatch.setenv("VX_SGM_AGG_FORM", form)
+        sgm = vx_sgm.SGMStereo(gpu_ctx)
+        got = run_batch(gpu_ctx, sgm, pairs, cfgs)
+        sgm.close()
+        for k, ((L, R), o, g) in enumerate(zip(pairs, ocfgs, got)):
+            d, di, _ = oracle.sgm(L, R, o)
+            assert_disparity_equal(g, (d, di), what=f"{form} pool={pool} pair {k}")

@@ -796,15 +796,19 @@ cudaError_t prepare_aggregate_kernels() {
 }
 
 int aggregate_max_warpgroups(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles) {
+    if (unit_scanlines == kScanForm) return 1;   // no warpgroup shape: warps per SM by occupancy
     return unit_scanlines == kUnitScanlines ? pairs::max_warpgroups(dp_max, dp_min, wide_tiles)
                                             : single::max_warpgroups(dp_max, census64);
 }
 
-cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, const AggLaunch& L,
+cudaError_t launch_aggregate(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles, const AggLaunch& L,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
                              int num_units, unsigned* counters, cudaStream_t stream, bool compact) {
     if (unit_scanlines == kUnitScanlines)
         return pairs::launch(dp_max, wide_tiles, L, d_pairs, d_jobs, d_units, num_units, counters, stream, compact);
+    if (unit_scanlines == kScanForm)
+        return scan::launch((dp_min <= 128 ? 1 : 0) | (dp_max > 128 ? 2 : 0), d_pairs, d_jobs, d_units, num_units,
+                            counters, stream, compact);
     return single::launch(dp_max, census64, L.warpgroups, d_pairs, d_jobs, d_units, num_units, counters, stream,
                           compact);
 }

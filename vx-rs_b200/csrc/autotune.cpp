@@ -77,11 +77,16 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
     int best_w = 0, best_unit = 0;
     float best = 0.0f;
     TuneKey key{};
-    // Both aggregation forms (32-scanline units on the single-scanline kernel,
-    // 64-scanline units on the scanline-pair kernel), every launch shape each.
-    for (int unit : {32, kUnitScanlines}) {
-        if (const char* f = std::getenv("VX_SGM_AGG_FORM"))
-            if ((unit == 32) != (std::strcmp(f, "single") == 0)) continue;
+    // Every aggregation form (32-scanline units on the single-scanline kernel,
+    // 64-scanline units on the scanline-pair kernel, the across-lanes scan
+    // kernel), every launch shape of each.
+    for (int unit : {32, kUnitScanlines, kScanForm}) {
+        if (const char* f = std::getenv("VX_SGM_AGG_FORM")) {
+            const int forced = std::strcmp(f, "single") == 0 ? 32
+                             : std::strcmp(f, "pairs") == 0 ? kUnitScanlines
+                             : std::strcmp(f, "scan") == 0 ? kScanForm : unit;
+            if (unit != forced) continue;
+        }
         Plan plan;
         st = build_plan(specs, &plan, unit);
         if (st != VX_OK) break;
@@ -186,7 +191,7 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
             field(pos, end, "unit_scanlines", &us);
             double dmin = dp;   // files without dp_min: batches of one D
             field(pos, end, "dp_min", &dmin);
-            if (wg >= 1 && dp >= 8 && dmin >= 8 && dmin <= dp && (us == 32 || us == kUnitScanlines)) {
+            if (wg >= 1 && dp >= 8 && dmin >= 8 && dmin <= dp && (us == 32 || us == kUnitScanlines || us == kScanForm)) {
                 sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide, (int)dmin}] = {(int)us, (int)wg, (float)ms};
                 ++loaded;
             }

@@ -37,6 +37,7 @@ size_t format_bytes(vx_format f) {
         case VX_FORMAT_U8: return 1;
         case VX_FORMAT_F32: return 4;
         case VX_FORMAT_I16: return 2;
+        case VX_FORMAT_RGBA8: return 4;
     }
     return 0;
 }

@@ -144,7 +144,7 @@ vx_status run_batch_graph(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>&
             cudaGraphExecEventRecordNodeSetEvent(entry->exec, entry->ev_nodes[i],
                                                  slot ? slot[i] : entry->baked[i]);
     // census, the cost volume (scanline-pair form), aggregation, WTA
-    count_launch(entry->plan.unit_scanlines == kUnitScanlines ? 4 : 3);
+    count_launch(entry->plan.unit_scanlines != 32 ? 4 : 3);   // the cost volume in the pair and scan forms
     err = cudaGraphLaunch(entry->exec, stream);
     if (err != cudaSuccess) return cuda_fail(err, "launching the batch graph");
     if (synchronous) {

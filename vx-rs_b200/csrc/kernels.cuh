@@ -105,6 +105,23 @@ constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
 // Scanlines per aggregation work unit of the scanline-pair kernel (one warp:
 // two scanlines per lane); the single-scanline kernel takes 32.
 constexpr int kUnitScanlines = 64;
+// The across-lanes scan form (aggregate_scan.cu): plans select it with this
+// value in place of a unit size; its units hold a pair-dependent number of
+// scanlines (ScanGeometry::scanlines).
+constexpr int kScanForm = 1;
+// Geometry of the scan form for a pair with Dv bytes a vector: K disparities a
+// lane, `lanes` lanes a scanline in a segment of `seg` lanes (a power of two),
+// `scanlines` = 32 / seg scanlines a warp.
+struct ScanGeometry {
+    int k, lanes, seg, scanlines;
+};
+__host__ __device__ constexpr ScanGeometry scan_geometry(int nd_vec) {
+    const int k = nd_vec > 128 ? 16 : 8;
+    const int lanes = nd_vec / k;
+    int seg = 1;
+    while (seg < lanes) seg <<= 1;
+    return ScanGeometry{k, lanes, seg, 32 / seg};
+}
 // Fewest 64-scanline units for which a batch whose key was not autotuned runs
 // the scanline-pair kernel (on B200 the forms cross over between 6 000 and
 // 8 000 units; the autotuner times both).

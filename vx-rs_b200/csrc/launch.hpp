@@ -46,7 +46,7 @@ struct AggLaunch {
 };
 cudaError_t prepare_aggregate_kernels();  // shared-memory limits of both; once per device
 int aggregate_max_warpgroups(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles);
-cudaError_t launch_aggregate(int unit_scanlines, int dp_max, bool census64, bool wide_tiles, const AggLaunch& L,
+cudaError_t launch_aggregate(int unit_scanlines, int dp_max, int dp_min, bool census64, bool wide_tiles, const AggLaunch& L,
                              const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
                              int num_units, unsigned* counters, cudaStream_t stream, bool compact = false);
 namespace pairs {
@@ -58,6 +58,12 @@ cudaError_t launch(int dp_max, bool wide_tiles, const AggLaunch& L, const PairDe
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counters,
                    cudaStream_t stream, bool compact = false);
 }  // namespace pairs
+namespace scan {
+// lane_widths: bit 0 = the batch has pairs of Dv <= 128 (8 disparities a lane),
+// bit 1 = pairs of Dv > 128 (16 a lane).
+cudaError_t launch(int lane_widths, const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
+                   int num_units, unsigned* counter, cudaStream_t stream, bool compact = false);
+}  // namespace scan
 namespace single {
 cudaError_t prepare();
 int max_warpgroups(int dp_max, bool census64);
@@ -83,6 +89,17 @@ cudaError_t launch_depth_median(const float* in, size_t in_pitch, float* out, si
                                 int radius, cudaStream_t stream);
 cudaError_t launch_depth_bilateral(const float* in, size_t in_pitch, float* out, size_t out_pitch, int W, int H,
                                    int radius, float sigma_s, float sigma_d, cudaStream_t stream);
+
+// The depth chain's ends (cloud.cu): RGBA8 -> U8 gray, and the unprojection of
+// an F32 depth map to 36-byte GpuPoint3D records (tile_counts: one word per
+// depth_to_cloud_tiles() tile; count: the number of pixels that passed).
+cudaError_t launch_rgba_to_gray(const uint8_t* in, size_t in_pitch, uint8_t* out, size_t out_pitch, int W, int H,
+                                cudaStream_t stream);
+int depth_to_cloud_tiles(int W, int H);
+cudaError_t launch_depth_to_cloud(const float* depth, size_t depth_pitch, const uint8_t* color, size_t color_pitch,
+                                  bool color_rgba, int W, int H, float fx, float fy, float cx, float cy,
+                                  float min_depth, float max_depth, float depth_scale, uint32_t max_points,
+                                  uint32_t* tile_counts, float* points, uint32_t* count, cudaStream_t stream);
 
 // Sparse ORB stereo matching (stereo_match.cu). Keypoints are CornerPoint
 // records read as float4 (x, y, response, level bits); descriptors are 8 words

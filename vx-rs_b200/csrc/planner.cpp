@@ -69,7 +69,9 @@ size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg
 
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
     const size_t P = cfg.num_paths;
-    const size_t units = P * (((size_t)width + height - 1 + 31) / 32);     // 32-scanline units at most
+    // Units of the scan form hold the fewest scanlines (ScanGeometry::scanlines >= 2).
+    const size_t per_unit = (size_t)scan_geometry((cfg.num_disparities + 15) / 16 * 16).scanlines;
+    const size_t units = P * (((size_t)width + height - 1 + per_unit - 1) / per_unit);
     return sizeof(PairDev) + P * sizeof(JobDev) + units * sizeof(UnitDev) + sizeof(unsigned) +
            4 * kAlign;
 }
@@ -139,6 +141,13 @@ vx_status plan_queues(Plan& pl, int warpgroups, CostFn unit_cost) {
     AggQueues& q = L.queues;
     const int nu = (int)pl.units.size();
     auto unit_dp = [&](const UnitDev& u) { return pl.pairs[pl.jobs[u.job].pair].nd_pad; };
+    if (pl.unit_scanlines == kScanForm) {      // one queue, warps per SM by occupancy
+        L.warpgroups = 1;
+        q.n_classes = 1;
+        q.begin[1] = nu;
+        for (int c = 2; c <= kMaxQueueClasses; ++c) q.begin[c] = nu;
+        return VX_OK;
+    }
     if (pl.unit_scanlines != kUnitScanlines) {
         const int wmax = single::max_warpgroups(pl.dp_max, pl.census64);
         L.warpgroups = warpgroups > 0 ? std::min(warpgroups, wmax)
@@ -317,22 +326,27 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
         units64 += (j.num_scanlines + kUnitScanlines - 1) / kUnitScanlines;
         pl.units32 += (j.num_scanlines + 31) / 32;
     }
-    if (unit_scanlines == kUnitScanlines || unit_scanlines == 32)
+    if (unit_scanlines == kUnitScanlines || unit_scanlines == 32 || unit_scanlines == kScanForm)
         pl.unit_scanlines = unit_scanlines;        // the autotuned form
     else
         pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines : 32;
-    // VX_SGM_AGG_FORM=pairs|single forces one form (both are exact; the tests run
-    // every case through each).
+    // VX_SGM_AGG_FORM=pairs|single|scan forces one form (all are exact; the tests
+    // run every case through each).
     if (const char* f = std::getenv("VX_SGM_AGG_FORM")) {
         if (std::strcmp(f, "pairs") == 0) pl.unit_scanlines = kUnitScanlines;
         if (std::strcmp(f, "single") == 0) pl.unit_scanlines = 32;
+        if (std::strcmp(f, "scan") == 0) pl.unit_scanlines = kScanForm;
     }
-    for (int job = 0; job < (int)pl.jobs.size(); ++job)
-        for (int k = 0; k < pl.jobs[job].num_scanlines; k += pl.unit_scanlines) units.push_back({job, k});
-    // The scanline-pair kernel reads the matching costs from a per-pair byte
-    // volume (cost.cu), laid out after every pair's census, slab and shadow
+    for (int job = 0; job < (int)pl.jobs.size(); ++job) {
+        const int per_unit = pl.unit_scanlines == kScanForm
+                                 ? scan_geometry(pl.pairs[pl.jobs[job].pair].nd_vec).scanlines
+                                 : pl.unit_scanlines;
+        for (int k = 0; k < pl.jobs[job].num_scanlines; k += per_unit) units.push_back({job, k});
+    }
+    // The scanline-pair and scan kernels read the matching costs from a per-pair
+    // byte volume (cost.cu), laid out after every pair's census, slab and shadow
     // region; the single-scanline kernel forms them from the census words.
-    if (pl.unit_scanlines == kUnitScanlines)
+    if (pl.unit_scanlines != 32)
         for (int i = 0; i < n; ++i) {
             PairDev& pd = pl.pairs[i];
             pd.costs = reinterpret_cast<uint8_t*>(data);
@@ -350,7 +364,9 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
         else {  // longest of the unit's diagonals
             len = 0;
             const int k0 = j.k_min + u.first_scanline;
-            const int k1 = j.k_min + std::min(u.first_scanline + pl.unit_scanlines, j.num_scanlines);
+            const int per_unit = pl.unit_scanlines == kScanForm ? scan_geometry(p.nd_vec).scanlines
+                                                                 : pl.unit_scanlines;
+            const int k1 = j.k_min + std::min(u.first_scanline + per_unit, j.num_scanlines);
             for (int k = k0; k < k1; ++k) {
                 int tb, te;
                 if (j.dx > 0) { tb = std::max(0, -k); te = std::min(p.height, p.width - k); }
@@ -401,7 +417,7 @@ void bind_plan(Plan& pl, char* base) {
         pd.census_lt = data + reinterpret_cast<size_t>(pd.census_lt);
         pd.census_rt = data + reinterpret_cast<size_t>(pd.census_rt);
         pd.slabs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.slabs));
-        if (pl.unit_scanlines == kUnitScanlines)
+        if (pl.unit_scanlines != 32)
             pd.costs = reinterpret_cast<uint8_t*>(data + reinterpret_cast<size_t>(pd.costs));
         pd.shadow = reinterpret_cast<uint16_t*>(data + reinterpret_cast<size_t>(pd.shadow));
         pd.esc_state = reinterpret_cast<uint32_t*>(base + reinterpret_cast<size_t>(pd.esc_state));
@@ -442,15 +458,15 @@ vx_status launch_plan(const Plan& pl, char* base, cudaStream_t stream, cudaEvent
 
     if (ev) record(ev[0]);
     e = launch_census(d_pairs, n, pl.total_tiles, pl.max_rx, pl.max_ry, pl.census64,
-                      pl.unit_scanlines != kUnitScanlines, stream);
+                      pl.unit_scanlines == 32, stream);
     if (e != cudaSuccess) return cuda_fail(e, "census launch");
     if (ev) record(ev[1]);
-    if (pl.unit_scanlines == kUnitScanlines) {
+    if (pl.unit_scanlines != 32) {
         e = launch_costs(d_pairs, n, pl.total_rows, pl.dp_max, pl.census64, stream);
         if (e != cudaSuccess) return cuda_fail(e, "cost volume launch");
     }
     if (ev) record(ev[2]);
-    e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.census64, pl.wide_tiles, pl.agg, d_pairs, d_jobs, d_units,
+    e = launch_aggregate(pl.unit_scanlines, pl.dp_max, pl.dp_min, pl.census64, pl.wide_tiles, pl.agg, d_pairs, d_jobs, d_units,
                          (int)pl.units.size(), counters, stream, pl.compact);
     if (e != cudaSuccess) return cuda_fail(e, "aggregation launch");
     if (ev) record(ev[3]);

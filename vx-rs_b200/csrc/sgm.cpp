@@ -68,6 +68,65 @@ vx_status run_batch(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs
     return st;
 }
 
+// A synchronous batch whose byte-slab pairs keep their escaped path vectors in
+// a pool of 1/16 of their vectors instead of a full u16 shadow (about a third
+// of the workspace), so that fewer, larger sub-batches fit the workspace limit.
+// After each sub-batch the pairs' overflow flags come back; a pair whose pool
+// ran out (more than 1/16 of its path vectors held a value above a byte) is
+// recomputed with a full shadow at the end, so results never depend on the pool.
+vx_status run_batch_pooled(vx_sgm* sgm, vx_ctx* ctx, const std::vector<PairSpec>& specs, cudaStream_t stream) {
+    std::vector<PairSpec> pooled(specs);
+    for (auto& s : pooled) s.compact_shadow = true;
+    for (const auto& s : pooled) {
+        const vx_status st = validate_pair(s);
+        if (st != VX_OK) return st;
+    }
+    DeviceGuard g(ctx->device);
+    std::vector<PairSpec> rerun;
+    size_t i0 = 0;
+    while (i0 < pooled.size()) {
+        // The longest run of pairs from i0 whose pooled workspaces fit the limit (at least one).
+        size_t i1 = i0, bytes = 0;
+        while (i1 < pooled.size()) {
+            const PairSpec& s = pooled[i1];
+            const size_t ct = census_bits(s.cfg) > 32 ? 8 : 4;
+            const size_t b = pair_workspace_bytes(s.left->width, s.left->height, s.cfg, ct, true) +
+                             pair_cost_bytes(s.left->width, s.left->height, s.cfg) + (64 << 10);
+            if (i1 > i0 && bytes + b > ctx->workspace_limit) break;
+            bytes += b;
+            ++i1;
+        }
+        const std::vector<PairSpec> chunk(pooled.begin() + i0, pooled.begin() + i1);
+        Plan plan;
+        vx_status st = sgm->plan_batch(chunk, &plan);
+        if (st != VX_OK) return st;
+        char* ws = nullptr;
+        count_alloc();
+        cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), plan.ws_bytes, ctx->pool, stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(VX_ERR_BUFFER_ALLOC, "buffer allocation failed (%zu bytes)", plan.ws_bytes);
+        }
+        bind_plan(plan, ws);
+        st = run_plan(plan, ws, stream, ctx->next_timing_slot());
+        std::vector<uint32_t> esc(2 * chunk.size(), 0u);
+        if (st == VX_OK) {
+            e = cudaMemcpyAsync(esc.data(), ws + plan.off_escape(), esc.size() * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) st = cuda_fail(e, "SGM execution");
+        }
+        cudaFreeAsync(ws, stream);
+        if (st != VX_OK) return st;
+        for (size_t k = 0; k < chunk.size(); ++k)
+            if (esc[2 * k + 1] != 0u) rerun.push_back(specs[i0 + k]);   // the pair as given: full shadow
+        i0 = i1;
+    }
+    if (!rerun.empty()) return run_batch(sgm, ctx, rerun, stream, true, nullptr, nullptr);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? VX_OK : cuda_fail(e, "SGM execution");
+}
+
 }  // namespace
 
 namespace vxsgm {
@@ -180,7 +239,8 @@ vx_status vx_sgm_compute_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_im
             if (p.left) total += vx_sgm_workspace_bytes(p.left->width, p.left->height, &p.cfg);
         if (total <= ctx->workspace_limit) return run_batch_graph(sgm, ctx, specs, s, stream == nullptr);
     }
-    return run_batch(sgm, ctx, specs, s, stream == nullptr, nullptr, nullptr);
+    if (!stream) return run_batch_pooled(sgm, ctx, specs, s);   // synchronous: escape pools, exact re-runs
+    return run_batch(sgm, ctx, specs, s, false, nullptr, nullptr);
 }
 
 size_t vx_sgm_workspace_bytes(uint32_t width, uint32_t height, const vx_sgm_config* cfg) {

@@ -38,8 +38,12 @@ STATUS_NAMES = {
     6: "VX_ERR_INVALID_CONFIG", 7: "VX_ERR_GPU", 8: "VX_ERR_BUDGET", 9: "VX_ERR_TIMEOUT",
     10: "VX_ERR_INVALID_ARGUMENT", 11: "VX_ERR_NOT_READY", 12: "VX_ERR_CANCELLED",
 }
-FORMAT_U8, FORMAT_F32, FORMAT_I16 = 0, 1, 2
-_FORMAT_DTYPE = {FORMAT_U8: np.uint8, FORMAT_F32: np.float32, FORMAT_I16: np.int16}
+FORMAT_U8, FORMAT_F32, FORMAT_I16, FORMAT_RGBA8 = 0, 1, 2, 3
+_FORMAT_DTYPE = {FORMAT_U8: np.uint8, FORMAT_F32: np.float32, FORMAT_I16: np.int16, FORMAT_RGBA8: np.uint8}
+
+
+def _host_shape(fmt, width, height):
+    return (height, width, 4) if fmt == FORMAT_RGBA8 else (height, width)
 
 
 class VxError(RuntimeError):
@@ -254,6 +258,18 @@ class Context:
     def texture_output_r32float(self, width: int, height: int) -> "Texture":
         return Texture.create(self, width, height, FORMAT_F32)
 
+    def texture_rgba8(self, pixels, width: int, height: int) -> "Texture":
+        """Context::texture_rgba8 (context.rs:54): an RGBA8 image from (H, W, 4) bytes."""
+        t = Texture.create(self, width, height, FORMAT_RGBA8)
+        t.upload(np.asarray(pixels, dtype=np.uint8).reshape(height, width, 4))
+        return t
+
+    def texture_output_rgba8(self, width: int, height: int) -> "Texture":
+        return Texture.create(self, width, height, FORMAT_RGBA8)
+
+    def texture_output_gray8(self, width: int, height: int) -> "Texture":
+        return Texture.create(self, width, height, FORMAT_U8)
+
     def texture_r32float(self, data, width: int, height: int) -> "Texture":
         """Context::texture_r32float (an F32 image from host data)."""
         t = Texture.create(self, width, height, FORMAT_F32)
@@ -297,12 +313,12 @@ class Texture:
 
     def upload(self, host: np.ndarray, stream: int | None = None):
         a = np.ascontiguousarray(host, dtype=_FORMAT_DTYPE[self.format])
-        assert a.shape == (self.height, self.width), (a.shape, self.height, self.width)
+        assert a.shape == _host_shape(self.format, self.width, self.height), (a.shape, self.height, self.width)
         _check(_img_upload(self._h, _P(a.ctypes.data), a.strides[0], _P(stream) if stream else None))
 
     def download(self, host: np.ndarray | None = None, stream: int | None = None) -> np.ndarray:
         if host is None:
-            host = np.empty((self.height, self.width), dtype=_FORMAT_DTYPE[self.format])
+            host = np.empty(_host_shape(self.format, self.width, self.height), dtype=_FORMAT_DTYPE[self.format])
         _check(_img_download(self._h, _P(host.ctypes.data), host.strides[0],
                              _P(stream) if stream else None))
         return host
@@ -375,10 +391,10 @@ class SGMStereo:
 
     def autotune_batch(self, ctx: Context, lefts, rights, outputs, configs, outputs_i16=None,
                        iterations: int = 2):
-        """Times both aggregation forms and every launch shape on this batch and keeps
-        the fastest for batches like it. Returns (warpgroups, aggregate_ms,
+        """Times every aggregation form and launch shape on this batch and keeps the
+        fastest for batches like it. Returns (warpgroups, aggregate_ms,
         unit_scanlines) of the winner (unit_scanlines 32: single-scanline kernel,
-        64: scanline-pair kernel)."""
+        64: scanline-pair kernel, 1: across-lanes scan kernel)."""
         n = len(lefts)
         arr = lambda ts: (_P * n)(*[t.handle if t is not None else None for t in ts])
         cfgs = (_CConfig * n)(*[c.to_c() for c in configs])
@@ -486,6 +502,118 @@ class DepthFilter:
     def close(self):
         if self._h:
             _df_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# The depth chain's ends: colour ingest (vx-vision/src/kernels/color.rs) and
+# point clouds (vx-vision/src/kernels/depth_to_cloud.rs)
+
+# GpuPoint3D (vx-vision/src/types.rs:440-448), 36 bytes.
+POINT3D = np.dtype([("position", "<f4", (3,)), ("_pad0", "<f4"), ("color", "u1", (4,)),
+                    ("normal", "<f4", (3,)), ("_pad1", "<f4")])
+assert POINT3D.itemsize == 36
+
+
+class _CDepthToCloudConfig(ctypes.Structure):
+    _fields_ = [("min_depth", ctypes.c_float), ("max_depth", ctypes.c_float), ("depth_scale", ctypes.c_float),
+                ("max_points", ctypes.c_uint32)]
+
+
+_color_gray = _sig("vx_color_rgba_to_gray", ctypes.c_int, _P, _P, _P, _P)
+_d2c_create = _sig("vx_depth_to_cloud_create", ctypes.c_int, _P, ctypes.POINTER(_P))
+_d2c_destroy = _sig("vx_depth_to_cloud_destroy", None, _P)
+_d2c_raw = _sig("vx_depth_to_cloud_compute_raw", ctypes.c_int, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                ctypes.c_float, ctypes.c_float, ctypes.POINTER(_CDepthToCloudConfig), _P, ctypes.c_size_t,
+                ctypes.POINTER(ctypes.c_size_t))
+_d2c_device = _sig("vx_depth_to_cloud_compute_device", ctypes.c_int, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                   ctypes.c_float, ctypes.c_float, ctypes.POINTER(_CDepthToCloudConfig), _P, ctypes.c_uint32, _P, _P)
+
+
+class ColorConvert:
+    """ColorConvert (color.rs:20-80): here its rgba_to_gray, the ingest of colour pairs."""
+
+    def __init__(self, ctx: Context):
+        self._ctx = ctx
+
+    @classmethod
+    def new(cls, ctx: Context) -> "ColorConvert":
+        return cls(ctx)
+
+    def rgba_to_gray(self, ctx: Context, input: Texture, output: Texture, stream=None):
+        _check(_color_gray(ctx.handle, input.handle, output.handle, _P(stream) if stream else None))
+
+
+@dataclass
+class DepthToCloudConfig:
+    """DepthToCloudConfig (depth_to_cloud.rs:23-59)."""
+    min_depth: float = 0.1
+    max_depth: float = 10.0
+    depth_scale: float = 1.0
+    max_points: int = 1_000_000
+
+    @classmethod
+    def new(cls, min_depth: float, max_depth: float) -> "DepthToCloudConfig":
+        return cls(min_depth=min_depth, max_depth=max_depth)
+
+    def to_c(self) -> _CDepthToCloudConfig:
+        return _CDepthToCloudConfig(self.min_depth, self.max_depth, self.depth_scale, self.max_points)
+
+
+@dataclass
+class PointCloud:
+    """PointCloud (types_3d.rs:50-90): the points as POINT3D records."""
+    points: np.ndarray
+
+    def __len__(self):
+        return len(self.points)
+
+
+class DepthToCloud:
+    """DepthToCloud (depth_to_cloud.rs:62-188): depth map -> point cloud."""
+
+    def __init__(self, ctx: Context):
+        h = _P()
+        _check(_d2c_create(ctx.handle, ctypes.byref(h)))
+        self._h, self._ctx = h, ctx
+
+    @classmethod
+    def new(cls, ctx: Context) -> "DepthToCloud":
+        return cls(ctx)
+
+    def compute_raw(self, ctx: Context, depth: Texture, color: Texture | None, fx: float, fy: float, cx: float,
+                    cy: float, config: DepthToCloudConfig | None = None) -> PointCloud:
+        cfg = config or DepthToCloudConfig()
+        cap = min(int(cfg.max_points), depth.width * depth.height)
+        out = np.zeros(cap, POINT3D)
+        n = ctypes.c_size_t()
+        c = cfg.to_c()
+        _check(_d2c_raw(self._h, ctx.handle, depth.handle, color.handle if color is not None else None, fx, fy, cx,
+                        cy, ctypes.byref(c), _P(out.ctypes.data) if cap else None, cap, ctypes.byref(n)))
+        return PointCloud(out[:n.value].copy())
+
+    def compute(self, ctx: Context, depth: "DepthMap", color: Texture | None = None,
+                config: DepthToCloudConfig | None = None) -> PointCloud:
+        k = depth.intrinsics
+        return self.compute_raw(ctx, depth.texture, color, k.fx, k.fy, k.cx, k.cy, config)
+
+    def compute_device(self, ctx: Context, depth: Texture, color: Texture | None, fx: float, fy: float, cx: float,
+                       cy: float, config: DepthToCloudConfig, points_ptr: int, capacity: int, count_ptr: int,
+                       stream=None):
+        c = config.to_c()
+        _check(_d2c_device(self._h, ctx.handle, depth.handle, color.handle if color is not None else None, fx, fy,
+                           cx, cy, ctypes.byref(c), _P(points_ptr), capacity, _P(count_ptr),
+                           _P(stream) if stream else None))
+
+    def close(self):
+        if self._h:
+            _d2c_destroy(self._h)
             self._h = None
 
     def __del__(self):
