@@ -8,7 +8,7 @@ f_d(x) = min(a_d, x + b_d) serially, the segment scans the lanes' compositions
 (Kogge-Stone over a power-of-two segment), each lane applies the incoming value;
 a pixel whose ushort arithmetic could leave [0, 65535] is recomputed in the
 shader's serial order. This replay follows the same steps with numpy on the same
-lane geometry (K = 8 for Dv <= 128, else 16) and must reproduce the oracle's
+lane geometry (K = 8 disparities a lane) and must reproduce the oracle's
 per-path costs L_r bit for bit (vx-vision/shaders/SGMStereo.metal:120-172),
 including a scene and penalties under which the shader's ushort values wrap."""
 import numpy as np
@@ -21,7 +21,7 @@ INF = 1 << 30
 
 
 def _geometry(dv):
-    k = 16 if dv > 128 else 8
+    k = 8
     lanes = dv // k
     seg = 1
     while seg < lanes:
@@ -174,4 +174,4 @@ def test_geometry_covers_every_disparity_count():
         dv = (D + 15) // 16 * 16
         k, lanes, seg = _geometry(dv)
         assert lanes * k == dv and lanes <= seg <= 32 and 32 % seg == 0
-        assert (seg & (seg - 1)) == 0 and 32 // seg >= 2      # at least two scanlines a warp
+        assert (seg & (seg - 1)) == 0 and 32 // seg >= 1

@@ -807,8 +807,7 @@ cudaError_t launch_aggregate(int unit_scanlines, int dp_max, int dp_min, bool ce
     if (unit_scanlines == kUnitScanlines)
         return pairs::launch(dp_max, wide_tiles, L, d_pairs, d_jobs, d_units, num_units, counters, stream, compact);
     if (unit_scanlines == kScanForm)
-        return scan::launch((dp_min <= 128 ? 1 : 0) | (dp_max > 128 ? 2 : 0), d_pairs, d_jobs, d_units, num_units,
-                            counters, stream, compact);
+        return scan::launch(d_pairs, d_jobs, d_units, num_units, counters, stream, compact);
     return single::launch(dp_max, census64, L.warpgroups, d_pairs, d_jobs, d_units, num_units, counters, stream,
                           compact);
 }

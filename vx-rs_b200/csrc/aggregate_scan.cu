@@ -36,7 +36,8 @@
 // the previous lane's last value broadcast to it.
 //
 // Data. Costs come from the pair's byte cost volume (cost.cu; Dv bytes a
-// pixel, 64 where x - d < 0), K bytes a lane, loaded two pixel steps ahead.
+// pixel, 64 where x - d < 0), K = 8 bytes a lane (a scanline takes Dv / 8
+// lanes: a segment of 2..32), loaded two pixel steps ahead.
 // The state of a scanline stays in registers (K values a lane). Results go to
 // the same path slabs as the other forms: a byte vector (K bytes a lane, one
 // coalesced store a segment) or, for a vector with a value of 255 or more, the
@@ -64,17 +65,10 @@ constexpr int kThreads = 256;
 
 template <int K>
 __device__ __forceinline__ void load_costs(const uint8_t* p, bool on, uint32_t (&w)[K / 4]) {
-    if constexpr (K == 8) {
-        const uint2 v = on ? __ldg(reinterpret_cast<const uint2*>(p)) : make_uint2(0u, 0u);
-        w[0] = v.x;
-        w[1] = v.y;
-    } else {
-        const uint4 v = on ? __ldg(reinterpret_cast<const uint4*>(p)) : make_uint4(0u, 0u, 0u, 0u);
-        w[0] = v.x;
-        w[1] = v.y;
-        w[2] = v.z;
-        w[3] = v.w;
-    }
+    static_assert(K == 8, "eight disparities a lane");
+    const uint2 v = on ? __ldg(reinterpret_cast<const uint2*>(p)) : make_uint2(0u, 0u);
+    w[0] = v.x;
+    w[1] = v.y;
 }
 
 // Cost of disparity j of the lane (byte j of its words).
@@ -103,10 +97,14 @@ __device__ __forceinline__ uint32_t pack2(int a, int b) { return __byte_perm((ui
 
 // One unit: the warp's 32 / seg scanlines first.. of one (pair, path), each on
 // one segment of seg lanes; lane li of a segment holds disparities
-// d0 = li*K .. d0+K-1 (lanes li >= ls hold only pads). All lanes run every
+// d0 = li*K .. d0+K-1 (lanes li >= lanes hold only pads). All lanes run every
 // step (the shuffles are warp-collective); a segment outside its scanline's
 // steps computes values it never stores.
-template <int K, bool CP>
+// NP (no pads): D is a multiple of 16 (D = Dv), so every disparity of a lane
+// li < lanes is real, d = D-1 is the last one of lane lanes-1 (its o2 = 0xFFFF
+// comes from a next-lane value of 0xFFFF - P1) and only the lanes past `lanes`
+// need masking, once per step. Otherwise each disparity is tested.
+template <int K, bool CP, bool NP>
 __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, int first, const ScanGeometry g,
                                          int lane) {
     const int W = pr.width, H = pr.height, D = pr.nd, Dv = pr.nd_vec, Dp = pr.nd_pad;
@@ -116,6 +114,7 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
     const int sl = lane / seg, li = lane % seg;
     const int d0 = li * K;
     const bool lane_on = li < g.lanes;
+    const bool last_lane = li == g.lanes - 1;
     const int k = first + sl;
     const int dx = job.dx, dy = job.dy;
 
@@ -146,6 +145,8 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
     uint8_t* slab = pr.slabs + pr.slab_stride * (size_t)job.path;
     uint16_t* shadow_path = pr.shadow + pr.shadow_stride * (size_t)job.path;
     const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
+    // A disparity of this lane takes part (NP: every one of an active lane).
+    auto real = [&](int j) { return NP ? true : d0 + j < D; };
 
     int L[K];                 // the scanline's state (previous pixel), disparities d0..d0+K-1
     int m = 0, pmx = 0;       // previous pixel's minimum and maximum
@@ -158,27 +159,30 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
     for (int t = t_lo; t < t_hi; ++t) {
         const bool active = on_step(t);
         load_costs<K>(cost_row(t + 2), on_step(t + 2) && lane_on, c2);   // two steps ahead
-        if (t == tb) {        // the scanline starts: Lp = 0, m = 0 give L = C (the shader's step 0)
+        if (__any_sync(kFull, t == tb)) {   // a scanline starts: Lp = 0, m = 0 give L = C (the shader's step 0)
+            if (t == tb) {
 #pragma unroll
-            for (int j = 0; j < K; ++j) L[j] = 0;
-            m = 0;
-            pmx = 0;
+                for (int j = 0; j < K; ++j) L[j] = 0;
+                m = 0;
+                pmx = 0;
+            }
         }
-        const int Lnext = __shfl_down_sync(kFull, L[0], 1, seg);   // the next lane's Lp[d0 + K]
+        int Lnext = __shfl_down_sync(kFull, L[0], 1, seg);   // the next lane's Lp[d0 + K]
+        if (NP && last_lane) Lnext = 0xFFFF - P1;             // o2 of d = D-1 is 0xFFFF
         const int o3 = m + P2;
+        const int p1m = P1 - m;
 
         // a_d (then y_d in place) and the lane's composition (AL, BL).
         int y[K];
         int AL = kInf, BL = 0;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            const int d = d0 + j;
+            const int c = cost_at<K>(c0, j);
             const int nb = j + 1 < K ? L[j + 1] : Lnext;
-            const int o2 = d == D - 1 ? 0xFFFF : nb + P1;
-            const int cm = cost_at<K>(c0, j) - m;
-            const bool real = d < D;
-            y[j] = real ? cm + __vimin3_s32(L[j], o2, o3) : kInf;
-            const int b = real ? cm + P1 : 0;
+            int o2 = nb + P1;
+            if (!NP && d0 + j == D - 1) o2 = 0xFFFF;
+            y[j] = real(j) ? c + __vimin3_s32(L[j], o2, o3) - m : kInf;
+            const int b = real(j) ? c + p1m : 0;
             AL = j == 0 ? y[0] : __viaddmin_s32(AL, b, y[j]);
             BL += b;
         }
@@ -193,15 +197,23 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
         }
         int X = __shfl_up_sync(kFull, AL, 1, seg);   // y at d0 - 1
         if (li == 0) X = kInf;
-        int mn = INT_MAX, mx = INT_MIN;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            const int d = d0 + j;
-            const int b = d < D ? cost_at<K>(c0, j) - m + P1 : 0;
+            const int b = real(j) ? cost_at<K>(c0, j) + p1m : 0;
             y[j] = __viaddmin_s32(X, b, y[j]);
             X = y[j];
-            mn = min(mn, y[j]);
-            mx = max(mx, y[j]);
+        }
+        int mn = y[0], mx = y[0];
+#pragma unroll
+        for (int j = 1; j + 1 < K; j += 2) {
+            mn = __vimin3_s32(mn, y[j], y[j + 1]);
+            mx = __vimax3_s32(mx, y[j], y[j + 1]);
+        }
+        mn = min(mn, y[K - 1]);
+        mx = max(mx, y[K - 1]);
+        if (!lane_on) {       // lanes past the vector: identities of the reductions
+            mn = INT_MAX;
+            mx = INT_MIN;
         }
         mn = seg_min(mn, seg);
         mx = seg_max(mx, seg);
@@ -233,7 +245,7 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
             int rmn = INT_MAX, rmx = INT_MIN;
 #pragma unroll
             for (int j = 0; j < K; ++j)
-                if (d0 + j < D) {
+                if (lane_on && d0 + j < D) {
                     rmn = min(rmn, y[j]);
                     rmx = max(rmx, y[j]);
                 }
@@ -262,8 +274,7 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
                 if (CP) w[1] = slot;                  // the shadow slot (bytes 4..7)
             }
             uint8_t* row = slab + pix * Dv + d0;
-            if constexpr (K == 8) __stcs(reinterpret_cast<uint2*>(row), make_uint2(w[0], w[1]));
-            else __stcs(reinterpret_cast<uint4*>(row), make_uint4(w[0], w[1], w[2], w[3]));
+            __stcs(reinterpret_cast<uint2*>(row), make_uint2(w[0], w[1]));
         }
         if (active && (wide || esc) && d0 < Dp) {
             uint16_t* dst = nullptr;
@@ -272,11 +283,6 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
             if (dst) {
                 __stcs(reinterpret_cast<uint4*>(dst),
                        make_uint4(pack2(y[0], y[1]), pack2(y[2], y[3]), pack2(y[4], y[5]), pack2(y[6], y[7])));
-                if constexpr (K == 16) {
-                    if (d0 + 8 < Dp)
-                        __stcs(reinterpret_cast<uint4*>(dst + 8), make_uint4(pack2(y[8], y[9]), pack2(y[10], y[11]),
-                                                                             pack2(y[12], y[13]), pack2(y[14], y[15])));
-                }
             }
         }
 
@@ -292,10 +298,8 @@ __device__ __forceinline__ void run_unit(const PairDev& pr, const JobDev& job, i
     }
 }
 
-// KS: which lane widths the batch needs (bit 0: K = 8, bit 1: K = 16), so that a
-// batch of one width compiles without the other's registers.
-template <bool CP, int KS>
-__global__ void __launch_bounds__(kThreads)
+template <bool CP>
+__global__ void __launch_bounds__(kThreads, 3)
 scan_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs, const UnitDev* __restrict__ units,
             const int num_units, unsigned* __restrict__ counter) {
     const int lane = threadIdx.x & 31;
@@ -308,29 +312,25 @@ scan_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs, 
         const JobDev job = jobs[unit.job];
         const PairDev& pr = pairs[job.pair];
         const ScanGeometry g = scan_geometry(pr.nd_vec);
-        if (KS == 2 || (KS == 3 && g.k == 16)) run_unit<16, CP>(pr, job, unit.first_scanline, g, lane);
-        else run_unit<8, CP>(pr, job, unit.first_scanline, g, lane);
+        if (pr.nd == pr.nd_vec) run_unit<8, CP, true>(pr, job, unit.first_scanline, g, lane);
+        else run_unit<8, CP, false>(pr, job, unit.first_scanline, g, lane);
         __syncwarp();
     }
 }
 
-const void* scan_kernel_fn(bool compact, int ks) {
-    if (compact)
-        return ks == 1 ? (const void*)scan_kernel<true, 1> : ks == 2 ? (const void*)scan_kernel<true, 2>
-                                                                  : (const void*)scan_kernel<true, 3>;
-    return ks == 1 ? (const void*)scan_kernel<false, 1> : ks == 2 ? (const void*)scan_kernel<false, 2>
-                                                                 : (const void*)scan_kernel<false, 3>;
+const void* scan_kernel_fn(bool compact) {
+    return compact ? (const void*)scan_kernel<true> : (const void*)scan_kernel<false>;
 }
 
 }  // namespace
 
-cudaError_t launch(int lane_widths, const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                   int num_units, unsigned* counter, cudaStream_t stream, bool compact) {
+cudaError_t launch(const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units, int num_units,
+                   unsigned* counter, cudaStream_t stream, bool compact) {
     if (num_units <= 0) return cudaSuccess;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void* fn = scan_kernel_fn(compact, lane_widths);
+    const void* fn = scan_kernel_fn(compact);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;

@@ -109,14 +109,14 @@ constexpr int kUnitScanlines = 64;
 // value in place of a unit size; its units hold a pair-dependent number of
 // scanlines (ScanGeometry::scanlines).
 constexpr int kScanForm = 1;
-// Geometry of the scan form for a pair with Dv bytes a vector: K disparities a
-// lane, `lanes` lanes a scanline in a segment of `seg` lanes (a power of two),
-// `scanlines` = 32 / seg scanlines a warp.
+// Geometry of the scan form for a pair with Dv bytes a vector: K = 8
+// disparities a lane, `lanes` lanes a scanline in a segment of `seg` lanes (a
+// power of two), `scanlines` = 32 / seg scanlines a warp.
 struct ScanGeometry {
     int k, lanes, seg, scanlines;
 };
 __host__ __device__ constexpr ScanGeometry scan_geometry(int nd_vec) {
-    const int k = nd_vec > 128 ? 16 : 8;
+    const int k = 8;
     const int lanes = nd_vec / k;
     int seg = 1;
     while (seg < lanes) seg <<= 1;

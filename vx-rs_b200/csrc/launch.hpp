@@ -59,10 +59,8 @@ cudaError_t launch(int dp_max, bool wide_tiles, const AggLaunch& L, const PairDe
                    cudaStream_t stream, bool compact = false);
 }  // namespace pairs
 namespace scan {
-// lane_widths: bit 0 = the batch has pairs of Dv <= 128 (8 disparities a lane),
-// bit 1 = pairs of Dv > 128 (16 a lane).
-cudaError_t launch(int lane_widths, const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units,
-                   int num_units, unsigned* counter, cudaStream_t stream, bool compact = false);
+cudaError_t launch(const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* d_units, int num_units,
+                   unsigned* counter, cudaStream_t stream, bool compact = false);
 }  // namespace scan
 namespace single {
 cudaError_t prepare();

@@ -69,7 +69,7 @@ size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg
 
 size_t pair_table_bytes_bound(uint32_t width, uint32_t height, const vx_sgm_config& cfg) {
     const size_t P = cfg.num_paths;
-    // Units of the scan form hold the fewest scanlines (ScanGeometry::scanlines >= 2).
+    // Units of the scan form hold the fewest scanlines (ScanGeometry::scanlines, 1..16).
     const size_t per_unit = (size_t)scan_geometry((cfg.num_disparities + 15) / 16 * 16).scanlines;
     const size_t units = P * (((size_t)width + height - 1 + per_unit - 1) / per_unit);
     return sizeof(PairDev) + P * sizeof(JobDev) + units * sizeof(UnitDev) + sizeof(unsigned) +
