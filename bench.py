@@ -51,6 +51,8 @@ def workload(rank: int, name: str = "mixed"):
         return [(320, 240, DISPARITIES[i % 3], 1_000_003 * (rank + 1) + i) for i in range(32)]
     if name == "profile-wide":  # 8 pairs of 1280x720, D=64: few border (x < D) pixels
         return [(1280, 720, 64, 1_000_003 * (rank + 1) + i) for i in range(8)]
+    if name == "profile-hd":  # 2 pairs of 1280x720, D=192: a 354 MB cost volume (> L2), 3.6 GB with --sync
+        return [(1280, 720, 192, 1_000_003 * (rank + 1) + i) for i in range(2)]
     rng = np.random.default_rng(20261203 + 7919 * rank)
     items = []
     for i in range(NUM_PAIRS):
@@ -233,6 +235,9 @@ def job_rate(job_pd, ms_per_step):
 # path-pd (ncu capture, dram__bytes_read.sum 26.04 GB of cost-volume reads, the
 # rest of the 29.90 GB served by L2, + dram__bytes_write.sum 29.96 GB of slabs).
 AGG_DRAM_BYTES_PER_PATH_PD = 56.00e9 / (8 * 3737760000)
+
+FORM_NAMES = {64: "scanline pairs, 64-scanline units", 32: "single scanline, 32-scanline units",
+              1: "across-lanes scan, one lane segment a scanline"}
 
 SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
 
@@ -659,7 +664,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "profile", "profile-mix", "profile-wide"])
+    ap.add_argument("--workload", default="mixed",
+                    choices=["mixed", "profile", "profile-mix", "profile-wide", "profile-hd"])
+    ap.add_argument("--sync", action="store_true",
+                    help="with --kernels-only: synchronous batch calls (escape pools, no graph), for "
+                         "profiler captures that must stay small")
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served measurement (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=300)
@@ -741,11 +750,17 @@ def main():
     oi = [ctx.texture_output_i16(w, h) for (w, h, _, _) in items]
 
     def batch():
-        sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
+        if args.sync:
+            sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi)
+        else:
+            sgm.compute_batch(ctx, tl, tr, of, cfgs, outputs_i16=oi, stream=ctx.stream)
 
     # ---- autotune the aggregation launch shape on this batch, then graph it ----
-    tuned_wg, tuned_ms, tuned_unit = sgm.autotune_batch(ctx, tl, tr, of, cfgs, oi, iterations=1)
-    sgm.set_graph_cache(2)
+    if args.sync:   # a profiler case: no autotuning runs, no graph (the planner's shape)
+        tuned_wg, tuned_ms, tuned_unit = 0, 0.0, 0
+    else:
+        tuned_wg, tuned_ms, tuned_unit = sgm.autotune_batch(ctx, tl, tr, of, cfgs, oi, iterations=1)
+        sgm.set_graph_cache(2)
 
     # ---- device-resident batched steps (headline value) ----
     for _ in range(args.warmup):
@@ -884,15 +899,15 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     # Algorithmic bytes (P2 = 120: byte path slabs, Dv = D rounded up to 16).
-    # Scanline-pair form: the cost kernel reads the left and right census and
-    # writes the cost volume (one byte per pixel-disparity); the aggregation
-    # reads the volume once per path and writes one byte per path-pd.
+    # Scanline-pair and scan forms: the cost kernel reads the left and right
+    # census and writes the cost volume (one byte per pixel-disparity); the
+    # aggregation reads the volume once per path and writes one byte per path-pd.
     # Single-scanline form: the aggregation reads the census words once per path
     # instead. The pipeline adds the census pass (images in, row-major and banded
     # planes out) and the WTA (slabs in, f32 + i16 disparities out).
     census_bytes = 4  # 5x5 census: one u32 word per pixel
     dv = lambda d: (d + 15) // 16 * 16
-    if tuned_unit == 64:
+    if tuned_unit in (64, 1):
         agg_bytes = sum(8 * 2 * w * h * dv(d) for (w, h, d, _) in items)
         costs_bytes = sum(w * h * dv(d) + 2 * w * h * census_bytes for (w, h, d, _) in items)
     else:
@@ -939,8 +954,7 @@ def main():
         "gpu_launches": launches,
         "batching": {"persistent_aggregation_launch": True, "cuda_graph_per_bucket": True,
                      "autotuned_warpgroups_per_cta": tuned_wg, "autotune_aggregate_ms": tuned_ms,
-                     "autotuned_form": "scanline pairs, 64-scanline units" if tuned_unit == 64
-                                       else "single scanline, 32-scanline units"},
+                     "autotuned_form": FORM_NAMES.get(tuned_unit, str(tuned_unit))},
         "clocks": clocks.summary(),
     }
 

@@ -221,16 +221,20 @@ __device__ __forceinline__ void cost_words(uint32_t (&cw)[8], const uint2 lo, co
 // half whose scanline starts at this pixel. row_lo / row_hi = the two
 // scanlines' rows of the warp's output tile (u16 values when WIDE, else bytes).
 // Returns the per-half maximum of the new vector (d < D). Software pipeline over
-// groups (loop unrolled by two, register sets in ping-pong): while group g runs
-// its chain, the costs (8 bytes a scanline) and state of group g+1 are in flight
-// (the state is waited for only before g's last disparity), and g+1's packed
-// costs are formed right after g's chain.
+// groups (loop unrolled by two, register sets in ping-pong): the costs come in
+// 16-byte loads of two groups a scanline (each lane reads its own rows, so one
+// load instruction touches 32 cache lines: halving the load count halves that
+// traffic), the pair after the current one in flight while it runs; the state
+// of group g+1 is in flight while group g runs its chain (waited for only
+// before g's last disparity), and g+1's packed costs are formed right after
+// g's chain. Reading 16 bytes never leaves the Dv-byte row (Dv = D rounded up
+// to 16).
 template <bool WIDE>
 __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m, const uint32_t start,
                                                  const uint8_t* __restrict__ cv_lo,
                                                  const uint8_t* __restrict__ cv_hi,
                                                  const uint8_t* __restrict__ nx_lo,
-                                                 const uint8_t* __restrict__ nx_hi, uint2& g0_lo, uint2& g0_hi,
+                                                 const uint8_t* __restrict__ nx_hi, uint4& g0_lo, uint4& g0_hi,
                                                  const ScanConst& k, unsigned char* __restrict__ row_lo,
                                                  unsigned char* __restrict__ row_hi) {
     PixelState ps;
@@ -240,9 +244,9 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
     ps.f = 0xFFFFFFFFu;            // o1 at d = 0
     ps.mn = 0xFFFFFFFFu;
     ps.mx = 0u;
-    auto load = [&](uint2& lo, uint2& hi, int g) {
-        lo = __ldg(reinterpret_cast<const uint2*>(cv_lo + 8 * g));
-        hi = __ldg(reinterpret_cast<const uint2*>(cv_hi + 8 * g));
+    auto load = [&](uint4& lo, uint4& hi, int g) {   // groups g, g+1 (g even)
+        lo = __ldg(reinterpret_cast<const uint4*>(cv_lo + 8 * g));
+        hi = __ldg(reinterpret_cast<const uint4*>(cv_hi + 8 * g));
     };
     auto store = [&](const Words8& o, int g) {
         if (WIDE) {             // u16 rows: 8 values (16 bytes) per group
@@ -260,42 +264,42 @@ __device__ __forceinline__ uint32_t sgm_pixel(const uint32_t tstate, uint32_t& m
         }
         tmem_st8(tstate + 8 * g, o);
     };
-    uint2 pa_l = g0_lo, pa_h = g0_hi, pb_l, pb_h;     // group 0, loaded during the previous pixel
+    uint4 q_l = g0_lo, q_h = g0_hi, n_l, n_h;      // groups 0 and 1, loaded during the previous pixel
     uint32_t ca[8], cb[8];
     Words8 oa, ob;
     uint32_t w7;
     Words8 sa = tmem_ld8(tstate), sb;
-    cost_words(ca, pa_l, pa_h);
+    cost_words(ca, make_uint2(q_l.x, q_l.y), make_uint2(q_h.x, q_h.y));
     tmem_wait_ld(sa);
     int g = 0;
 #pragma unroll 1
     for (; g + 2 < k.G; g += 2) {
+        load(n_l, n_h, g + 2);                       // groups g+2, g+3 in flight
         sb = tmem_ld8(tstate + 8 * (g + 1));
-        load(pb_l, pb_h, g + 1);
         sgm_group_head<false>(sa, ca, k, ps, oa, w7);
         tmem_wait_ld(sb);
         sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
         store(oa, g);
-        cost_words(cb, pb_l, pb_h);
+        cost_words(cb, make_uint2(q_l.z, q_l.w), make_uint2(q_h.z, q_h.w));
         sa = tmem_ld8(tstate + 8 * (g + 2));
-        load(pa_l, pa_h, g + 2);
         sgm_group_head<false>(sb, cb, k, ps, ob, w7);
         tmem_wait_ld(sa);
         sgm_group_tail<false>(sb, sa.w[0], w7, k, ps, ob);
         store(ob, g + 1);
-        cost_words(ca, pa_l, pa_h);
+        q_l = n_l;
+        q_h = n_h;
+        cost_words(ca, make_uint2(q_l.x, q_l.y), make_uint2(q_h.x, q_h.y));
     }
-    // The next pixel's group 0 (nx_lo / nx_hi: its rows, or any valid row).
-    g0_lo = __ldg(reinterpret_cast<const uint2*>(nx_lo));
-    g0_hi = __ldg(reinterpret_cast<const uint2*>(nx_hi));
+    // The next pixel's groups 0 and 1 (nx_lo / nx_hi: its rows, or any valid row).
+    g0_lo = __ldg(reinterpret_cast<const uint4*>(nx_lo));
+    g0_hi = __ldg(reinterpret_cast<const uint4*>(nx_hi));
     if (g + 1 < k.G) {
         sb = tmem_ld8(tstate + 8 * (g + 1));
-        load(pb_l, pb_h, g + 1);
         sgm_group_head<false>(sa, ca, k, ps, oa, w7);
         tmem_wait_ld(sb);
         sgm_group_tail<false>(sa, sb.w[0], w7, k, ps, oa);
         store(oa, g);
-        cost_words(cb, pb_l, pb_h);
+        cost_words(cb, make_uint2(q_l.z, q_l.w), make_uint2(q_h.z, q_h.w));
         sgm_group_head<true>(sb, cb, k, ps, ob, w7);
         sgm_group_tail<true>(sb, 0u, w7, k, ps, ob);
         store(ob, g + 1);
@@ -469,13 +473,13 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     const int t_hi = __reduce_max_sync(kFull, max(te_lo, te_hi));
     if (t_lo >= t_hi) return;
 
+    const uint8_t* __restrict__ CV = pr.costs;
+    uint32_t m = 0u;
     // Costs from the pair's cost volume: the two scanlines' rows at the step's
     // pixels (a half outside its scanline reads pixel 0's row, in bounds and
     // unused: it restarts from L = C where its scanline begins).
-    const uint8_t* __restrict__ CV = pr.costs;
     unsigned char* row_lo = tile + lane * row_bytes;
     unsigned char* row_hi = tile + (lane + 32) * row_bytes;
-    uint32_t m = 0u;
     // Cost rows of step t's two scanlines (pixel 0's row for a half outside its scanline).
     auto rows_at = [&](int t, const uint8_t*& lo, const uint8_t*& hi) {
         const size_t p0 = (size_t)((ptrdiff_t)(y0 + dy * t) * W + k0 + dx * t);
@@ -484,7 +488,7 @@ __device__ __forceinline__ void run_vertical_unit(const PairDev& pr, const JobDe
     };
     const uint8_t *cv_lo, *cv_hi;
     rows_at(t_lo, cv_lo, cv_hi);
-    uint2 g0_lo = __ldg(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint2*>(cv_hi));
+    uint4 g0_lo = __ldg(reinterpret_cast<const uint4*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint4*>(cv_hi));
     for (int t = t_lo; t < t_hi; ++t) {
         const bool act_lo = t >= tb_lo && t < te_lo, act_hi = t >= tb_hi && t < te_hi;
         const uint32_t start = (t == tb_lo ? 0x0000FFFFu : 0u) | (t == tb_hi ? 0xFFFF0000u : 0u);
@@ -517,18 +521,18 @@ __device__ __forceinline__ void run_horizontal_unit(const PairDev& pr, const Job
     const EscapeTarget et = CP ? escape_target(pr, job.path) : EscapeTarget{};
     const bool act_lo = first + lane < job.num_scanlines;
     const bool act_hi = first + 32 + lane < job.num_scanlines;
-    // Costs from the pair's cost volume: rows first + lane and first + 32 + lane
-    // at column x (a row past the image reads pixel 0's row, unused).
     const uint8_t* __restrict__ CV = pr.costs;
-    unsigned char* row_lo = tile + lane * row_bytes;
-    unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     uint32_t m = 0u;
     const int x0 = dx > 0 ? 0 : W - 1;
+    // Costs from the pair's cost volume: rows first + lane and first + 32 + lane
+    // at column x (a row past the image reads pixel 0's row, unused).
+    unsigned char* row_lo = tile + lane * row_bytes;
+    unsigned char* row_hi = tile + (lane + 32) * row_bytes;
     // Column x's cost rows of the two scanlines (pixel 0's row for a row past the image).
     const uint8_t* cv_lo = CV + (act_lo ? ((size_t)(first + lane) * W + x0) * Dv : 0);
     const uint8_t* cv_hi = CV + (act_hi ? ((size_t)(first + 32 + lane) * W + x0) * Dv : 0);
     const ptrdiff_t step_lo = act_lo ? (ptrdiff_t)dx * Dv : 0, step_hi = act_hi ? (ptrdiff_t)dx * Dv : 0;
-    uint2 g0_lo = __ldg(reinterpret_cast<const uint2*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint2*>(cv_hi));
+    uint4 g0_lo = __ldg(reinterpret_cast<const uint4*>(cv_lo)), g0_hi = __ldg(reinterpret_cast<const uint4*>(cv_hi));
     for (int t = 0; t < W; ++t) {
         const int x = x0 + dx * t;
         const uint32_t start = t == 0 ? 0xFFFFFFFFu : 0u;

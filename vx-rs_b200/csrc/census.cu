@@ -6,9 +6,10 @@
 // texels as value/255 floats; comparing those is the same as comparing the
 // u8 values, which is what this kernel does.
 //
-// Layout: each 32x8 tile of one view is staged once in shared memory with its
-// (rx, ry) apron (clamped coordinates), then every thread builds one
-// descriptor from shared memory. Descriptors are written row-major (read by
+// Layout: each 32x32 tile of one view is staged once in shared memory with its
+// (rx, ry) apron (clamped coordinates), then every thread builds four
+// descriptors (rows 8 apart) from shared memory: large tiles, so that the
+// per-CTA costs (finding the pair, staging latency) are paid per 1024 pixels. Descriptors are written row-major (read by
 // the cost-volume kernel and by the vertical and diagonal paths of the
 // single-scanline aggregation) and, for batches run by the single-scanline
 // aggregation only, a second time in 32-row bands, x-major inside a band, word
@@ -59,10 +60,11 @@ __device__ __forceinline__ uint64_t window_bits(const uint8_t* __restrict__ tile
 }
 
 template <typename CT, bool BANDED>
-__global__ void __launch_bounds__(kCensusTileW * kCensusTileH)
+__global__ void __launch_bounds__(kCensusTileW * kCensusThreadsY)
 census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ uint8_t tile_px[];
-    __shared__ CT tile_bits[kCensusTileH][kCensusTileW];
+    __shared__ CT tile_bits[kCensusTileH][kCensusTileW + 1];
+    constexpr int kRowsPerThread = kCensusTileH / kCensusThreadsY;
     const int pi = find_pair_by_tile(pairs, num_pairs, blockIdx.x);
     const PairDev& pr = pairs[pi];
     const int W = pr.width, H = pr.height, rx = pr.rx, ry = pr.ry;
@@ -78,35 +80,41 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
 
     const int sw = kCensusTileW + 2 * rx, sh = kCensusTileH + 2 * ry;
     const int tid = threadIdx.y * kCensusTileW + threadIdx.x;
-    for (int i = tid; i < sw * sh; i += kCensusTileW * kCensusTileH) {
+    constexpr int kThreads = kCensusTileW * kCensusThreadsY;
+    for (int i = tid; i < sw * sh; i += kThreads) {
         const int sx = min(max(bx - rx + i % sw, 0), W - 1);
         const int sy = min(max(by - ry + i / sw, 0), H - 1);
         tile_px[i] = img[(size_t)sy * pitch + sx];
     }
     __syncthreads();
 
-    const int x = bx + threadIdx.x, y = by + threadIdx.y;
     // Clamped reads at the image border equal reads of the staged apron, which
     // was filled with clamped coordinates; interior threads read their window.
     // The common windows (5x5, 9x7) are unrolled; the radii are uniform per CTA.
-    const int cx = threadIdx.x + rx, cy = threadIdx.y + ry;
-    uint64_t bits;
-    if (rx == 2 && ry == 2) bits = window_bits<2, 2>(tile_px, sw, cx, cy, rx, ry);
-    else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, sw, cx, cy, rx, ry);
-    else bits = window_bits<-1, -1>(tile_px, sw, cx, cy, rx, ry);
     CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
-    if (x < W && y < H) rm[(size_t)y * W + x] = (CT)bits;
-    if constexpr (!BANDED) return;   // the scanline-pair aggregation reads the cost volume instead
+    const int x = bx + threadIdx.x, cx = threadIdx.x + rx;
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        const int ty = threadIdx.y + k * kCensusThreadsY;
+        const int y = by + ty, cy = ty + ry;
+        uint64_t bits;
+        if (rx == 2 && ry == 2) bits = window_bits<2, 2>(tile_px, sw, cx, cy, rx, ry);
+        else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, sw, cx, cy, rx, ry);
+        else bits = window_bits<-1, -1>(tile_px, sw, cx, cy, rx, ry);
+        if (x < W && y < H) rm[(size_t)y * W + x] = (CT)bits;
+        if constexpr (BANDED) tile_bits[ty][threadIdx.x] = (CT)bits;
+    }
+    if constexpr (!BANDED) return;   // the scanline-pair and scan aggregations read the cost volume instead
+    // Banded copy: the tile is one 32-row band (by is a multiple of 32), so a
+    // tile column is 32 consecutive words there; the descriptors go through
+    // shared memory and consecutive threads write consecutive words.
     CT* cm = static_cast<CT*>(view ? pr.census_rt : pr.census_lt);
-    // Banded copy: the tile's 8 rows of one column are 8 consecutive words
-    // there, so the descriptors go through shared memory and thread t writes
-    // column t / 8, row t % 8: eight threads fill one contiguous run.
-    tile_bits[threadIdx.y][threadIdx.x] = (CT)bits;
     __syncthreads();
-    const int tid2 = threadIdx.y * kCensusTileW + threadIdx.x;
-    const int ox = bx + tid2 / kCensusTileH, oy = by + tid2 % kCensusTileH;
-    if (ox < W && oy < H)
-        cm[((size_t)(oy >> 5) * W + ox) * 32 + (oy & 31)] = tile_bits[tid2 % kCensusTileH][tid2 / kCensusTileH];
+    for (int w = tid; w < kCensusTileW * kCensusTileH; w += kThreads) {
+        const int col = w / kCensusTileH, row = w % kCensusTileH;
+        const int ox = bx + col, oy = by + row;
+        if (ox < W && oy < H) cm[((size_t)(oy >> 5) * W + ox) * 32 + (oy & 31)] = tile_bits[row][col];
+    }
 }
 
 }  // namespace
@@ -114,7 +122,7 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
 cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles, int max_rx,
                           int max_ry, bool census64, bool banded, cudaStream_t stream) {
     if (total_tiles == 0) return cudaSuccess;
-    const dim3 block(kCensusTileW, kCensusTileH);
+    const dim3 block(kCensusTileW, kCensusThreadsY);
     const size_t smem = (size_t)(kCensusTileW + 2 * max_rx) * (kCensusTileH + 2 * max_ry);
     count_launch();
     if (census64) {

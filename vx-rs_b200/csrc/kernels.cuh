@@ -99,8 +99,9 @@ struct UnitDev {
     int first_scanline;
 };
 
-constexpr int kCensusTileW = 32;
-constexpr int kCensusTileH = 8;
+constexpr int kCensusTileW = 32;   // census tile: 32 x 32 pixels of one view a CTA
+constexpr int kCensusTileH = 32;
+constexpr int kCensusThreadsY = 8; // CTA of 32 x 8 threads, four rows a thread
 constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
 // Scanlines per aggregation work unit of the scanline-pair kernel (one warp:
 // two scanlines per lane); the single-scanline kernel takes 32.
@@ -123,9 +124,17 @@ __host__ __device__ constexpr ScanGeometry scan_geometry(int nd_vec) {
     return ScanGeometry{k, lanes, seg, 32 / seg};
 }
 // Fewest 64-scanline units for which a batch whose key was not autotuned runs
-// the scanline-pair kernel (on B200 the forms cross over between 6 000 and
-// 8 000 units; the autotuner times both).
-constexpr long long kPairKernelMinUnits = 7500;
+// the scanline-pair kernel (below: the across-lanes scan kernel; the
+// single-scanline kernel is left to the autotuner, which times all three).
+constexpr long long kPairKernelMinUnits = 1500;
+// Fewer 64-scanline units than this run the across-lanes scan kernel when the
+// batch's key was not autotuned (a lone pair, small batches: it gives every
+// scanline a segment of lanes, so few scanlines still fill the GPU). Measured
+// on B200 with the leading pairs of the 64-pair mixed batch: up to 8 pairs
+// (1 020 units) the scan form is fastest (1 pair: 2.29 ms against 6.45 ms for the
+// scanline pairs, whose time there is that of its longest unit), from 16 pairs
+// (2 232 units) the scanline pairs (6.45 against 9.64 single, 12.0 scan).
+constexpr long long kScanFormMaxUnits = 1500;
 // Largest aggregation CTA (4 warpgroups); keeps registers per thread <= 128.
 constexpr int kAggMaxThreads = 512;
 constexpr int kAggMaxWarpgroups = kAggMaxThreads / 128;

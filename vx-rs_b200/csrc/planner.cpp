@@ -316,10 +316,11 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     pl.total_tiles = tiles;
     pl.total_rows = rows;
 
-    // Unit size, i.e. aggregation form: a batch with enough 64-scanline units to
-    // give every warp of the GPU several runs the scanline-pair kernel; fewer
-    // units (a single pair, small batches) run the single-scanline kernel on
-    // 32-scanline units, twice the parallelism for the same work.
+    // Unit size, i.e. aggregation form: few units (a single pair, small batches)
+    // run the across-lanes scan kernel, a segment of lanes per scanline; larger
+    // batches the scanline-pair kernel (fewest instructions per path-pd). The
+    // single-scanline kernel runs when the autotuner picked it for the batch's
+    // key or VX_SGM_AGG_FORM asks for it.
     long long units64 = 0;
     pl.units32 = 0;
     for (const JobDev& j : pl.jobs) {
@@ -329,7 +330,9 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     if (unit_scanlines == kUnitScanlines || unit_scanlines == 32 || unit_scanlines == kScanForm)
         pl.unit_scanlines = unit_scanlines;        // the autotuned form
     else
-        pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines : 32;
+        pl.unit_scanlines = units64 >= kPairKernelMinUnits ? kUnitScanlines
+                            : units64 < kScanFormMaxUnits  ? kScanForm
+                                                           : 32;
     // VX_SGM_AGG_FORM=pairs|single|scan forces one form (all are exact; the tests
     // run every case through each).
     if (const char* f = std::getenv("VX_SGM_AGG_FORM")) {
