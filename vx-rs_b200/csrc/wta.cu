@@ -167,25 +167,15 @@ __device__ __forceinline__ void sum_paths(const RowView& rv, size_t pix, int c, 
     acc[3] = __byte_perm(a[2], a[3], 0x7632);
 }
 
-// Four CTAs per SM (at most 64 registers a thread, no spills) keep enough slab loads in flight.
-__global__ void __launch_bounds__(kWtaThreads, 4)
-wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
-    const PairDev pr = pairs[pi];                  // fields live in registers
-    const int y = blockIdx.x - pr.row_begin;
-    const int W = pr.width, D = pr.nd, P = pr.num_paths;
+// The disparity loop of one image row: every pixel's first-minimum key, its
+// neighbours' sums and (LR) the row's right-view keys into shared memory. The
+// path count and slab form are template parameters, so each variant is its own
+// straight-line loop with no per-round dispatch.
+template <int NP, bool WIDE>
+__device__ __forceinline__ void wta_row(const PairDev& pr, int y, uint32_t* smem, uint32_t* right_key,
+                                        uint32_t* best_key, uint32_t* nbr) {
+    const int W = pr.width, D = pr.nd;
     const bool lr = pr.lr_check != 0;
-
-    uint32_t* right_key = smem;                               // W keys (LR only)
-    uint32_t* best_key = smem + W;                            // W: S(bd) << 8 | bd
-    uint32_t* nbr = smem + 2 * W;                             // W: S(bd-1) | S(bd+1) << 16
-                                                              // then the warps' sums
-
-    if (lr)
-        for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
-    __syncthreads();
-
     const int chunks = pr.nd_vec / 8;               // 8-disparity chunks per pixel
     int seg = 1;
     while (seg < chunks && seg < 8) seg <<= 1;      // lanes per pixel (power of two, at most 8)
@@ -194,9 +184,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const int nwarps = blockDim.x >> 5;
     const int sub = lane / seg, c = lane % seg;
     const int ppw = 32 / seg;
-    const int kind = (P == 2 ? 0 : P == 4 ? 1 : 2) + (pr.wide_slabs ? 3 : 0);
     const RowView rv{pr.slabs, pr.shadow, pr.slab_stride, pr.shadow_stride, pr.nd_pad, pr.nd_vec, pr.shadow_cap};
-    const bool subpixel = pr.subpixel != 0;
 
     // This warp's sums of the current pixels: ppw rows of 8 * seg * rounds u16
     // (S(d) at d), read back for S(bd-1) and S(bd+1).
@@ -213,25 +201,8 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
             const int cc = r * seg + c;             // this lane's chunk: d = 8cc..8cc+7
             const bool act = actx && cc < chunks;
             uint32_t acc[4] = {0u, 0u, 0u, 0u};     // acc[k] = S(8cc+2k) | S(8cc+2k+1) << 16
-            if (r == 0) {
-                switch (kind) {                     // uniform over the CTA
-                    case 0: sum_paths<2, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 1: sum_paths<4, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 2: sum_paths<8, false, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 3: sum_paths<2, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 4: sum_paths<4, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    default: sum_paths<8, true, true>(rv, pix, cc, act, sub * seg, em, acc); break;
-                }
-            } else {
-                switch (kind) {
-                    case 0: sum_paths<2, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 1: sum_paths<4, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 2: sum_paths<8, false, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 3: sum_paths<2, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    case 4: sum_paths<4, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                    default: sum_paths<8, true, false>(rv, pix, cc, act, sub * seg, em, acc); break;
-                }
-            }
+            if (r == 0) sum_paths<NP, WIDE, true>(rv, pix, cc, act, sub * seg, em, acc);
+            else        sum_paths<NP, WIDE, false>(rv, pix, cc, act, sub * seg, em, acc);
             *reinterpret_cast<uint4*>(srow_p + 8 * cc) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
             // key = S(d) << 8 | d (one byte permute: d in byte 0, S in bytes 1-2;
             // d = 8cc + j < 256), whose minimum is the first minimum.
@@ -274,6 +245,36 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
             nbr[x] = c0 | (c2 << 16);
         }
         __syncwarp();                               // before the next pixels' sums
+    }
+}
+
+// Four CTAs per SM (at most 64 registers a thread, no spills) keep enough slab loads in flight.
+__global__ void __launch_bounds__(kWtaThreads, 4)
+wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
+    const PairDev pr = pairs[pi];                  // fields live in registers
+    const int y = blockIdx.x - pr.row_begin;
+    const int W = pr.width, D = pr.nd, P = pr.num_paths;
+    const bool lr = pr.lr_check != 0;
+
+    uint32_t* right_key = smem;                               // W keys (LR only)
+    uint32_t* best_key = smem + W;                            // W: S(bd) << 8 | bd
+    uint32_t* nbr = smem + 2 * W;                             // W: S(bd-1) | S(bd+1) << 16
+                                                              // then the warps' sums
+
+    if (lr)
+        for (int x = threadIdx.x; x < W; x += blockDim.x) right_key[x] = 0xFFFFFFFFu;
+    __syncthreads();
+
+    const bool subpixel = pr.subpixel != 0;
+    switch ((P == 2 ? 0 : P == 4 ? 1 : 2) + (pr.wide_slabs ? 3 : 0)) {   // uniform over the CTA
+        case 0: wta_row<2, false>(pr, y, smem, right_key, best_key, nbr); break;
+        case 1: wta_row<4, false>(pr, y, smem, right_key, best_key, nbr); break;
+        case 2: wta_row<8, false>(pr, y, smem, right_key, best_key, nbr); break;
+        case 3: wta_row<2, true>(pr, y, smem, right_key, best_key, nbr); break;
+        case 4: wta_row<4, true>(pr, y, smem, right_key, best_key, nbr); break;
+        default: wta_row<8, true>(pr, y, smem, right_key, best_key, nbr); break;
     }
     __syncthreads();
 
