@@ -230,11 +230,21 @@ def job_rate(job_pd, ms_per_step):
     return job_pd / (ms_per_step * 1e-3) / 1e9
 
 
-# DRAM bytes (read + write) one aggregation launch (scanline-pair form) of the
-# 64-pair workload moved per path-pixel-disparity: 56.00 GB over 8 x 3.738 G
-# path-pd (ncu capture, dram__bytes_read.sum 26.04 GB of cost-volume reads, the
-# rest of the 29.90 GB served by L2, + dram__bytes_write.sum 29.96 GB of slabs).
-AGG_DRAM_BYTES_PER_PATH_PD = 56.00e9 / (8 * 3737760000)
+# DRAM bytes (read + write) per path-pixel-disparity of one aggregation launch in
+# the scanline-pair form (three warpgroups a CTA), measured on a small case of
+# the same workload and scaled by path-pd: the first 8 pairs of the mixed
+# workload (3.741 G path-pd, 3.74 GB of byte slabs), one launch,
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:aggregate_kernel
+#   (VX_SGM_AGG_FORM=pairs VX_SGM_AGG_WARPGROUPS=3 python bench.py --workload mixed
+#    --pairs 8 --kernels-only --steps 2 --warmup 3)
+# read 2.141 GB (cost-volume reads that missed L2) + write 3.703 GB (slabs and
+# escaped vectors' shadow) = 5.845 GB. Traffic grows with path-pd: the
+# 1280x720 D=192 pair case gives 0.77 of its algorithmic bytes too.
+AGG_DRAM_BYTES_PER_PATH_PD = (2.141e9 + 3.703e9) / 3740620800
+AGG_TRAFFIC_SAMPLE = ("first 8 pairs of the mixed workload (3.741 G path-pd), one scanline-pair launch "
+                      "with 3 warpgroups: ncu dram__bytes_read.sum 2.141 GB + dram__bytes_write.sum "
+                      "3.703 GB, scaled by path-pd")
 
 FORM_NAMES = {64: "scanline pairs, 64-scanline units", 32: "single scanline, 32-scanline units",
               1: "across-lanes scan, one lane segment a scanline"}
@@ -941,13 +951,14 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "path aggregation (all pairs, all paths)",
                      "achieved": agg_gbs, "peak": peak, "unit": "GB/s", "frac": agg_gbs / peak,
                      "peak_source": peak_src,
-                     "traffic": AGG_DRAM_BYTES_PER_PATH_PD * 8 * total_pd,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "aggregation launch of this workload, per path-pixel-disparity",
+                     "traffic": AGG_DRAM_BYTES_PER_PATH_PD * 8 * total_pd if tuned_unit == 64 else None,
+                     "traffic_source": AGG_TRAFFIC_SAMPLE if tuned_unit == 64 else
+                     "not measured for this form (the capture is of the scanline-pair form)",
                      "algorithmic_bytes_per_launch": agg_bytes,
-                     "bound_note": "the recurrence is latency-bound (two warps a scheduler: tensor "
-                                   "memory holds two warpgroups' state at D <= 256; each pixel's "
-                                   "chain is serial over d); HBM is not its limit"},
+                     "bound_note": "the recurrence is bound by L1 requests and latency, not HBM: each "
+                                   "lane reads its own scanline's cost row (a 16-byte load of a warp "
+                                   "touches ~27 sectors) and each pixel's chain is serial over d; "
+                                   "tensor memory holds three warpgroups' state a CTA"},
         "pipeline_roofline": {"bytes_per_step": pipeline_bytes,
                               "achieved_gbs": pipeline_bytes / (ms * 1e-3) / 1e9,
                               "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / peak},

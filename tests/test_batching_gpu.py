@@ -166,7 +166,7 @@ def test_synchronous_batch_escape_pools(gpu_ctx, monkeypatch, pool):
     pairs, cfgs, ocfgs = [], [], []
     for i in range(6):
         w, h = int(rng.choice([120, 203])), int(rng.choice([70, 101]))
-        nd = [64, 128, 96][i % 3]
+        nd = [64, 128, 96, 192, 160, 48][i]     # both WTA lane forms (16 a lane; 8 at 129..192)
         L, R, _ = vx_sgm.synth_pair(2, w, h, 0, nd - 6, 900 + i)
         c, o = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2, num_paths=8, lr_check=True,
                         p1=float(rng.choice([2, 10])), p2=float(rng.choice([60, 120])))

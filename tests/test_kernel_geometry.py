@@ -5,8 +5,10 @@ matching cost (popcount of the census XOR, 64 where x - d < 0, 0 in the pads),
 every census load stays inside the planes' guard words and is 16-byte aligned,
 and every shared-memory tile index stays inside the launch's allocation.
 
-wta.cu (per-warp sums): every 16-byte store into the sums rows is aligned and
-inside the dynamic shared memory, for odd widths too.
+wta.cu (row loop): the lane form chosen per pair (16 or 8 disparities a lane),
+every 16-byte store into the per-warp sums rows aligned and inside the
+dynamic shared memory, for odd widths too; the padded right-view key indices
+inside their array and the atomics' bank conflicts bounded.
 
 The constants mirror the kernels' (cost.cu: kBlockPx, kTileRows, kMaxTileBytes;
 kernels.cuh: kCensusGuardWords, kWtaThreads, kWtaSumsPerWarp)."""
@@ -111,27 +113,106 @@ def test_cost_kernel_passes_fill_the_warps():
         assert _tile_units(dv) * 16 <= K_MAX_TILE_BYTES
 
 
+FORM_BYTES16, FORM_BYTES8, FORM_WIDE = 0, 1, 2
+
+
+def _wta_k(form):
+    return 16 if form == FORM_BYTES16 else 8
+
+
+def _wta_seg(dv, form):
+    chunks, cap = dv // _wta_k(form), 16 if form == FORM_BYTES16 else 8
+    seg = 1
+    while seg < chunks and seg < cap:
+        seg <<= 1
+    return seg
+
+
+def _wta_form(dv, wide):
+    if wide:
+        return FORM_WIDE
+    c16, s16 = dv // 16, _wta_seg(dv, FORM_BYTES16)
+    c8, s8 = dv // 8, _wta_seg(dv, FORM_BYTES8)
+    slots16, slots8 = s16 * -(-c16 // s16), s8 * -(-c8 // s8)
+    return FORM_BYTES8 if c8 * slots16 > c16 * slots8 else FORM_BYTES16
+
+
+def _right_key_words(w):
+    return w + ((w + 15) >> 4) * 4
+
+
+def _right_key_pad(seg, form):
+    return 0 if form != FORM_BYTES16 else 2 if seg >= 16 else 4 if seg == 8 else 0
+
+
+def _right_key_index(a, pad):
+    return a + (a >> 4) * pad
+
+
+def _wta_sums_base(w):
+    return ((_right_key_words(w) + 2 * w + 3) & ~3) * 4           # bytes
+
+
 def _wta_smem_bytes(max_width):
-    return ((max_width * 3 + 3) // 4 * 4) * 4 + (K_WTA_THREADS // 32) * K_WTA_SUMS_PER_WARP * 2
+    return _wta_sums_base(max_width) + (K_WTA_THREADS // 32) * K_WTA_SUMS_PER_WARP * 2
+
+
+def test_wta_forms_keep_lanes_busy():
+    # 16 disparities a lane unless 8 fills more lane-rounds: D = 144..192 (Dv / 16 = 9..12).
+    forms = {d: _wta_form((d + 15) // 16 * 16, False) for d in range(1, 257)}
+    assert {d for d, f in forms.items() if f == FORM_BYTES8} == set(range(129, 193))
+    assert forms[64] == forms[128] == forms[256] == FORM_BYTES16 and forms[192] == FORM_BYTES8
+    # The largest launch fits the 227 KB a CTA may hold.
+    assert _wta_smem_bytes(16384) <= 227 * 1024
 
 
 def test_wta_sums_rows_aligned_and_in_bounds():
     for D in range(1, 257):
         dv = (D + 15) // 16 * 16
-        chunks = dv // 8
-        seg = 1
-        while seg < chunks and seg < 8:
-            seg <<= 1
-        rounds = (chunks + seg - 1) // seg
-        assert (32 // seg) * 8 * seg * rounds <= K_WTA_SUMS_PER_WARP
-        for W in (1, 2, 3, 5, 7, 33, 1241, 1242, 16383):
-            base = ((3 * W + 3) & ~3) * 4                # bytes
-            assert base % 16 == 0
-            for warp in range(K_WTA_THREADS // 32):
+        for form in {_wta_form(dv, False), FORM_WIDE}:
+            k, seg = _wta_k(form), _wta_seg(dv, form)
+            chunks = dv // k
+            rounds = (chunks + seg - 1) // seg
+            assert (32 // seg) * k * seg * rounds <= K_WTA_SUMS_PER_WARP
+            for W in (1, 2, 3, 5, 7, 33, 1241, 1242, 16383, 16384):
+                base = _wta_sums_base(W)
+                assert base % 16 == 0
+                for warp in range(K_WTA_THREADS // 32):
+                    for lane in range(32):
+                        sub, c = divmod(lane, seg)
+                        row = base + (warp * K_WTA_SUMS_PER_WARP + sub * k * seg * rounds) * 2
+                        for r in range(rounds):
+                            for q in range(k // 8):
+                                off = row + 2 * (k * (r * seg + c) + 8 * q)
+                                assert off % 16 == 0 and off + 16 <= _wta_smem_bytes(W)
+                        assert row + 2 * D <= _wta_smem_bytes(W)   # the S(bd +- 1) reads
+
+
+def test_wta_right_keys_in_bounds_and_spread_over_banks():
+    # Every right-view column 0..W-1 maps inside the padded array, below the
+    # per-pixel arrays; one atomicMin instruction (fixed key index j) of a warp
+    # meets at most 2 lanes on a bank (the byte form at 8 and 16 lanes a pixel: 1).
+    for W in (1, 15, 16, 17, 1242, 16384):
+        for form in (FORM_BYTES16, FORM_BYTES8, FORM_WIDE):
+            for seg in (1, 2, 4, 8, 16):
+                pad = _right_key_pad(seg, form)
+                assert _right_key_index(W - 1, pad) < _right_key_words(W)
+    for D in (64, 128, 192, 256, 48, 96, 200):
+        dv = (D + 15) // 16 * 16
+        form = _wta_form(dv, False)
+        k, seg = _wta_k(form), _wta_seg(dv, form)
+        pad = _right_key_pad(seg, form)
+        worst = 0
+        for xb in range(256, 256 + 64):
+            for j in range(k):
+                banks = {}
                 for lane in range(32):
-                    sub, c = divmod(lane, seg)
-                    row = base + (warp * K_WTA_SUMS_PER_WARP + sub * 8 * seg * rounds) * 2
-                    for r in range(rounds):
-                        off = row + 16 * (r * seg + c)
-                        assert off % 16 == 0 and off + 16 <= _wta_smem_bytes(W)
-                    assert row + 2 * D <= _wta_smem_bytes(W)   # the S(bd +- 1) reads
+                    s, c = divmod(lane, seg)
+                    if k * c >= D:
+                        continue
+                    b = _right_key_index(xb + s - k * c - j, pad) % 32
+                    banks[b] = banks.get(b, 0) + 1
+                worst = max(worst, max(banks.values()))
+        assert worst <= 2, (D, worst)
+        if form == FORM_BYTES16 and seg >= 8 and D % 128 == 0:
+            assert worst == 1, (D, worst)

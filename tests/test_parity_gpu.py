@@ -83,6 +83,25 @@ def test_edge_shapes(gpu_ctx, sgm, agg_form):
         assert_disparity_equal(got, (d, di), what=f"{w}x{h} D={nd}")
 
 
+@pytest.mark.parametrize("nd,paths,p2", [
+    (128, 8, 120), (129, 2, 120), (144, 8, 300), (160, 4, 120), (192, 8, 300), (193, 4, 120),
+    (208, 8, 120), (248, 2, 300), (256, 4, 300), (80, 8, 300), (24, 4, 120),
+])
+def test_wta_lane_forms_match_oracle(gpu_ctx, sgm, nd, paths, p2):
+    """The WTA's row-loop forms (16 disparities a lane; 8 a lane where D = 129..192
+    fills its lanes better; padded right-view keys) on each side of the form
+    boundaries, every path count, with LR and with escaped byte vectors (P2 = 300
+    lifts path costs past a byte)."""
+    w, h = 233, 19
+    L, R, _ = vx_sgm.synth_pair(nd % 3, w, h, 0, nd - 3, nd * 31 + paths)
+    for lr in (True, False):
+        cfg, ocfg = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2, num_paths=paths,
+                             p1=15 if p2 == 300 else 10, p2=p2, lr_check=lr, lr_tolerance=1)
+        got = run_pair(gpu_ctx, sgm, L, R, cfg)
+        d, di, _ = oracle.sgm(L, R, ocfg)
+        assert_disparity_equal(got, (d, di), what=f"D={nd} P={paths} p2={p2} lr={lr}")
+
+
 def test_batch_equals_solo(gpu_ctx, sgm, agg_form):
     rng = np.random.default_rng(1)
     pairs, cfgs = [], []

@@ -174,9 +174,11 @@ __host__ __device__ constexpr size_t aggregate_tile_offset(int dp_max) { return 
 
 constexpr int kWtaThreads = 256;
 // u16 sums per WTA warp in shared memory: its pixels (32 / lanes per pixel) x
-// their padded disparities (8 x lanes per pixel x rounds) <= 4 x 256.
+// their padded disparities (disparities a lane x lanes per pixel x rounds):
+// byte slabs 32 x 16 x 1, wide slabs 32 x 8 x 4 at most.
 constexpr int kWtaSumsPerWarp = 1024;
-// Widest image the WTA kernel accepts (three 4-byte words per pixel in shared memory).
+// Widest image the WTA kernel accepts (three 4-byte words per pixel and the
+// right-view keys' padding, a quarter word per pixel, in shared memory).
 constexpr int kMaxWidth = 16384;
 
 }  // namespace vxsgm
