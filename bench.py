@@ -231,20 +231,22 @@ def job_rate(job_pd, ms_per_step):
 
 
 # DRAM bytes (read + write) per path-pixel-disparity of one aggregation launch in
-# the scanline-pair form (three warpgroups a CTA), measured on a small case of
-# the same workload and scaled by path-pd: the first 8 pairs of the mixed
-# workload (3.741 G path-pd, 3.74 GB of byte slabs), one launch,
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#       --clock-control none -k regex:aggregate_kernel
-#   (VX_SGM_AGG_FORM=pairs VX_SGM_AGG_WARPGROUPS=3 python bench.py --workload mixed
-#    --pairs 8 --kernels-only --steps 2 --warmup 3)
-# read 2.141 GB (cost-volume reads that missed L2) + write 3.703 GB (slabs and
-# escaped vectors' shadow) = 5.845 GB. Traffic grows with path-pd: the
-# 1280x720 D=192 pair case gives 0.77 of its algorithmic bytes too.
-AGG_DRAM_BYTES_PER_PATH_PD = (2.141e9 + 3.703e9) / 3740620800
-AGG_TRAFFIC_SAMPLE = ("first 8 pairs of the mixed workload (3.741 G path-pd), one scanline-pair launch "
-                      "with 3 warpgroups: ncu dram__bytes_read.sum 2.141 GB + dram__bytes_write.sum "
-                      "3.703 GB, scaled by path-pd")
+# the scanline-pair form with three warpgroups a CTA (the shape the autotuner
+# picks for the 64-pair batch), measured on a small case of the same workload
+# and scaled by path-pd: the first 8 pairs of the mixed workload (3.741 G
+# path-pd, 3.74 GB of byte slabs), the autotuner's two three-warpgroup launches
+# (the 5th and 6th aggregation launches) of
+#   VX_SGM_AGG_FORM=pairs ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,
+#       gpu__time_duration.sum --clock-control none -k regex:aggregate_kernel
+#       python bench.py --workload mixed --pairs 8 --kernels-only --steps 2 --warmup 3
+# read 2.520 / 2.462 GB (cost-volume reads that missed L2) + write 3.703 GB
+# (slabs and escaped vectors' shadow) = 6.19 GB a launch. One warpgroup a CTA
+# moves 5.84 GB (fewer pairs in flight share L2 better); the 1280x720 D=192
+# pair case moves 0.77 of its algorithmic bytes, as here (0.83).
+AGG_DRAM_BYTES_PER_PATH_PD = (0.5 * (2.520e9 + 2.462e9) + 3.703e9) / 3740620800
+AGG_TRAFFIC_SAMPLE = ("first 8 pairs of the mixed workload (3.741 G path-pd), the autotuner's "
+                      "three-warpgroup scanline-pair launches: ncu dram__bytes_read.sum 2.49 GB + "
+                      "dram__bytes_write.sum 3.70 GB per launch, scaled by path-pd")
 
 FORM_NAMES = {64: "scanline pairs, 64-scanline units", 32: "single scanline, 32-scanline units",
               1: "across-lanes scan, one lane segment a scanline"}
