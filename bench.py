@@ -44,7 +44,9 @@ def workload(rank: int, name: str = "mixed"):
     """(w, h, D, seed) tuples; seeds differ per rank (replicas). "mixed" is the 64-pair
     mixed-size workload; "profile" is a small case for profiler captures (2 pairs of
     1242x375, D=128: 1.9 GB of path slabs, larger than L2) and "profile-mix" a
-    medium one that fills the GPU with all three D (32 pairs of 320x240)."""
+    medium one that fills the GPU with all three D (32 pairs of 320x240);
+    "profile-many" has enough aggregation units (3840) to keep every warp of a
+    three-warpgroup launch busy in a small memory footprint."""
     if name == "profile":
         return [(1242, 375, 128, 1_000_003 * (rank + 1) + i) for i in range(2)]
     if name == "profile-mix":  # 32 pairs of 320x240, D cycling 64/128/192: 5 GB of slabs
@@ -53,6 +55,8 @@ def workload(rank: int, name: str = "mixed"):
         return [(1280, 720, 64, 1_000_003 * (rank + 1) + i) for i in range(8)]
     if name == "profile-hd":  # 2 pairs of 1280x720, D=192: a 354 MB cost volume (> L2), 3.6 GB with --sync
         return [(1280, 720, 192, 1_000_003 * (rank + 1) + i) for i in range(2)]
+    if name == "profile-many":  # 128 pairs of 160x120, D cycling 64/128/192: 3840 aggregation units, 2.5 GB
+        return [(160, 120, DISPARITIES[i % 3], 1_000_003 * (rank + 1) + i) for i in range(128)]
     rng = np.random.default_rng(20261203 + 7919 * rank)
     items = []
     for i in range(NUM_PAIRS):
@@ -677,7 +681,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "profile", "profile-mix", "profile-wide", "profile-hd"])
+                    choices=["mixed", "profile", "profile-mix", "profile-wide", "profile-hd", "profile-many"])
     ap.add_argument("--sync", action="store_true",
                     help="with --kernels-only: synchronous batch calls (escape pools, no graph), for "
                          "profiler captures that must stay small")
