@@ -5,6 +5,11 @@ matching cost (popcount of the census XOR, 64 where x - d < 0, 0 in the pads),
 every census load stays inside the planes' guard words and is 16-byte aligned,
 and every shared-memory tile index stays inside the launch's allocation.
 
+census.cu (staging): the asynchronously staged rows of an interior tile are
+16-byte aligned, read only inside the image row, fit the shared memory the
+launch reserves, and every window tap lands on the pixel the clamped staging
+puts there.
+
 wta.cu (row loop): the lane form chosen per pair (16 or 8 disparities a lane),
 every 16-byte store into the per-warp sums rows aligned and inside the
 dynamic shared memory, for odd widths too; the padded right-view key indices
@@ -216,3 +221,48 @@ def test_wta_right_keys_in_bounds_and_spread_over_banks():
         assert worst <= 2, (D, worst)
         if form == FORM_BYTES16 and seg >= 8 and D % 128 == 0:
             assert worst == 1, (D, worst)
+
+
+K_CENSUS_TILE = 32
+
+
+def _census_lead(rx):
+    return (16 - (rx & 15)) & 15
+
+
+def _census_row_bytes(rx):
+    return (_census_lead(rx) + K_CENSUS_TILE + 2 * rx + 15) & ~15
+
+
+def _census_smem(max_rx, max_ry):
+    w = max([K_CENSUS_TILE + 2 * max_rx] + [_census_row_bytes(r) for r in range(max_rx + 1)])
+    return w * (K_CENSUS_TILE + 2 * max_ry)
+
+
+def test_census_async_staging_geometry():
+    import numpy as np
+    rng = np.random.default_rng(3)
+    for rx in range(0, 32):
+        lead, rw = _census_lead(rx), _census_row_bytes(rx)
+        assert rw % 16 == 0 and lead + K_CENSUS_TILE + 2 * rx <= rw
+        for ry in (0, 1, 3, 7, 31):
+            assert rw * (K_CENSUS_TILE + 2 * ry) <= _census_smem(rx, ry) <= 48 * 1024
+        for W, H in ((97, 70), (1242, 375), (160, 120), (2048, 99)):
+            img = rng.integers(0, 256, (H, W), dtype=np.uint8)
+            ry = min(rx, 5)
+            sh = K_CENSUS_TILE + 2 * ry
+            for bx in range(0, W, 32):
+                for by in range(0, H, 32):
+                    x0 = bx - rx - lead
+                    interior = x0 >= 0 and x0 + rw <= W and by - ry >= 0 and by + K_CENSUS_TILE + ry <= H
+                    if not interior:
+                        continue
+                    assert x0 % 16 == 0                       # 16-byte aligned source (pitch, base aligned)
+                    staged = img[by - ry:by - ry + sh, x0:x0 + rw]  # the copies: inside rows, inside the image
+                    sw = K_CENSUS_TILE + 2 * rx
+                    ys = np.clip(np.arange(by - ry, by - ry + sh), 0, H - 1)
+                    xs = np.clip(np.arange(bx - rx, bx - rx + sw), 0, W - 1)
+                    clamped = img[np.ix_(ys, xs)]
+                    # window tap (tx + dx, ty + dy) of both stagings
+                    assert np.array_equal(staged[:, lead:lead + sw], clamped)
+

@@ -83,6 +83,32 @@ def test_edge_shapes(gpu_ctx, sgm, agg_form):
         assert_disparity_equal(got, (d, di), what=f"{w}x{h} D={nd}")
 
 
+@pytest.mark.parametrize("rx,ry", [(2, 2), (4, 3), (3, 4), (0, 3), (31, 0), (10, 1), (5, 2), (20, 0), (1, 1)])
+def test_census_staging_forms_match_oracle(gpu_ctx, sgm, rx, ry):
+    """Interior census tiles of 16-byte aligned views are staged with cp.async, border tiles
+    and unaligned views byte by byte with clamped coordinates: both give the oracle's words
+    (vx-vision/shaders/SGMStereo.metal:25-66) for an aligned texture and for a wrapped one
+    whose base and pitch are odd."""
+    import torch
+    w, h = 301, 141
+    L, R, _ = vx_sgm.synth_pair(1, w, h, 0, 12, rx * 100 + ry)
+    cfg = vx_sgm.SGMStereoConfig(num_disparities=16, census_radius_x=rx, census_radius_y=ry, num_paths=2)
+    want_l, want_r = oracle.census(L, rx, ry), oracle.census(R, rx, ry)
+    tl, tr = gpu_ctx.texture_gray8(L, w, h), gpu_ctx.texture_gray8(R, w, h)
+    assert tl.pitch % 16 == 0
+    cl, cr, _, _ = sgm.debug_dump(gpu_ctx, tl, tr, cfg)
+    assert np.array_equal(cl, want_l) and np.array_equal(cr, want_r)
+    pitch = w + 1
+    bufs = [torch.zeros(pitch * h + 1, dtype=torch.uint8, device="cuda") for _ in range(2)]
+    wl, wr = (vx_sgm.Texture.wrap_device(gpu_ctx, b.data_ptr() + 1, pitch, w, h, vx_sgm.FORMAT_U8) for b in bufs)
+    wl.upload(L)
+    wr.upload(R)
+    cl2, cr2, _, _ = sgm.debug_dump(gpu_ctx, wl, wr, cfg)
+    assert np.array_equal(cl2, want_l) and np.array_equal(cr2, want_r)
+    torch.cuda.synchronize()
+    del wl, wr, bufs
+
+
 @pytest.mark.parametrize("nd,paths,p2", [
     (128, 8, 120), (129, 2, 120), (144, 8, 300), (160, 4, 120), (192, 8, 300), (193, 4, 120),
     (208, 8, 120), (248, 2, 300), (256, 4, 300), (80, 8, 300), (24, 4, 120),

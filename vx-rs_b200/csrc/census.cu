@@ -7,7 +7,7 @@
 // u8 values, which is what this kernel does.
 //
 // Layout: each 32x32 tile of one view is staged once in shared memory with its
-// (rx, ry) apron (clamped coordinates), then every thread builds four
+// (rx, ry) apron, then every thread builds four
 // descriptors (rows 8 apart) from shared memory: large tiles, so that the
 // per-CTA costs (finding the pair, staging latency) are paid per 1024 pixels. Descriptors are written row-major (read by
 // the cost-volume kernel and by the vertical and diagonal paths of the
@@ -16,6 +16,14 @@
 // (x, y) at ((y/32)*W + x)*32 + y%32 (read by its horizontal paths: the 32
 // scanlines of a warp are the 32 rows of a band, so each column is 128
 // contiguous bytes). Output word: u32 when the window has <= 32 bits, else u64.
+//
+// Staging. A tile whose apron lies inside the image, of a view whose base and
+// pitch are 16-byte aligned, is copied with asynchronous 16-byte copies
+// (cp.async, global -> shared without registers): each staged row is the
+// 16-byte aligned segment [bx - rx - lead, +rw) with lead = (-rx) mod 16 (bx is
+// a multiple of 32), rw = lead + 32 + 2 rx rounded up to 16, read only inside
+// the row. Border tiles (and unaligned views) stage byte by byte with clamped
+// coordinates, which reproduces the shader's clamp.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -62,7 +70,7 @@ __device__ __forceinline__ uint64_t window_bits(const uint8_t* __restrict__ tile
 template <typename CT, bool BANDED>
 __global__ void __launch_bounds__(kCensusTileW * kCensusThreadsY)
 census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
-    extern __shared__ uint8_t tile_px[];
+    extern __shared__ __align__(16) uint8_t tile_px[];
     __shared__ CT tile_bits[kCensusTileH][kCensusTileW + 1];
     constexpr int kRowsPerThread = kCensusTileH / kCensusThreadsY;
     const int pi = find_pair_by_tile(pairs, num_pairs, blockIdx.x);
@@ -81,10 +89,30 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     const int sw = kCensusTileW + 2 * rx, sh = kCensusTileH + 2 * ry;
     const int tid = threadIdx.y * kCensusTileW + threadIdx.x;
     constexpr int kThreads = kCensusTileW * kCensusThreadsY;
-    for (int i = tid; i < sw * sh; i += kThreads) {
-        const int sx = min(max(bx - rx + i % sw, 0), W - 1);
-        const int sy = min(max(by - ry + i / sw, 0), H - 1);
-        tile_px[i] = img[(size_t)sy * pitch + sx];
+    const int lead = census_stage_lead(rx), rw = census_stage_row_bytes(rx);
+    const int x0 = bx - rx - lead;
+    const bool async_stage = ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch) & 15) == 0 && x0 >= 0 &&
+                             x0 + rw <= W && by - ry >= 0 && by + kCensusTileH + ry <= H;
+    int stride = sw, col0 = 0;           // staged row stride, column of x = bx - rx
+    if (async_stage) {
+        stride = rw;
+        col0 = lead;
+        const uint8_t* src = img + (size_t)(by - ry) * pitch + x0;
+        const int cpr = rw >> 4;         // 16-byte copies a row
+        const uint32_t dst0 = (uint32_t)__cvta_generic_to_shared(tile_px);
+        for (int i = tid; i < sh * cpr; i += kThreads) {
+            const int r = i / cpr, c = i - r * cpr;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst0 + (uint32_t)(r * rw + 16 * c)),
+                         "l"(src + (size_t)r * pitch + 16 * c)
+                         : "memory");
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else {
+        for (int i = tid; i < sw * sh; i += kThreads) {
+            const int sx = min(max(bx - rx + i % sw, 0), W - 1);
+            const int sy = min(max(by - ry + i / sw, 0), H - 1);
+            tile_px[i] = img[(size_t)sy * pitch + sx];
+        }
     }
     __syncthreads();
 
@@ -92,15 +120,15 @@ census_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     // was filled with clamped coordinates; interior threads read their window.
     // The common windows (5x5, 9x7) are unrolled; the radii are uniform per CTA.
     CT* rm = static_cast<CT*>(view ? pr.census_r : pr.census_l);
-    const int x = bx + threadIdx.x, cx = threadIdx.x + rx;
+    const int x = bx + threadIdx.x, cx = col0 + threadIdx.x + rx;
 #pragma unroll
     for (int k = 0; k < kRowsPerThread; ++k) {
         const int ty = threadIdx.y + k * kCensusThreadsY;
         const int y = by + ty, cy = ty + ry;
         uint64_t bits;
-        if (rx == 2 && ry == 2) bits = window_bits<2, 2>(tile_px, sw, cx, cy, rx, ry);
-        else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, sw, cx, cy, rx, ry);
-        else bits = window_bits<-1, -1>(tile_px, sw, cx, cy, rx, ry);
+        if (rx == 2 && ry == 2) bits = window_bits<2, 2>(tile_px, stride, cx, cy, rx, ry);
+        else if (rx == 4 && ry == 3) bits = window_bits<4, 3>(tile_px, stride, cx, cy, rx, ry);
+        else bits = window_bits<-1, -1>(tile_px, stride, cx, cy, rx, ry);
         if (x < W && y < H) rm[(size_t)y * W + x] = (CT)bits;
         if constexpr (BANDED) tile_bits[ty][threadIdx.x] = (CT)bits;
     }
@@ -123,7 +151,7 @@ cudaError_t launch_census(const PairDev* d_pairs, int num_pairs, int total_tiles
                           int max_ry, bool census64, bool banded, cudaStream_t stream) {
     if (total_tiles == 0) return cudaSuccess;
     const dim3 block(kCensusTileW, kCensusThreadsY);
-    const size_t smem = (size_t)(kCensusTileW + 2 * max_rx) * (kCensusTileH + 2 * max_ry);
+    const size_t smem = census_smem_bytes(max_rx, max_ry);
     count_launch();
     if (census64) {
         if (banded) census_kernel<uint64_t, true><<<total_tiles, block, smem, stream>>>(d_pairs, num_pairs);

@@ -102,6 +102,20 @@ struct UnitDev {
 constexpr int kCensusTileW = 32;   // census tile: 32 x 32 pixels of one view a CTA
 constexpr int kCensusTileH = 32;
 constexpr int kCensusThreadsY = 8; // CTA of 32 x 8 threads, four rows a thread
+// Asynchronously staged census rows (interior tiles): the 16-byte aligned
+// segment that starts lead = (-rx) mod 16 bytes before x = bx - rx (bx is a
+// multiple of 32) and covers the 32 + 2 rx apron columns, rw bytes long.
+__host__ __device__ constexpr int census_stage_lead(int rx) { return (16 - (rx & 15)) & 15; }
+__host__ __device__ constexpr int census_stage_row_bytes(int rx) {
+    return (census_stage_lead(rx) + kCensusTileW + 2 * rx + 15) & ~15;
+}
+// Dynamic shared memory of a census CTA for radii up to (max_rx, max_ry): the
+// clamped staging (rows of 32 + 2 rx bytes) or the asynchronous one (rw bytes).
+__host__ __device__ constexpr size_t census_smem_bytes(int max_rx, int max_ry) {
+    int w = kCensusTileW + 2 * max_rx;
+    for (int rx = 0; rx <= max_rx; ++rx) w = census_stage_row_bytes(rx) > w ? census_stage_row_bytes(rx) : w;
+    return (size_t)w * (kCensusTileH + 2 * max_ry);
+}
 constexpr int kAggWarpsPerBlock = 4;   // warps per TMEM warpgroup
 // Scanlines per aggregation work unit of the scanline-pair kernel (one warp:
 // two scanlines per lane); the single-scanline kernel takes 32.
