@@ -52,7 +52,13 @@ struct PairDev {
     int subpixel, lr_check, lr_tolerance;
     float invalid_value;
     int census_tile_begin; // first census tile of this pair (census launch)
-    int row_begin;         // first WTA row of this pair (WTA launch)
+    int row_begin;         // first cost-volume row of this pair (cost launch)
+    // The WTA launch takes the pairs in the order of its row-loop variants (path
+    // count, lane form), so that the CTAs running at once mostly share one
+    // variant's code: entry k of the pair array also holds the index of the k-th
+    // pair of that order and the first WTA row of that k-th pair.
+    int wta_pair;
+    int wta_row_begin;
 };
 
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
@@ -187,6 +193,34 @@ __host__ __device__ constexpr size_t aggregate_warp_smem(int dp_max, bool wide_t
 __host__ __device__ constexpr size_t aggregate_tile_offset(int dp_max) { return (size_t)(dp_max + 72) * 8; }
 
 constexpr int kWtaThreads = 256;
+// Row-loop forms of the WTA kernel: byte slabs summed 16 disparities a lane (a
+// pixel's lanes read its whole vector of a path in one round) or 8 a lane, and
+// wide slabs (8 u16 a lane). Byte slabs take 16 unless 8 keeps more lanes busy:
+// lanes per pixel are a power of two, so Dv / 16 = 9..12 chunks (D = 192: 12 of
+// 16 lanes) fill 8 lanes over 3 rounds better.
+constexpr int kFormBytes16 = 0, kFormBytes8 = 1, kFormWide = 2;
+__host__ __device__ constexpr int wta_disparities_per_lane(int form) { return form == kFormBytes16 ? 16 : 8; }
+// Lanes per pixel: the pixel's chunks rounded up to a power of two, at most
+// 16 (16-disparity chunks) or 8 (8-disparity chunks).
+__host__ __device__ constexpr int wta_lanes_per_pixel(int nd_vec, int form) {
+    const int chunks = nd_vec / wta_disparities_per_lane(form);
+    const int cap = form == kFormBytes16 ? 16 : 8;
+    int seg = 1;
+    while (seg < chunks && seg < cap) seg <<= 1;
+    return seg;
+}
+__host__ __device__ constexpr int wta_form(int nd_vec, bool wide) {
+    if (wide) return kFormWide;
+    // busy lane-rounds per lane-round: chunks / (seg * rounds), compared exactly
+    const int c16 = nd_vec / 16, s16 = wta_lanes_per_pixel(nd_vec, kFormBytes16);
+    const int c8 = nd_vec / 8, s8 = wta_lanes_per_pixel(nd_vec, kFormBytes8);
+    const int slots16 = s16 * ((c16 + s16 - 1) / s16), slots8 = s8 * ((c8 + s8 - 1) / s8);
+    return c8 * slots16 > c16 * slots8 ? kFormBytes8 : kFormBytes16;
+}
+// The row-loop variant of a pair (0..8): path class x form.
+__host__ __device__ constexpr int wta_variant(int num_paths, int nd_vec, bool wide) {
+    return (num_paths == 2 ? 0 : num_paths == 4 ? 1 : 2) * 3 + wta_form(nd_vec, wide);
+}
 // u16 sums per WTA warp in shared memory: its pixels (32 / lanes per pixel) x
 // their padded disparities (disparities a lane x lanes per pixel x rounds):
 // byte slabs 32 x 16 x 1, wide slabs 32 x 8 x 4 at most.

@@ -315,6 +315,24 @@ vx_status build_plan(const std::vector<PairSpec>& specs, Plan* plan, int unit_sc
     }
     pl.total_tiles = tiles;
     pl.total_rows = rows;
+    // The WTA launch's order: the pairs grouped by the WTA row-loop variant
+    // (path count, lane form), batch order inside a group, so that the CTAs
+    // resident at once mostly run one variant's code.
+    {
+        std::vector<int> ord(n);
+        for (int i = 0; i < n; ++i) ord[i] = i;
+        auto variant = [&](int i) {
+            const PairDev& q = pl.pairs[i];
+            return wta_variant(q.num_paths, q.nd_vec, q.wide_slabs != 0);
+        };
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return variant(a) < variant(b); });
+        int r = 0;
+        for (int k = 0; k < n; ++k) {
+            pl.pairs[k].wta_pair = ord[k];
+            pl.pairs[k].wta_row_begin = r;
+            r += pl.pairs[ord[k]].height;
+        }
+    }
 
     // Unit size, i.e. aggregation form: few units (a single pair, small batches)
     // run the across-lanes scan kernel, a segment of lanes per scanline; larger

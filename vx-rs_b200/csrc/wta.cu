@@ -35,11 +35,12 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ int find_pair_by_row(const PairDev* pairs, int n, int row) {
+// Position k of the WTA order whose rows hold this row (wta_row_begin rises with k).
+__device__ __forceinline__ int find_wta_position(const PairDev* pairs, int n, int row) {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (pairs[mid].row_begin <= row) lo = mid; else hi = mid - 1;
+        if (pairs[mid].wta_row_begin <= row) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -249,34 +250,6 @@ __device__ __forceinline__ void sum_bytes16(const RowView& rv, size_t pix, int c
     }
 }
 
-// Row-loop forms: byte slabs summed 16 disparities a lane (a pixel's lanes read
-// its whole vector of a path in one round) or 8 a lane, and wide slabs (8 u16 a
-// lane). Byte slabs take 16 unless 8 keeps more lanes busy: lanes per pixel are
-// a power of two, so Dv / 16 = 9..12 chunks (D = 192: 12 of 16 lanes) fill
-// 8 lanes over 3 rounds better.
-constexpr int kFormBytes16 = 0, kFormBytes8 = 1, kFormWide = 2;
-
-__host__ __device__ constexpr int wta_disparities_per_lane(int form) { return form == kFormBytes16 ? 16 : 8; }
-
-// Lanes per pixel: the pixel's chunks rounded up to a power of two, at most
-// 16 (16-disparity chunks) or 8 (8-disparity chunks).
-__host__ __device__ constexpr int wta_lanes_per_pixel(int nd_vec, int form) {
-    const int chunks = nd_vec / wta_disparities_per_lane(form);
-    const int cap = form == kFormBytes16 ? 16 : 8;
-    int seg = 1;
-    while (seg < chunks && seg < cap) seg <<= 1;
-    return seg;
-}
-
-__host__ __device__ constexpr int wta_form(int nd_vec, bool wide) {
-    if (wide) return kFormWide;
-    // busy lane-rounds per lane-round: chunks / (seg * rounds), compared exactly
-    const int c16 = nd_vec / 16, s16 = wta_lanes_per_pixel(nd_vec, kFormBytes16);
-    const int c8 = nd_vec / 8, s8 = wta_lanes_per_pixel(nd_vec, kFormBytes8);
-    const int slots16 = s16 * ((c16 + s16 - 1) / s16), slots8 = s8 * ((c8 + s8 - 1) / s8);
-    return c8 * slots16 > c16 * slots8 ? kFormBytes8 : kFormBytes16;
-}
-
 // Right-view keys in shared memory: column a at a + (a / 16) * pad. A warp's
 // atomicMin of one key index j goes to columns x + s - K c - j (s its pixel,
 // c the lane in the pixel), K c apart across lanes: unpadded, the 16-disparity
@@ -383,9 +356,9 @@ __device__ __forceinline__ void wta_row(const PairDev& pr, int y, uint32_t* righ
 __global__ void __launch_bounds__(kWtaThreads, 4)
 wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     extern __shared__ __align__(16) uint32_t smem[];
-    const int pi = find_pair_by_row(pairs, num_pairs, blockIdx.x);
-    const PairDev pr = pairs[pi];                  // fields live in registers
-    const int y = blockIdx.x - pr.row_begin;
+    const int k = find_wta_position(pairs, num_pairs, blockIdx.x);
+    const int y = blockIdx.x - pairs[k].wta_row_begin;
+    const PairDev pr = pairs[pairs[k].wta_pair];   // fields live in registers
     const int W = pr.width, D = pr.nd, P = pr.num_paths;
     const bool lr = pr.lr_check != 0;
 
@@ -395,7 +368,7 @@ wta_kernel(const PairDev* __restrict__ pairs, int num_pairs) {
     uint32_t* nbr = best_key + W;                             // W: S(bd-1) | S(bd+1) << 16
     // then the warps' sums (16-byte aligned)
     uint16_t* sums = reinterpret_cast<uint16_t*>(smem + ((rk + 2 * W + 3) & ~3));
-    const int form = wta_form(pr.nd_vec, pr.wide_slabs != 0);
+    const int form = wta_form(pr.nd_vec, pr.wide_slabs != 0);   // the order groups pairs by (P, form)
     const int pad = right_key_pad(wta_lanes_per_pixel(pr.nd_vec, form), form);
 
     if (lr)
