@@ -181,3 +181,27 @@ def test_synchronous_batch_escape_pools(gpu_ctx, monkeypatch, pool):
         for k, ((L, R), o, g) in enumerate(zip(pairs, ocfgs, got)):
             d, di, _ = oracle.sgm(L, R, o)
             assert_disparity_equal(g, (d, di), what=f"{form} pool={pool} pair {k}")
+
+
+def test_plan_cache_rebinds_and_revalidates(gpu_ctx):
+    """Calls whose pairs have the shapes of an earlier call reuse its plan: the pair table's
+    image and output pointers are refreshed (two pairs of one shape, alternated, each equal
+    to the oracle) and the pairs are validated again (an output of the wrong size is still
+    rejected on a cached shape)."""
+    import oracle
+    from gpu_helpers import cfg_pair, run_pair
+    w, h, nd = 211, 97, 64
+    cfg, ocfg = cfg_pair(num_disparities=nd, census_radius_x=2, census_radius_y=2, num_paths=8, lr_check=True)
+    pairs = [vx_sgm.synth_pair(k, w, h, 0, nd - 4, 500 + k)[:2] for k in range(2)]
+    want = [oracle.sgm(L, R, ocfg)[:2] for (L, R) in pairs]
+    sgm = vx_sgm.SGMStereo(gpu_ctx)
+    for k in (0, 1, 0, 1):
+        L, R = pairs[k]
+        assert_disparity_equal(run_pair(gpu_ctx, sgm, L, R, cfg), want[k], what=f"call of pair {k}")
+    L, R = pairs[0]
+    tl, tr = gpu_ctx.texture_gray8(L, w, h), gpu_ctx.texture_gray8(R, w, h)
+    small, oi = gpu_ctx.texture_output_r32float(w - 1, h), gpu_ctx.texture_output_i16(w, h)
+    with pytest.raises(vx_sgm.VxError) as e:      # the same key as the calls above: a cache hit
+        sgm.compute_disparity(gpu_ctx, tl, tr, small, cfg, output_i16=oi)
+    assert e.value.status == 5   # VX_ERR_SIZE_MISMATCH
+    sgm.close()

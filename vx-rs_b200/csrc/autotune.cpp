@@ -11,6 +11,7 @@
 // a real batch with CUDA events around the aggregation launch and records the
 // fastest in the SGMStereo handle; later batches with the same key use it. The
 // table is saved to / loaded from a small JSON file.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -37,14 +38,17 @@ TuneKey tune_key(const Plan& plan) {
 
 using namespace vxsgm;
 
-vx_status vx_sgm::plan_batch(const std::vector<PairSpec>& specs, Plan* plan) {
+namespace {
+
+// The planner proper: the plan in the autotuned form and launch shape.
+vx_status plan_uncached(vx_sgm* sgm, const std::vector<PairSpec>& specs, Plan* plan) {
     vx_status st = build_plan(specs, plan);
     if (st != VX_OK) return st;
-    Tuned t{0, 0, 0.0f};
+    vx_sgm::Tuned t{0, 0, 0.0f};
     {
-        std::lock_guard<std::mutex> lk(tune_mu);
-        auto it = tuned.find(tune_key(*plan));
-        if (it != tuned.end()) t = it->second;
+        std::lock_guard<std::mutex> lk(sgm->tune_mu);
+        auto it = sgm->tuned.find(tune_key(*plan));
+        if (it != sgm->tuned.end()) t = it->second;
     }
     if (t.warpgroups == 0) return st;          // not tuned: the planner's heuristic
     int unit = t.unit_scanlines;
@@ -54,6 +58,42 @@ vx_status vx_sgm::plan_batch(const std::vector<PairSpec>& specs, Plan* plan) {
         *plan = Plan();
         st = build_plan(specs, plan, unit, wg);
     }
+    return st;
+}
+
+}  // namespace
+
+vx_status vx_sgm::plan_batch(const std::vector<PairSpec>& specs, Plan* plan) {
+    std::string key = bucket_key(specs);
+    for (const auto& s : specs) key += s.compact_shadow ? 'c' : 'f';
+    uint64_t version;
+    {
+        std::lock_guard<std::mutex> lk(tune_mu);
+        version = tune_version;
+    }
+    {
+        std::lock_guard<std::mutex> lk(plan_mu);
+        for (auto& e : plans) {
+            if (e.key != key || e.version != version) continue;
+            for (const auto& s : specs) {          // formats, output sizes and pitches may differ
+                const vx_status vs = validate_pair(s);
+                if (vs != VX_OK) return vs;
+            }
+            *plan = e.plan;
+            rebind_pointers(*plan, specs);
+            e.last_use = ++plan_clock;
+            return VX_OK;
+        }
+    }
+    const vx_status st = plan_uncached(this, specs, plan);
+    if (st != VX_OK) return st;
+    std::lock_guard<std::mutex> lk(plan_mu);
+    if (plans.size() >= kPlanCacheEntries) {
+        auto lru = std::min_element(plans.begin(), plans.end(),
+                                    [](const PlanEntry& a, const PlanEntry& b) { return a.last_use < b.last_use; });
+        plans.erase(lru);
+    }
+    plans.push_back({key, version, *plan, ++plan_clock});
     return st;
 }
 
@@ -135,6 +175,7 @@ vx_status vx_sgm_autotune_batch(vx_sgm* sgm, vx_ctx* ctx, uint32_t n, const vx_i
     {
         std::lock_guard<std::mutex> lk(sgm->tune_mu);
         sgm->tuned[key] = {best_unit, best_w, best};
+        ++sgm->tune_version;
     }
     if (best_warpgroups) *best_warpgroups = (uint32_t)best_w;
     if (best_ms) *best_ms = best;
@@ -193,6 +234,7 @@ vx_status vx_sgm_tuning_load(vx_sgm* sgm, const char* path) {
             field(pos, end, "dp_min", &dmin);
             if (wg >= 1 && dp >= 8 && dmin >= 8 && dmin <= dp && (us == 32 || us == kUnitScanlines || us == kScanForm)) {
                 sgm->tuned[TuneKey{(int)dp, (int)c64, (int)ul, (int)wide, (int)dmin}] = {(int)us, (int)wg, (float)ms};
+                ++sgm->tune_version;
                 ++loaded;
             }
         }

@@ -18,8 +18,6 @@
 
 namespace vxsgm {
 
-namespace {
-
 std::string bucket_key(const std::vector<PairSpec>& specs) {
     std::ostringstream k;
     for (const auto& s : specs) {
@@ -35,10 +33,12 @@ std::string bucket_key(const std::vector<PairSpec>& specs) {
     }
     // The planner's overrides of the slab format and the aggregation form
     // change the plan for the same shapes.
-    for (const char* v : {"VX_SGM_SLAB_FORMAT", "VX_SGM_AGG_FORM", "VX_SGM_AGG_WARPGROUPS"})
+    for (const char* v : {"VX_SGM_SLAB_FORMAT", "VX_SGM_AGG_FORM", "VX_SGM_AGG_WARPGROUPS", "VX_SGM_SHADOW_POOL"})
         if (const char* e = std::getenv(v)) k << v << '=' << e << ';';
     return k.str();
 }
+
+namespace {
 
 void destroy_entry(vx_sgm::GraphEntry* e, cudaStream_t stream) {
     if (e->exec) cudaGraphExecDestroy(e->exec);

@@ -137,6 +137,9 @@ size_t pair_cost_bytes(uint32_t width, uint32_t height, const vx_sgm_config& cfg
 // Points plan.pairs at the images and outputs of specs (same sizes and order
 // as the specs the plan was built from).
 void rebind_pointers(Plan& plan, const std::vector<PairSpec>& specs);
+// Key of a batch's shapes: every pair's size and config in order, the output
+// kinds and the planner's environment overrides (graphs.cpp).
+std::string bucket_key(const std::vector<PairSpec>& specs);
 // Resolves the workspace-relative pointers of plan.pairs against `base`.
 void bind_plan(Plan& plan, char* base);
 // Issues the whole batch (census, cost volume, aggregation, WTA) on `stream`
@@ -194,6 +197,21 @@ struct vx_sgm {
     };
     std::mutex tune_mu;
     std::map<vxsgm::TuneKey, Tuned> tuned;
+    uint64_t tune_version = 0;      // bumped whenever `tuned` changes (under tune_mu)
+    // Plans of recent batch shapes, unbound (workspace offsets), so that a call
+    // with the shapes of an earlier one skips the planner: the pair table's
+    // pointers are refreshed and the pairs validated again. Keyed by the bucket
+    // key, the pairs' shadow kinds and the tuning table's version.
+    struct PlanEntry {
+        std::string key;
+        uint64_t version;
+        vxsgm::Plan plan;
+        uint64_t last_use;
+    };
+    static constexpr size_t kPlanCacheEntries = 16;
+    std::mutex plan_mu;
+    std::vector<PlanEntry> plans;
+    uint64_t plan_clock = 0;
     // Plan of a batch in the autotuned form and launch shape (the planner's
     // heuristic when the batch's key was not tuned).
     vx_status plan_batch(const std::vector<vxsgm::PairSpec>& specs, vxsgm::Plan* plan);
