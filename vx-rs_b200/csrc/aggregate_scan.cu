@@ -303,10 +303,12 @@ __global__ void __launch_bounds__(kThreads, 3)
 scan_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs, const UnitDev* __restrict__ units,
             const int num_units, unsigned* __restrict__ counter) {
     const int lane = threadIdx.x & 31;
+    // First unit of a warp by an interleaved rank (warp w of CTA b: w * grid + b),
+    // so that the first, longest units of the LPT order go one to an SM before any
+    // SM gets a second; later units come from the counter, after the warps' firsts.
+    const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+    int u = (int)((threadIdx.x >> 5) * gridDim.x + blockIdx.x);
     for (;;) {
-        int u = 0;
-        if (lane == 0) u = (int)atomicAdd(counter, 1u);
-        u = __shfl_sync(kFull, u, 0);
         if (u >= num_units) break;
         const UnitDev unit = units[u];
         const JobDev job = jobs[unit.job];
@@ -315,6 +317,8 @@ scan_kernel(const PairDev* __restrict__ pairs, const JobDev* __restrict__ jobs, 
         if (pr.nd == pr.nd_vec) run_unit<8, CP, true>(pr, job, unit.first_scanline, g, lane);
         else run_unit<8, CP, false>(pr, job, unit.first_scanline, g, lane);
         __syncwarp();
+        if (lane == 0) u = warps + (int)atomicAdd(counter, 1u);
+        u = __shfl_sync(kFull, u, 0);
     }
 }
 
@@ -335,8 +339,10 @@ cudaError_t launch(const PairDev* d_pairs, const JobDev* d_jobs, const UnitDev* 
         cudaGetLastError();
         per_sm = 1;
     }
+    // At least one CTA an SM even for few units: a lone pair's units then run one
+    // warp to a scheduler where they can (its scanlines are latency-bound chains).
     int grid = sms * per_sm;
-    const int needed = (num_units + kThreads / 32 - 1) / (kThreads / 32);
+    const int needed = std::max((num_units + kThreads / 32 - 1) / (kThreads / 32), sms);
     if (grid > needed) grid = needed;
     if (std::getenv("VX_SGM_DEBUG"))
         std::fprintf(stderr, "vx_sgm: aggregation (scan) %d CTAs x %d threads (%d an SM), %d units\n", grid, kThreads,
