@@ -255,7 +255,11 @@ AGG_TRAFFIC_SAMPLE = ("first 8 pairs of the mixed workload (3.741 G path-pd), th
 FORM_NAMES = {64: "scanline pairs, 64-scanline units", 32: "single scanline, 32-scanline units",
               1: "across-lanes scan, one lane segment a scanline"}
 
-SERVE_BUDGET = 40 << 30  # device bytes the server may hold for in-flight requests
+# Device bytes the server may hold for in-flight requests. A served batch lasts at
+# least as long as its longest scanline chain (a 1920-wide D = 192 request: ~10 ms),
+# so the budget sets how many requests share that time: at 1500 req/s saturation
+# 40 GB gave batches of ~13 and 130 Gpd/s, 80 GB batches of ~21 and 164 Gpd/s.
+SERVE_BUDGET = 80 << 30
 
 
 SERVED_KEYS = ("rate_per_s", "requests", "completed", "latency_ms_p50", "latency_ms_p99",
@@ -263,7 +267,7 @@ SERVED_KEYS = ("rate_per_s", "requests", "completed", "latency_ms_p50", "latency
 
 
 def served(vx_sgm, ctx, sgm, rates, max_batch=32, slots=2):
-    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, 40 GB budget.
+    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, SERVE_BUDGET device bytes.
     rates: (requests per second, number of requests) per point; a fresh server per
     point so that each point's counters are its own."""
     import loadgen
@@ -702,7 +706,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-sat-rate", type=float, default=1500.0,
                     help="arrival rate of the saturated served point (requests/s)")
-    ap.add_argument("--serve-sat-requests", type=int, default=500)
+    ap.add_argument("--serve-sat-requests", type=int, default=1000)
     ap.add_argument("--cpu-rounds", type=int, default=2,
                     help="stratified CPU-baseline rounds (one pair of every (W, H, D) stratum each)")
     ap.add_argument("--serve-max-batch", type=int, default=32, help="server: requests per batch at most")
@@ -913,7 +917,7 @@ def main():
     plain_ms = max_over_ranks(dist, plain_ms / args.plain_steps)
     plain_value = job_rate(job_pd, plain_ms)
 
-    # ---- served: continuous batching under a 40 GB budget, Poisson arrivals ----
+    # ---- served: continuous batching under SERVE_BUDGET, Poisson arrivals ----
     # One point at a moderate rate and one past saturation (arrivals faster than the
     # service rate: the queue grows, batches fill and several run at once).
     serve, serve_sat = served(vx_sgm, ctx, sgm, [(args.serve_rate, args.serve_requests),
