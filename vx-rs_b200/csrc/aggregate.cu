@@ -709,28 +709,35 @@ double budgets_for(const int* dps, const double* work, int n_dps, int warpgroups
     return best_sum < 0 ? 0.0 : best;
 }
 
-int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, int num_units) {
-    // The count with the most balanced capacity (warpgroups / budgets_for's
-    // ratio), among those that still leave every warp ~2.5 units of the queue:
-    // a scanline is serial work, so a crowded SM slows the longest units down
-    // and few units per warp cannot even that out.
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, double path_pd,
+                       double chain_steps) {
+    // The count whose estimated launch time is lowest. A launch lasts at least
+    // as long as its queued work at the rate of w warpgroups an SM, and as long
+    // as its longest unit: a serial chain of chain_steps (pixel step x D)
+    // updates, slower the more warps share its scheduler. Rates and chain
+    // times measured on B200 (148 SMs, 1.965 GHz) with batches of 13 to 64
+    // mixed pairs (D 64..192, up to 1920 wide) at each warpgroup count; the
+    // work is scaled by budgets_for's ratio when the TMEM budgets of w
+    // warpgroups cannot share the work evenly. Four warpgroups (D <= 128
+    // only) extrapolate the trend.
+    static constexpr double kPathPdPerUs[kAggMaxWarpgroups] = {1.42e6, 2.10e6, 2.32e6, 2.40e6};
+    static constexpr double kUsPerChainStep[kAggMaxWarpgroups] = {0.0288, 0.037, 0.045, 0.053};
     const int wmax = max_warpgroups(dps[0], dps[n_dps - 1], wide_tiles);
     int best_w = 1;
-    double best_cap = 0.0;
+    double best_us = 0.0;
     for (int w = 1; w <= wmax; ++w) {
-        if (w > 1 && (double)num_units < 2.5 * sms * 4 * w) break;
         int cols[kAggMaxWarpgroups];
         const double ratio = budgets_for(dps, work, n_dps, w, cols);
         if (ratio <= 0.0) break;
-        const double cap = w / ratio;
-        if (cap > best_cap * 1.03) {
-            best_cap = cap;
+        const double us = std::max(path_pd * ratio / kPathPdPerUs[w - 1], chain_steps * kUsPerChainStep[w - 1]);
+        if (w == 1 || us < best_us) {
+            best_us = us;
             best_w = w;
         }
     }
+    if (std::getenv("VX_SGM_DEBUG"))
+        std::fprintf(stderr, "vx_sgm: %.3g path-pd, longest chain %.3g steps: %d warpgroups (%.0f us estimated)\n",
+                     path_pd, chain_steps, best_w, best_us);
     return best_w;
 }
 

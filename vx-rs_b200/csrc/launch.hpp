@@ -53,7 +53,10 @@ namespace pairs {
 cudaError_t prepare();
 int max_warpgroups(int dp_max, int dp_min, bool wide_tiles);
 double budgets_for(const int* dps, const double* work, int n_dps, int warpgroups, int* cols);
-int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, int num_units);
+// Warpgroups a CTA for a batch of path_pd path-pixel-disparities whose longest
+// unit is a chain of chain_steps (pixel step x D) updates.
+int default_warpgroups(const int* dps, const double* work, int n_dps, bool wide_tiles, double path_pd,
+                       double chain_steps);
 cudaError_t launch(int dp_max, bool wide_tiles, const AggLaunch& L, const PairDev* d_pairs,
                    const JobDev* d_jobs, const UnitDev* d_units, int num_units, unsigned* counters,
                    cudaStream_t stream, bool compact = false);

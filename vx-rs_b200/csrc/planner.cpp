@@ -174,8 +174,11 @@ vx_status plan_queues(Plan& pl, int warpgroups, CostFn unit_cost) {
     }
     const int nd = (int)dps.size();
     const int wmax = pairs::max_warpgroups(dps[0], dps[nd - 1], pl.wide_tiles);
+    double path_pd = 0.0;
+    for (const PairDev& p : pl.pairs) path_pd += (double)p.width * p.height * p.nd * p.num_paths;
+    const double chain = nu > 0 ? (double)unit_cost(pl.units[0]) : 0.0;   // units are longest-first
     int wg = warpgroups > 0 ? std::min(warpgroups, wmax)
-                            : pairs::default_warpgroups(dps.data(), work.data(), nd, pl.wide_tiles, nu);
+                            : pairs::default_warpgroups(dps.data(), work.data(), nd, pl.wide_tiles, path_pd, chain);
     int cols[kAggMaxWarpgroups] = {};
     while (wg > 1 && pairs::budgets_for(dps.data(), work.data(), nd, wg, cols) <= 0.0) --wg;
     if (wg == 1) cols[0] = dps[0];
