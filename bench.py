@@ -255,26 +255,28 @@ AGG_TRAFFIC_SAMPLE = ("first 8 pairs of the mixed workload (3.741 G path-pd), th
 FORM_NAMES = {64: "scanline pairs, 64-scanline units", 32: "single scanline, 32-scanline units",
               1: "across-lanes scan, one lane segment a scanline"}
 
-# Device bytes the server may hold for in-flight requests. A served batch lasts at
-# least as long as its longest scanline chain (a 1920-wide D = 192 request: ~10 ms),
-# so the budget sets how many requests share that time: at 1500 req/s saturation
-# 40 GB gave batches of ~13 and 130 Gpd/s, 80 GB batches of ~21 and 164 Gpd/s.
-SERVE_BUDGET = 80 << 30
+# Device bytes the server may hold for in-flight requests: the served workload's
+# 40 GB admission cap. A served batch lasts at least as long as its longest scanline
+# chain (a 1920-wide D = 192 request: ~10 ms), so the budget sets how many requests
+# share that time; the saturated point is also measured with SERVE_BUDGET_LARGE
+# (batches of ~21 requests instead of ~13) and reported apart.
+SERVE_BUDGET = 40 << 30
+SERVE_BUDGET_LARGE = 80 << 30
 
 
 SERVED_KEYS = ("rate_per_s", "requests", "completed", "latency_ms_p50", "latency_ms_p99",
                "throughput_gpd_s", "achieved_rate_per_s", "mean_batch", "max_batches_in_flight")
 
 
-def served(vx_sgm, ctx, sgm, rates, max_batch=32, slots=2):
-    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, SERVE_BUDGET device bytes.
+def served(vx_sgm, ctx, sgm, rates, max_batch=32, slots=2, budget=SERVE_BUDGET):
+    """Served SGM: open-loop Poisson arrivals, mixed sizes and D, `budget` device bytes.
     rates: (requests per second, number of requests) per point; a fresh server per
     point so that each point's counters are its own."""
     import loadgen
     reqs = loadgen.make_requests(48)
     out = []
     for r, num_requests in rates:
-        srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=SERVE_BUDGET, max_batch=max_batch,
+        srv = vx_sgm.Server(sgm, ctx, memory_budget_bytes=budget, max_batch=max_batch,
                             max_inflight_batches=slots)
         loadgen.run_poisson(srv, reqs, 100.0, 16)  # warm the pool and the planner
         before = srv.stats()
@@ -285,7 +287,7 @@ def served(vx_sgm, ctx, sgm, rates, max_batch=32, slots=2):
         batches = after["batches"] - before["batches"]
         res["mean_batch"] = (after["completed"] - before["completed"]) / batches if batches else None
         res["max_batches_in_flight"] = after["max_batches_in_flight"]
-        res["max_batch"], res["slots"] = max_batch, slots
+        res["max_batch"], res["slots"], res["budget_bytes"] = max_batch, slots, budget
         out.append(res)
     return out
 
@@ -296,8 +298,8 @@ def run_serve_sweep(args, local_rank):
     sgm = vx_sgm.SGMStereo(ctx)
     rates = [float(x) for x in args.serve_sweep.split(",") if x]
     for res in served(vx_sgm, ctx, sgm, [(r, args.serve_requests) for r in rates], args.serve_max_batch,
-                      args.serve_slots):
-        print(json.dumps({"metric": "served SGM", "unit": UNIT, "budget_bytes": SERVE_BUDGET,
+                      args.serve_slots, int(args.serve_budget_gb * (1 << 30))):
+        print(json.dumps({"metric": "served SGM", "unit": UNIT,
                           "workload": "Poisson arrivals, sizes {640x480,1242x375,1280x720,1920x1080} "
                                       "x D{64,128,192}, 8 paths", **res}), flush=True)
 
@@ -711,6 +713,8 @@ def main():
                     help="stratified CPU-baseline rounds (one pair of every (W, H, D) stratum each)")
     ap.add_argument("--serve-max-batch", type=int, default=32, help="server: requests per batch at most")
     ap.add_argument("--serve-slots", type=int, default=2, help="server: batches in flight at most")
+    ap.add_argument("--serve-budget-gb", type=float, default=SERVE_BUDGET / (1 << 30),
+                    help="server: device budget of the served sweep (GiB)")
     ap.add_argument("--serve-sweep", default="",
                     help="comma-separated arrival rates: run the served sweep and print one JSON "
                          "line per rate instead of the benchmark")
@@ -919,9 +923,12 @@ def main():
 
     # ---- served: continuous batching under SERVE_BUDGET, Poisson arrivals ----
     # One point at a moderate rate and one past saturation (arrivals faster than the
-    # service rate: the queue grows, batches fill and several run at once).
+    # service rate: the queue grows, batches fill and several run at once), and the
+    # saturated point again with the larger budget.
     serve, serve_sat = served(vx_sgm, ctx, sgm, [(args.serve_rate, args.serve_requests),
                                                  (args.serve_sat_rate, args.serve_sat_requests)])
+    serve_sat_large, = served(vx_sgm, ctx, sgm, [(args.serve_sat_rate, args.serve_sat_requests)],
+                              budget=SERVE_BUDGET_LARGE)
 
     # ---- roofline of the dominant kernel (path aggregation) ----
     peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
@@ -963,8 +970,10 @@ def main():
                   "latency_ms_p50": float(np.percentile(lat, 50)),
                   "latency_ms_p99": float(np.percentile(lat, 99)),
                   "batched_over_plain": value / plain_value},
-        "served": {k: serve[k] for k in SERVED_KEYS},
-        "served_saturated": {k: serve_sat[k] for k in SERVED_KEYS},
+        "served": {**{k: serve[k] for k in SERVED_KEYS}, "budget_bytes": SERVE_BUDGET},
+        "served_saturated": {**{k: serve_sat[k] for k in SERVED_KEYS}, "budget_bytes": SERVE_BUDGET},
+        "served_saturated_80gb": {**{k: serve_sat_large[k] for k in SERVED_KEYS},
+                                  "budget_bytes": SERVE_BUDGET_LARGE},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "copies": "pinned host buffers, every step; double-buffered on two copy streams, "
