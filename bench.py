@@ -924,7 +924,11 @@ def main():
     # ---- served: continuous batching under SERVE_BUDGET, Poisson arrivals ----
     # One point at a moderate rate and one past saturation (arrivals faster than the
     # service rate: the queue grows, batches fill and several run at once), and the
-    # saturated point again with the larger budget.
+    # saturated point again with the larger budget. The batched steps are done: their
+    # graph's workspace (~94 GB with full u16 shadows) goes back to the pool first, so
+    # that the server's arena fits beside the rest on every rank.
+    sgm.set_graph_cache(0)
+    ctx.synchronize()
     serve, serve_sat = served(vx_sgm, ctx, sgm, [(args.serve_rate, args.serve_requests),
                                                  (args.serve_sat_rate, args.serve_sat_requests)])
     serve_sat_large, = served(vx_sgm, ctx, sgm, [(args.serve_sat_rate, args.serve_sat_requests)],
