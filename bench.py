@@ -11,8 +11,11 @@ Metric: Gpixel-disparities/s (sum of W*H*D over pairs / seconds), whole job.
 Also reported: the plain per-pair path on the same pairs (one synchronous
 compute_disparity call per pair, like the reference) with p50/p99 latency per
 pair, the end-to-end rate through the C ABI with host buffers (H2D of the
-images and D2H of the disparity maps inside the timed region), the roofline
-of the aggregation kernel, and the CPU oracle on a bounded sample.
+images and D2H of the disparity maps inside the timed region), the served
+path (continuous batching of Poisson arrivals of mixed requests under the 40 GB
+device budget, at a moderate rate and past saturation, and past saturation
+again under 80 GB), the roofline of the aggregation kernel, and the CPU oracle
+on a bounded sample.
 
 Multi-GPU (torchrun): replicas only - every rank runs its own 64 pairs
 (different seeds), no data-path collective; value = all ranks' pixel-
